@@ -1,0 +1,153 @@
+/* C ABI of libqsfb200.so, the B200 (sm_100a) Brouwer-Zimmermann distance engine.
+ *
+ * Part 1 is the drop-in boundary: the nine distfind_* entry points with the exact
+ * signatures, struct layouts and return codes of the reference's
+ * cpp/distfind/capi.h:12-111 (Quantinuum/Qubitserf), which its Python layer binds with
+ * ctypes (python/qubitserf/distfind/_native.py:15-107).  Pointing QUBITSERF_LIB at this
+ * library makes the unchanged reference Python call it.  Only method "bz" on backend
+ * "gpu"/"auto" runs here; there is no CPU fallback.
+ *
+ * Return codes: 0 ok; 1 null pointer; 2 not a [z|x] matrix / bad operator length;
+ * 3 method "cc" on a non-CSS code (the reference's own codes, capi.cpp:152-404);
+ * 4 no usable sm_100 device or a CUDA error; 5 method/backend/size this engine does not
+ * run (e.g. "mitm", "cc", backend "cpu", n > 1024 after pivot removal); 6 device memory
+ * exhausted.  Codes 4-6 surface in the reference Python as RuntimeError.
+ *
+ * Part 2 (qsfb_*) adds what the reference has no ABI for: the per-level enumeration on a
+ * raw plan, the host problem reduction, the witness and per-level counts of the last
+ * call, and the batched engine.
+ */
+#ifndef QSF_B200_H
+#define QSF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- Part 1: drop-in */
+
+/* Same layout as the reference DistfindResult (cpp/distfind/capi.h:12-19). */
+typedef struct {
+    int distance;       /* -1 if undefined (no logicals / empty code) */
+    int lower_bound;
+    int proven;
+    int levels;
+    double seconds;
+    char backend[16];   /* "cuda" */
+} DistfindResult;
+
+/* Same layout as the reference DistfindOpResult (cpp/distfind/capi.h:39-45). */
+typedef struct {
+    int z_weight;
+    int x_weight;
+    int proven;
+    double seconds;
+    char backend[16];
+} DistfindOpResult;
+
+/* Replaces distfind_css_distance, cpp/distfind/capi.h:24-29 (which: 'Z','X','M'). */
+int distfind_css_distance(const uint8_t* Hx, int hx_rows, int hx_cols,
+                          const uint8_t* Hz, int hz_rows, int hz_cols,
+                          const char* method, char which, const char* backend,
+                          int threads, int verbose, DistfindResult* out);
+
+/* Replaces distfind_classical_distance, cpp/distfind/capi.h:32-36. */
+int distfind_classical_distance(const uint8_t* H, int rows, int cols,
+                                const char* method, const char* backend,
+                                int threads, int verbose, DistfindResult* out);
+
+/* Replaces distfind_operator_weight, cpp/distfind/capi.h:52-58. */
+int distfind_operator_weight(const uint8_t* Gx, int gx_rows, int gx_cols,
+                             const uint8_t* Gz, int gz_rows, int gz_cols,
+                             const uint8_t* z_op, const uint8_t* x_op, int n,
+                             const char* method, const char* backend,
+                             int threads, int verbose, DistfindOpResult* out);
+
+/* Replaces distfind_subsystem_distance, cpp/distfind/capi.h:63-68. */
+int distfind_subsystem_distance(const uint8_t* Gx, int gx_rows, int gx_cols,
+                                const uint8_t* Gz, int gz_rows, int gz_cols,
+                                const char* method, char which, const char* backend,
+                                int threads, int verbose, DistfindResult* out);
+
+/* Replaces distfind_stabilizer_distance, cpp/distfind/capi.h:81-85. */
+int distfind_stabilizer_distance(const uint8_t* S, int rows, int cols,
+                                 const char* method, char which, const char* backend,
+                                 int threads, int verbose, DistfindResult* out);
+
+/* Replaces distfind_subsystem_stabilizer_distance, cpp/distfind/capi.h:91-95. */
+int distfind_subsystem_stabilizer_distance(const uint8_t* G, int rows, int cols,
+                                           const char* method, char which, const char* backend,
+                                           int threads, int verbose, DistfindResult* out);
+
+/* Replaces distfind_stabilizer_operator_weight, cpp/distfind/capi.h:103-108. */
+int distfind_stabilizer_operator_weight(const uint8_t* G, int rows, int cols,
+                                        const uint8_t* op, int op_len,
+                                        const char* method, const char* backend,
+                                        int threads, int verbose, DistfindResult* out);
+
+/* Replaces distfind_backend_available, cpp/distfind/capi.h:110: "gpu"/"cuda"/"auto" -> 1
+ * when an sm_100 device is usable; "cpu"/"metal" -> 0. */
+int distfind_backend_available(const char* name);
+
+/* Replaces distfind_version, cpp/distfind/capi.h:111. */
+const char* distfind_version(void);
+
+/* ---------------------------------------------------------------- Part 2: engine */
+
+/* Summary of the last distance call made on the calling thread. */
+typedef struct {
+    int distance;
+    int lower_bound;
+    int proven;
+    int levels;
+    int witness_ok;          /* 1: the witness was verified on the host */
+    int witness_bits;        /* length of the witness (problem columns) */
+    int witness_side;        /* 0 = single/Z side, 1 = X side */
+    int kernel_launches;
+    double seconds;          /* wall time of the call */
+    double device_ms;        /* device time of list generation + pair sweeps */
+    unsigned long long codewords;  /* evaluated (information set, combination) pairs */
+} QsfbReport;
+
+/* One weight level of one BZ subproblem on a raw plan: the semantics of the reference's
+ * qsf::Backend::enumerate(EnumPlan) (cpp/qsf/backend.hpp:21-42, 53-61;
+ * cpp/qsf/enum_core.hpp:74-88, 109-194).  gamma = num_gamma*K*stride words, check =
+ * kcheck*stride words, row-major; kcheck == 0 means every codeword counts.  Rows need not be
+ * systematic.  *out_best = min(current_best, lightest logical codeword < current_best);
+ * out_counts[g] = evaluated combinations of set g (== C(K,d)); the arg-min is returned as
+ * (*out_g, *out_rank) with rank in the lexicographic order of cpp/qsf/combinatorics.hpp:52-61
+ * (-1 if nothing beat current_best). */
+int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const uint64_t* gamma,
+                        int kcheck, const uint64_t* check, int current_best, int* out_best,
+                        unsigned long long* out_counts, int* out_g, unsigned long long* out_rank);
+
+/* Host reduction only (no device): the BZ subproblem and its information sets exactly as
+ * the reference's bz_distance sees them (cpp/distfind/bz.cpp:141-159).  kind: 0 classical(H=A),
+ * 1 css Z (Hx=A,Hz=B), 2 css X, 3 subsystem Z (Gx=A,Gz=B), 4 subsystem X, 5 non-CSS
+ * stabilizer S=A after the (a|b)->(a|b|a^b) isometry.  meta = {n, K, num_gamma, kcheck, even,
+ * count_all, seed_upper, stride}; gamma (num_gamma*K*stride words) and check
+ * (kcheck*stride words) are written when they fit.  Returns 0, 1 (null), 7 (buffer small). */
+int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
+                         int bc, int* meta, int* ranks, int max_gamma, uint64_t* gamma,
+                         long long max_words, uint64_t* check, long long max_check);
+
+/* Report / witness / per-level counts of the last distance call on this thread. */
+int qsfb_last_report(QsfbReport* out);
+/* Witness codeword as 0/1 bytes (problem columns: n for CSS/classical, 3q after the
+ * symplectic isometry); returns its length or -1. */
+int qsfb_last_witness(uint8_t* out, int cap);
+/* Level records: side[i], w[i], g[i], count[i] for every (level, active set); returns the
+ * number of records (written up to cap). */
+int qsfb_last_counts(int* side, int* w, int* g, unsigned long long* count, int cap);
+
+/* Name of the device in use ("" without one) and its SM count. */
+const char* qsfb_device_name(void);
+int qsfb_device_sms(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSF_B200_H */

@@ -1,0 +1,285 @@
+"""ctypes binding to libqsfb200.so (the C ABI in include/qsf_b200.h).
+
+The distfind_* part mirrors the reference's python/qubitserf/distfind/_native.py:15-258
+(same structs, argtypes and rc -> exception mapping); the qsfb_* part exposes the engine
+extras (raw-plan enumeration, host reduction, witness, per-level counts, batch).
+The library is loaded in-tree; importing this module never builds anything and raises if
+the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("QSFB_LIB", PKG / "libqsfb200.so"))
+
+ERRORS = {
+    1: "null pointer",
+    2: "not a [z|x] matrix / bad operator length",
+    3: "method 'cc' is not supported for non-CSS codes",
+    4: "no usable sm_100 device, or a CUDA error",
+    5: "unsupported method/backend/size on the B200 engine",
+    6: "device memory exhausted",
+    7: "output buffer too small",
+}
+
+
+class DistfindResult(ctypes.Structure):
+    _fields_ = [("distance", ctypes.c_int), ("lower_bound", ctypes.c_int),
+                ("proven", ctypes.c_int), ("levels", ctypes.c_int),
+                ("seconds", ctypes.c_double), ("backend", ctypes.c_char * 16)]
+
+
+class DistfindOpResult(ctypes.Structure):
+    _fields_ = [("z_weight", ctypes.c_int), ("x_weight", ctypes.c_int),
+                ("proven", ctypes.c_int), ("seconds", ctypes.c_double),
+                ("backend", ctypes.c_char * 16)]
+
+
+class QsfbReport(ctypes.Structure):
+    _fields_ = [("distance", ctypes.c_int), ("lower_bound", ctypes.c_int),
+                ("proven", ctypes.c_int), ("levels", ctypes.c_int),
+                ("witness_ok", ctypes.c_int), ("witness_bits", ctypes.c_int),
+                ("witness_side", ctypes.c_int), ("kernel_launches", ctypes.c_int),
+                ("seconds", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("codewords", ctypes.c_ulonglong)]
+
+
+# (name, restype, argtypes) of every exported function; tests check the export list.
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_ip = ctypes.POINTER(ctypes.c_int)
+_ullp = ctypes.POINTER(ctypes.c_ulonglong)
+_rp = ctypes.POINTER(DistfindResult)
+_i, _c, _s, _d = ctypes.c_int, ctypes.c_char, ctypes.c_char_p, ctypes.c_double
+SIGNATURES = [
+    ("distfind_css_distance", _i, [_u8p, _i, _i, _u8p, _i, _i, _s, _c, _s, _i, _i, _rp]),
+    ("distfind_classical_distance", _i, [_u8p, _i, _i, _s, _s, _i, _i, _rp]),
+    ("distfind_operator_weight", _i, [_u8p, _i, _i, _u8p, _i, _i, _u8p, _u8p, _i, _s, _s, _i, _i,
+                                      ctypes.POINTER(DistfindOpResult)]),
+    ("distfind_subsystem_distance", _i, [_u8p, _i, _i, _u8p, _i, _i, _s, _c, _s, _i, _i, _rp]),
+    ("distfind_stabilizer_distance", _i, [_u8p, _i, _i, _s, _c, _s, _i, _i, _rp]),
+    ("distfind_subsystem_stabilizer_distance", _i, [_u8p, _i, _i, _s, _c, _s, _i, _i, _rp]),
+    ("distfind_stabilizer_operator_weight", _i, [_u8p, _i, _i, _u8p, _i, _s, _s, _i, _i, _rp]),
+    ("distfind_backend_available", _i, [_s]),
+    ("distfind_version", _s, []),
+    ("qsfb_enumerate_plan", _i, [_i, _i, _i, _i, _i, _u64p, _i, _u64p, _i, _ip, _ullp, _ip,
+                                 _ullp]),
+    ("qsfb_prepare_problem", _i, [_i, _u8p, _i, _i, _u8p, _i, _i, _ip, _ip, _i, _u64p,
+                                  ctypes.c_longlong, _u64p, ctypes.c_longlong]),
+    ("qsfb_last_report", _i, [ctypes.POINTER(QsfbReport)]),
+    ("qsfb_last_witness", _i, [_u8p, _i]),
+    ("qsfb_last_counts", _i, [_ip, _ip, _ip, _ullp, _i]),
+    ("qsfb_device_name", _s, []),
+    ("qsfb_device_sms", _i, []),
+]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m qubitserf_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc == 3:
+        raise ValueError("method 'cc' (connected cluster) is not supported for non-CSS "
+                         "codes; use 'bz' or 'mitm'")
+    if rc != 0:
+        raise RuntimeError(f"{what} failed (rc={rc}: {ERRORS.get(rc, 'error')})")
+
+
+def as_u8(mat) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(mat, dtype=np.uint8) & 1)
+    if a.ndim != 2:
+        raise ValueError("expected a 2D 0/1 matrix")
+    return a
+
+
+def as_u8_vec(v) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(v, dtype=np.uint8) & 1).reshape(-1)
+
+
+def _p(a):
+    return a.ctypes.data_as(_u8p)
+
+
+def css_distance_raw(Hx, Hz, method, which, backend, threads, verbose):
+    ax, az = as_u8(Hx), as_u8(Hz)
+    out = DistfindResult()
+    rc = lib().distfind_css_distance(_p(ax), ax.shape[0], ax.shape[1], _p(az), az.shape[0],
+                                     az.shape[1], method.encode(), which.encode()[:1] or b"M",
+                                     backend.encode(), int(threads), 1 if verbose else 0,
+                                     ctypes.byref(out))
+    _check(rc, "distfind_css_distance")
+    return out
+
+
+def classical_distance_raw(H, method, backend, threads, verbose):
+    a = as_u8(H)
+    out = DistfindResult()
+    rc = lib().distfind_classical_distance(_p(a), a.shape[0], a.shape[1], method.encode(),
+                                           backend.encode(), int(threads), 1 if verbose else 0,
+                                           ctypes.byref(out))
+    _check(rc, "distfind_classical_distance")
+    return out
+
+
+def operator_weight_raw(Gx, Gz, z_op, x_op, method, backend, threads, verbose):
+    ax, az = as_u8(Gx), as_u8(Gz)
+    z, x = as_u8_vec(z_op), as_u8_vec(x_op)
+    n = ax.shape[1]
+    if az.shape[1] != n:
+        raise ValueError("Gx and Gz must have the same number of columns (n)")
+    if z.shape[0] != n or x.shape[0] != n:
+        raise ValueError("z_op and x_op must be length n = %d" % n)
+    out = DistfindOpResult()
+    rc = lib().distfind_operator_weight(_p(ax), ax.shape[0], ax.shape[1], _p(az), az.shape[0],
+                                        az.shape[1], _p(z), _p(x), n, method.encode(),
+                                        backend.encode(), int(threads), 1 if verbose else 0,
+                                        ctypes.byref(out))
+    _check(rc, "distfind_operator_weight")
+    return out
+
+
+def subsystem_distance_raw(Gx, Gz, method, which, backend, threads, verbose):
+    ax, az = as_u8(Gx), as_u8(Gz)
+    out = DistfindResult()
+    rc = lib().distfind_subsystem_distance(_p(ax), ax.shape[0], ax.shape[1], _p(az),
+                                           az.shape[0], az.shape[1], method.encode(),
+                                           which.encode()[:1] or b"M", backend.encode(),
+                                           int(threads), 1 if verbose else 0, ctypes.byref(out))
+    _check(rc, "distfind_subsystem_distance")
+    return out
+
+
+def stabilizer_distance_raw(S, method, which, backend, threads, verbose):
+    a = as_u8(S)
+    if a.shape[1] % 2 != 0:
+        raise ValueError("symplectic stabilizer matrix must have 2n (even) columns")
+    out = DistfindResult()
+    rc = lib().distfind_stabilizer_distance(_p(a), a.shape[0], a.shape[1], method.encode(),
+                                            which.encode()[:1] or b"M", backend.encode(),
+                                            int(threads), 1 if verbose else 0, ctypes.byref(out))
+    _check(rc, "distfind_stabilizer_distance")
+    return out
+
+
+def subsystem_stabilizer_distance_raw(G, method, which, backend, threads, verbose):
+    a = as_u8(G)
+    if a.shape[1] % 2 != 0:
+        raise ValueError("symplectic gauge matrix must have 2n (even) columns")
+    out = DistfindResult()
+    rc = lib().distfind_subsystem_stabilizer_distance(_p(a), a.shape[0], a.shape[1],
+                                                      method.encode(),
+                                                      which.encode()[:1] or b"M",
+                                                      backend.encode(), int(threads),
+                                                      1 if verbose else 0, ctypes.byref(out))
+    _check(rc, "distfind_subsystem_stabilizer_distance")
+    return out
+
+
+def stabilizer_operator_weight_raw(G, op, method, backend, threads, verbose):
+    a = as_u8(G)
+    o = as_u8_vec(op)
+    if a.shape[1] % 2 != 0:
+        raise ValueError("symplectic gauge matrix must have 2n (even) columns")
+    if o.shape[0] != a.shape[1]:
+        raise ValueError("operator must be a length-2n symplectic [z|x] vector")
+    out = DistfindResult()
+    rc = lib().distfind_stabilizer_operator_weight(_p(a), a.shape[0], a.shape[1], _p(o),
+                                                   o.shape[0], method.encode(), backend.encode(),
+                                                   int(threads), 1 if verbose else 0,
+                                                   ctypes.byref(out))
+    _check(rc, "distfind_stabilizer_operator_weight")
+    return out
+
+
+def backend_available(name: str) -> bool:
+    return bool(lib().distfind_backend_available(name.encode()))
+
+
+def version() -> str:
+    return lib().distfind_version().decode()
+
+
+# ---------------------------------------------------------------- engine extras
+def enumerate_plan(n, K, d, gamma, check, current_best):
+    """One level on a raw plan (gamma: [ng, K, stride] uint64, check: [kcheck, stride])."""
+    stride = (n + 63) // 64
+    g = np.ascontiguousarray(gamma, dtype=np.uint64).reshape(-1)
+    ng = g.size // (K * stride)
+    c = np.ascontiguousarray(check, dtype=np.uint64).reshape(-1)
+    kcheck = c.size // stride
+    cbuf = c if c.size else np.zeros(1, np.uint64)
+    best = ctypes.c_int(0)
+    counts = np.zeros(ng, dtype=np.uint64)
+    og = ctypes.c_int(-1)
+    orank = ctypes.c_ulonglong(0)
+    rc = lib().qsfb_enumerate_plan(n, stride, K, d, ng, g.ctypes.data_as(_u64p), kcheck,
+                                   cbuf.ctypes.data_as(_u64p), int(current_best),
+                                   ctypes.byref(best), counts.ctypes.data_as(_ullp),
+                                   ctypes.byref(og), ctypes.byref(orank))
+    _check(rc, "qsfb_enumerate_plan")
+    return best.value, counts, og.value, orank.value
+
+
+def prepare_problem(kind, A, B=None):
+    a = as_u8(A)
+    b = as_u8(B) if B is not None else np.zeros((0, a.shape[1]), np.uint8)
+    meta = (ctypes.c_int * 8)()
+    ncol = a.shape[1] * 3 // 2 if kind == 5 else a.shape[1]
+    stride = (ncol + 63) // 64
+    maxg = ncol + 2
+    ranks = (ctypes.c_int * maxg)()
+    gamma = np.zeros(maxg * ncol * stride + 1, dtype=np.uint64)
+    check = np.zeros(ncol * stride + 1, dtype=np.uint64)
+    rc = lib().qsfb_prepare_problem(kind, _p(a), a.shape[0], a.shape[1],
+                                    _p(b) if b.size else None, b.shape[0], b.shape[1], meta,
+                                    ranks, maxg, gamma.ctypes.data_as(_u64p), gamma.size,
+                                    check.ctypes.data_as(_u64p), check.size)
+    _check(rc, "qsfb_prepare_problem")
+    n, K, ng, kcheck, even, count_all, seed_upper, stride = list(meta)
+    return {"n": n, "K": K, "stride": stride, "ranks": [ranks[i] for i in range(ng)],
+            "gamma": gamma[: ng * K * stride].reshape(ng, K, stride).copy(),
+            "check": check[: kcheck * stride].reshape(kcheck, stride).copy(),
+            "even": bool(even), "count_all": bool(count_all), "seed_upper": seed_upper}
+
+
+def last_report() -> QsfbReport:
+    r = QsfbReport()
+    lib().qsfb_last_report(ctypes.byref(r))
+    return r
+
+
+def last_witness():
+    n = lib().qsfb_last_witness(None, 0)
+    if n < 0:
+        return None
+    buf = np.zeros(n, dtype=np.uint8)
+    lib().qsfb_last_witness(_p(buf), n)
+    return buf
+
+
+def last_counts():
+    n = lib().qsfb_last_counts(None, None, None, None, 0)
+    side = (ctypes.c_int * max(n, 1))()
+    w = (ctypes.c_int * max(n, 1))()
+    g = (ctypes.c_int * max(n, 1))()
+    cnt = (ctypes.c_ulonglong * max(n, 1))()
+    lib().qsfb_last_counts(side, w, g, cnt, n)
+    return [(side[i], w[i], g[i], int(cnt[i])) for i in range(n)]

@@ -1,0 +1,438 @@
+// extern "C" boundary of libqsfb200.so.  The distfind_* functions keep the reference's
+// signatures, result structs, dispatch and return codes (cpp/distfind/capi.cpp:144-420);
+// every accepted call runs the BZ enumeration on the GPU and there is no CPU path.
+#include "../../include/qsf_b200.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bz.hpp"
+#include "engine.hpp"
+#include "problem.hpp"
+
+using namespace qsfb;
+
+namespace {
+
+struct LastCall {
+    QsfbReport rep{};
+    std::vector<u8> witness;
+    std::vector<int> side, w, g;
+    std::vector<unsigned long long> count;
+};
+thread_local LastCall g_last;
+
+void record(const BzResult& r, int n_bits) {
+    LastCall& L = g_last;
+    std::memset(&L.rep, 0, sizeof(L.rep));
+    L.rep.distance = r.distance;
+    L.rep.lower_bound = r.lower_bound;
+    L.rep.proven = r.proven ? 1 : 0;
+    L.rep.levels = r.levels;
+    L.rep.witness_ok = r.witness_ok ? 1 : 0;
+    L.rep.witness_side = r.witness_side;
+    L.rep.kernel_launches = r.stats.launches;
+    L.rep.seconds = r.seconds;
+    L.rep.device_ms = r.stats.ms_gen + r.stats.ms_pairs;
+    L.rep.codewords = r.stats.codewords;
+    L.witness.clear();
+    if (!r.witness.empty()) {
+        L.witness.resize(n_bits);
+        for (int j = 0; j < n_bits; ++j)
+            L.witness[j] = (u8)((r.witness[j >> 6] >> (j & 63)) & 1u);
+    }
+    L.rep.witness_bits = (int)L.witness.size();
+    L.side.clear(); L.w.clear(); L.g.clear(); L.count.clear();
+    for (const LevelRecord& lr : r.trace)
+        for (size_t gi = 0; gi < lr.counts.size(); ++gi) {
+            L.side.push_back(lr.side);
+            L.w.push_back(lr.w);
+            L.g.push_back((int)gi);
+            L.count.push_back(lr.counts[gi]);
+        }
+}
+
+void fill(DistfindResult* out, const BzResult& r) {
+    out->distance = r.distance;
+    out->lower_bound = r.lower_bound;
+    out->proven = r.proven ? 1 : 0;
+    out->levels = r.levels;
+    out->seconds = r.seconds;
+    std::strncpy(out->backend, "cuda", sizeof(out->backend) - 1);
+    out->backend[sizeof(out->backend) - 1] = '\0';
+}
+
+// Only method "bz" on an accelerator backend runs here.
+int check_dispatch(const char* method, const char* backend) {
+    const std::string m = method ? method : "bz";
+    const std::string b = backend ? backend : "auto";
+    if (m != "bz") return kErrUnsupported;
+    if (b != "auto" && b != "gpu" && b != "cuda") return kErrUnsupported;
+    return kOk;
+}
+
+Device* device_or(int* rc) {
+    Device* d = Device::get(rc);
+    if (!d) *rc = kErrDevice;
+    return d;
+}
+
+BzOptions options(int verbose) {
+    BzOptions o;
+    o.verbose = verbose != 0;
+    return o;
+}
+
+// Merge for the (non-interleaved) subsystem min, cpp/distfind/capi.cpp:265-274.
+BzResult min_of(const BzResult& z, const BzResult& x) {
+    auto v = [](int d) { return d < 0 ? (1 << 30) : d; };
+    BzResult r = (v(x.distance) < v(z.distance)) ? x : z;
+    r.distance = std::min(v(z.distance), v(x.distance));
+    if (r.distance >= (1 << 30)) r.distance = -1;
+    r.lower_bound = std::min(z.lower_bound, x.lower_bound);
+    r.seconds = z.seconds + x.seconds;
+    r.proven = z.proven && x.proven;
+    r.levels = (v(x.distance) < v(z.distance)) ? x.levels : z.levels;
+    r.stats.ms_gen = z.stats.ms_gen + x.stats.ms_gen;
+    r.stats.ms_pairs = z.stats.ms_pairs + x.stats.ms_pairs;
+    r.stats.codewords = z.stats.codewords + x.stats.codewords;
+    r.stats.launches = z.stats.launches + x.stats.launches;
+    r.trace = z.trace;
+    for (LevelRecord lr : x.trace) { lr.side = 1; r.trace.push_back(lr); }
+    return r;
+}
+
+// CSS routing shared by distfind_css_distance and the symplectic CSS fast path.
+int css_like(Device* dev, const Mat& A, const Mat& B, bool subsystem, char which, int verbose,
+             DistfindResult* out) {
+    auto prob = [&](char w) {
+        return subsystem ? subsystem_problem(A, B, w) : css_problem(A, B, w);
+    };
+    BzResult r;
+    int rc;
+    int nbits;
+    if (which == 'Z' || which == 'X') {
+        Problem p = prob(which);
+        nbits = p.n;
+        rc = bz_distance(dev, p, options(verbose), r);
+    } else if (subsystem) {
+        Problem pz = prob('Z'), px = prob('X');
+        nbits = pz.n;
+        BzResult rz, rx;
+        rc = bz_distance(dev, pz, options(verbose), rz);
+        if (rc == kOk) rc = bz_distance(dev, px, options(verbose), rx);
+        if (rc == kOk) r = min_of(rz, rx);
+    } else {
+        Problem pz = prob('Z'), px = prob('X');
+        nbits = pz.n;
+        rc = bz_min_interleaved(dev, pz, px, options(verbose), r);
+    }
+    if (rc != kOk) return rc;
+    fill(out, r);
+    record(r, nbits);
+    return kOk;
+}
+
+int symplectic_driver(const Mat& gauge, bool subsystem, const char* method, char which,
+                      const char* backend, int verbose, DistfindResult* out) {
+    if (gauge.cols % 2 != 0) return kErrShape;
+    const std::string m = method ? method : "bz";
+    const bool css = is_css_symplectic(gauge);
+    if (m == "cc" && !css) return kErrMethod;
+    int rc = check_dispatch(method, backend);
+    if (rc != kOk) return rc;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    if (css) {
+        auto hxhz = split_css(gauge);
+        return css_like(dev, hxhz.first, hxhz.second, subsystem, which, verbose, out);
+    }
+    Mat Snorm = subsystem ? symplectic_center(gauge) : gauge;
+    Problem sp = symplectic_problem(Snorm, gauge);
+    BzResult r;
+    rc = symplectic_bz_distance(dev, sp, options(verbose), r);
+    if (rc != kOk) return rc;
+    fill(out, r);
+    record(r, 3 * sp.qubits);
+    return kOk;
+}
+
+}  // namespace
+
+extern "C" {
+
+int distfind_css_distance(const uint8_t* Hx, int hx_rows, int hx_cols, const uint8_t* Hz,
+                          int hz_rows, int hz_cols, const char* method, char which,
+                          const char* backend, int threads, int verbose, DistfindResult* out) {
+    (void)threads;
+    if (!out || !Hx || !Hz) return kErrNull;
+    int rc = check_dispatch(method, backend);
+    if (rc != kOk) return rc;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    Mat A = from_dense(Hx, hx_rows, hx_cols), B = from_dense(Hz, hz_rows, hz_cols);
+    return css_like(dev, A, B, false, which, verbose, out);
+}
+
+int distfind_classical_distance(const uint8_t* H, int rows, int cols, const char* method,
+                                const char* backend, int threads, int verbose,
+                                DistfindResult* out) {
+    (void)threads;
+    if (!out || !H) return kErrNull;
+    int rc = check_dispatch(method, backend);
+    if (rc != kOk) return rc;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    Problem p = classical_problem(from_dense(H, rows, cols));
+    BzResult r;
+    rc = bz_distance(dev, p, options(verbose), r);
+    if (rc != kOk) return rc;
+    fill(out, r);
+    record(r, p.n);
+    return kOk;
+}
+
+int distfind_operator_weight(const uint8_t* Gx, int gx_rows, int gx_cols, const uint8_t* Gz,
+                             int gz_rows, int gz_cols, const uint8_t* z_op, const uint8_t* x_op,
+                             int n, const char* method, const char* backend, int threads,
+                             int verbose, DistfindOpResult* out) {
+    (void)threads;
+    (void)n;
+    if (!out || !Gx || !Gz || !z_op || !x_op) return kErrNull;
+    std::string m = method ? method : "bz";
+    if (m == "cc") {
+        std::fprintf(stderr,
+                     "distfind: operator weight has no connected-cluster form (the coset "
+                     "parity-check is dense); using BZ instead.\n");
+        m = "bz";
+    }
+    int rc = check_dispatch(m.c_str(), backend);
+    if (rc != kOk) return rc;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    Mat A = from_dense(Gx, gx_rows, gx_cols), B = from_dense(Gz, gz_rows, gz_cols);
+    double secs = 0.0;
+    bool proven = true;
+    BzResult last;
+    int nbits = A.cols;
+    // cpp/distfind/op_weight.cpp:22-41: Z part modulo rowspace(Gz), X part modulo rowspace(Gx).
+    auto solve = [&](const Mat& G, const uint8_t* vec, int* res) -> int {
+        if (in_rowspace(G, vec)) { *res = 0; return kOk; }
+        Problem p = coset_problem(G, vec);
+        BzResult r;
+        const int e = bz_distance(dev, p, options(verbose), r);
+        if (e != kOk) return e;
+        secs += r.seconds;
+        proven = proven && r.proven;
+        last = r;
+        *res = r.distance;
+        return kOk;
+    };
+    int zw = -1, xw = -1;
+    rc = solve(B, z_op, &zw);
+    if (rc != kOk) return rc;
+    rc = solve(A, x_op, &xw);
+    if (rc != kOk) return rc;
+    out->z_weight = zw;
+    out->x_weight = xw;
+    out->proven = proven ? 1 : 0;
+    out->seconds = secs;
+    std::strncpy(out->backend, "cuda", sizeof(out->backend) - 1);
+    out->backend[sizeof(out->backend) - 1] = '\0';
+    record(last, nbits);
+    return kOk;
+}
+
+int distfind_subsystem_distance(const uint8_t* Gx, int gx_rows, int gx_cols, const uint8_t* Gz,
+                                int gz_rows, int gz_cols, const char* method, char which,
+                                const char* backend, int threads, int verbose,
+                                DistfindResult* out) {
+    (void)threads;
+    if (!out || !Gx || !Gz) return kErrNull;
+    int rc = check_dispatch(method, backend);
+    if (rc != kOk) return rc;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    Mat A = from_dense(Gx, gx_rows, gx_cols), B = from_dense(Gz, gz_rows, gz_cols);
+    return css_like(dev, A, B, true, which, verbose, out);
+}
+
+int distfind_stabilizer_distance(const uint8_t* S, int rows, int cols, const char* method,
+                                 char which, const char* backend, int threads, int verbose,
+                                 DistfindResult* out) {
+    (void)threads;
+    if (!out || !S) return kErrNull;
+    return symplectic_driver(from_dense(S, rows, cols), false, method, which, backend, verbose,
+                             out);
+}
+
+int distfind_subsystem_stabilizer_distance(const uint8_t* G, int rows, int cols,
+                                           const char* method, char which, const char* backend,
+                                           int threads, int verbose, DistfindResult* out) {
+    (void)threads;
+    if (!out || !G) return kErrNull;
+    return symplectic_driver(from_dense(G, rows, cols), true, method, which, backend, verbose,
+                             out);
+}
+
+int distfind_stabilizer_operator_weight(const uint8_t* G, int rows, int cols, const uint8_t* op,
+                                        int op_len, const char* method, const char* backend,
+                                        int threads, int verbose, DistfindResult* out) {
+    (void)threads;
+    if (!out || !G || !op) return kErrNull;
+    if (cols % 2 != 0 || op_len != cols) return kErrShape;
+    int rc = check_dispatch(method, backend);
+    if (rc != kOk) return rc;
+    Mat mG = from_dense(G, rows, cols);
+    BzResult r;
+    if (in_rowspace(mG, op)) {
+        r.distance = 0;
+        r.lower_bound = 0;
+        r.proven = true;
+        fill(out, r);
+        record(r, 0);
+        return kOk;
+    }
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    Problem sp = symplectic_coset_problem(mG, op);
+    rc = symplectic_bz_distance(dev, sp, options(verbose), r);
+    if (rc != kOk) return rc;
+    fill(out, r);
+    record(r, 3 * sp.qubits);
+    return kOk;
+}
+
+int distfind_backend_available(const char* name) {
+    const std::string b = name ? name : "auto";
+    if (b == "gpu" || b == "cuda" || b == "auto") return Device::available() ? 1 : 0;
+    return 0;
+}
+
+const char* distfind_version(void) { return "0.1.0"; }
+
+// ---------------------------------------------------------------- Part 2
+int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const uint64_t* gamma,
+                        int kcheck, const uint64_t* check, int current_best, int* out_best,
+                        unsigned long long* out_counts, int* out_g,
+                        unsigned long long* out_rank) {
+    if (!gamma || !out_best || (kcheck > 0 && !check)) return kErrNull;
+    if (stride != words_for(n) || K < 1 || d < 1 || d > K || num_gamma < 1) return kErrShape;
+    int rc = kOk;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    Problem p;
+    p.n = n;
+    p.count_all = kcheck == 0;
+    p.code_gen = Mat(K, n);
+    p.check = Mat(kcheck, n);
+    if (kcheck > 0) std::copy(check, check + (size_t)kcheck * stride, p.check.w.begin());
+    std::vector<InfoSet> sets(num_gamma);
+    for (int g = 0; g < num_gamma; ++g) {
+        sets[g].g = Mat(K, n);
+        std::copy(gamma + (size_t)g * K * stride, gamma + (size_t)(g + 1) * K * stride,
+                  sets[g].g.w.begin());
+        sets[g].rank = 0;   // raw rows: no pivot structure is assumed
+    }
+    SessionLease lease(dev);
+    if (!lease.s) return kErrDevice;
+    SideDev S;
+    rc = S.init(dev, lease.s, p, sets);
+    if (rc != kOk) return rc;
+    std::vector<LevelReq> q(1);
+    q[0].side = &S;
+    q[0].w = d;
+    q[0].active = num_gamma;
+    q[0].bound = current_best >= kWeightNone ? 4094 : current_best - 1;
+    std::vector<LevelOut> o;
+    rc = run_levels(lease.s, q, o, nullptr);
+    if (rc != kOk) return rc;
+    *out_best = o[0].found ? std::min(current_best, o[0].wt) : current_best;
+    if (out_counts)
+        for (int g = 0; g < num_gamma; ++g) out_counts[g] = o[0].counts[g];
+    if (out_g) *out_g = o[0].found ? o[0].g : -1;
+    if (out_rank) *out_rank = o[0].found ? o[0].rank : ~0ull;
+    return kOk;
+}
+
+int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
+                         int bc, int* meta, int* ranks, int max_gamma, uint64_t* gamma,
+                         long long max_words, uint64_t* check, long long max_check) {
+    if (!A || !meta) return kErrNull;
+    Mat mA = from_dense(A, ar, ac);
+    Mat mB = (B && br > 0) ? from_dense(B, br, bc) : Mat(0, ac);
+    Problem p;
+    switch (kind) {
+        case 0: p = classical_problem(mA); break;
+        case 1: p = css_problem(mA, mB, 'Z'); break;
+        case 2: p = css_problem(mA, mB, 'X'); break;
+        case 3: p = subsystem_problem(mA, mB, 'Z'); break;
+        case 4: p = subsystem_problem(mA, mB, 'X'); break;
+        case 5:
+            if (ac % 2) return kErrShape;
+            p = isometry_extend(symplectic_problem(mA, mA));
+            break;
+        default: return kErrShape;
+    }
+    const int K = p.code_gen.rows, stride = words_for(p.n);
+    std::vector<InfoSet> sets;
+    if (K > 0) sets = information_sets(p.code_gen);
+    const int ng = (int)sets.size();
+    const int kcheck = p.count_all ? 0 : p.check.rows;
+    meta[0] = p.n; meta[1] = K; meta[2] = ng; meta[3] = kcheck;
+    meta[4] = p.even ? 1 : 0; meta[5] = p.count_all ? 1 : 0; meta[6] = p.seed_upper;
+    meta[7] = stride;
+    if (ng > max_gamma || (long long)ng * K * stride > max_words ||
+        (long long)kcheck * stride > max_check)
+        return 7;
+    for (int g = 0; g < ng; ++g) {
+        if (ranks) ranks[g] = sets[g].rank;
+        if (gamma)
+            std::copy(sets[g].g.w.begin(), sets[g].g.w.end(), gamma + (size_t)g * K * stride);
+    }
+    if (check)
+        for (int c = 0; c < kcheck; ++c)
+            std::copy(p.check.row(c), p.check.row(c) + stride, check + (size_t)c * stride);
+    return kOk;
+}
+
+int qsfb_last_report(QsfbReport* out) {
+    if (!out) return kErrNull;
+    *out = g_last.rep;
+    return kOk;
+}
+
+int qsfb_last_witness(uint8_t* out, int cap) {
+    if (g_last.witness.empty()) return -1;
+    const int n = (int)g_last.witness.size();
+    if (out) std::copy(g_last.witness.begin(), g_last.witness.begin() + std::min(n, cap), out);
+    return n;
+}
+
+int qsfb_last_counts(int* side, int* w, int* g, unsigned long long* count, int cap) {
+    const int n = (int)g_last.count.size();
+    for (int i = 0; i < std::min(n, cap); ++i) {
+        if (side) side[i] = g_last.side[i];
+        if (w) w[i] = g_last.w[i];
+        if (g) g[i] = g_last.g[i];
+        if (count) count[i] = g_last.count[i];
+    }
+    return n;
+}
+
+const char* qsfb_device_name(void) {
+    int rc = 0;
+    Device* d = Device::get(&rc);
+    return d ? d->name.c_str() : "";
+}
+
+int qsfb_device_sms(void) {
+    int rc = 0;
+    Device* d = Device::get(&rc);
+    return d ? d->num_sms : 0;
+}
+
+}  // extern "C"

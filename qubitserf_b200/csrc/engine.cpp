@@ -1,0 +1,543 @@
+// Host side of the device engine: context, allocator, side upload and the level runner.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+namespace qsfb {
+
+cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
+                             const unsigned long long* d_binom, int num_sms, cudaStream_t st);
+cudaError_t launch_pairs(int H, int HP, bool full, const LevelDesc* d, int nd,
+                         unsigned long long jobs, unsigned long long* ctr,
+                         const unsigned long long* B, int num_sms, cudaStream_t st);
+
+namespace {
+constexpr unsigned long long kSat = ~0ull;
+size_t round_bucket(size_t b) {
+    if (b < 256) return 256;
+    size_t r = 256;
+    while (r < b) r <<= 1;
+    return r;
+}
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+}  // namespace
+
+// ------------------------------------------------------------------ Device
+Device* Device::get(int* rc) {
+    static Device* inst = nullptr;
+    static int status = -1;
+    static std::mutex once;
+    std::lock_guard<std::mutex> lk(once);
+    if (status < 0) {
+        Device* d = new Device();
+        status = d->init();
+        if (status == kOk) inst = d; else delete d;
+    }
+    if (rc) *rc = status;
+    return inst;
+}
+
+bool Device::available() {
+    int rc = 0;
+    return get(&rc) != nullptr;
+}
+
+int Device::init() {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return kErrDevice;
+    }
+    const char* env = std::getenv("QSFB_DEVICE");
+    id = env ? std::atoi(env) : 0;
+    if (id < 0 || id >= count) return kErrDevice;
+    if (cudaSetDevice(id) != cudaSuccess) return kErrDevice;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, id) != cudaSuccess) return kErrDevice;
+    // The kernels are built for sm_100a only.
+    if (prop.major != 10 || prop.minor != 0) return kErrDevice;
+    num_sms = prop.multiProcessorCount;
+    name = prop.name;
+    const int ld = kBinomMaxK + 1;
+    h_binom_.assign((size_t)(kBinomMaxN + 1) * ld, 0ull);
+    for (int n = 0; n <= kBinomMaxN; ++n) {
+        h_binom_[(size_t)n * ld] = 1ull;
+        for (int k = 1; k <= std::min(n, kBinomMaxK); ++k) {
+            const unsigned long long a = h_binom_[(size_t)(n - 1) * ld + k - 1];
+            const unsigned long long b = (k <= n - 1) ? h_binom_[(size_t)(n - 1) * ld + k] : 0ull;
+            h_binom_[(size_t)n * ld + k] = (a == kSat || b == kSat || a > kSat - b) ? kSat : a + b;
+        }
+    }
+    const size_t bytes = h_binom_.size() * sizeof(unsigned long long);
+    if (cudaMalloc((void**)&d_binom, bytes) != cudaSuccess) return kErrDevice;
+    if (cudaMemcpy(d_binom, h_binom_.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return kErrDevice;
+    return kOk;
+}
+
+unsigned long long Device::binom(int n, int k) const {
+    if (k < 0 || n < 0 || k > n) return 0ull;
+    if (n > kBinomMaxN || k > kBinomMaxK) return kSat;
+    return h_binom_[(size_t)n * (kBinomMaxK + 1) + k];
+}
+
+void* Device::alloc(size_t bytes) {
+    const size_t b = round_bucket(bytes);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.find(b);
+        if (it != free_.end()) {
+            void* p = it->second;
+            free_.erase(it);
+            cached_ -= b;
+            in_use_ += b;
+            return p;
+        }
+    }
+    cudaSetDevice(id);
+    void* p = nullptr;
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+        cudaGetLastError();
+        // Drop the cache and retry once.
+        std::multimap<size_t, void*> drop;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            drop.swap(free_);
+            cached_ = 0;
+        }
+        for (auto& kv : drop) cudaFree(kv.second);
+        if (cudaMalloc(&p, b) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    in_use_ += b;
+    return p;
+}
+
+void Device::release(void* p, size_t bytes) {
+    if (!p) return;
+    const size_t b = round_bucket(bytes);
+    std::lock_guard<std::mutex> lk(mu_);
+    free_.emplace(b, p);
+    in_use_ -= b;
+    cached_ += b;
+}
+
+Session* Device::acquire() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!idle_.empty()) {
+            Session* s = idle_.back();
+            idle_.pop_back();
+            return s;
+        }
+    }
+    cudaSetDevice(id);
+    Session* s = new Session();
+    s->dev = this;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
+void Device::give_back(Session* s) {
+    std::lock_guard<std::mutex> lk(mu_);
+    idle_.push_back(s);
+}
+
+int Session::ensure(size_t dbytes, size_t hbytes) {
+    if (d_stage.cap < dbytes) {
+        if (d_stage.d) dev->release(d_stage.d, d_stage.cap);
+        d_stage.cap = round_bucket(dbytes);
+        d_stage.d = dev->alloc(d_stage.cap);
+        if (!d_stage.d) { d_stage.cap = 0; return kErrMemory; }
+    }
+    if (h_stage.cap < hbytes) {
+        if (h_stage.h) cudaFreeHost(h_stage.h);
+        h_stage.cap = round_bucket(hbytes);
+        if (cudaMallocHost(&h_stage.h, h_stage.cap) != cudaSuccess) {
+            cudaGetLastError();
+            h_stage.h = nullptr;
+            h_stage.cap = 0;
+            return kErrMemory;
+        }
+    }
+    if (!d_ctr.d) {
+        d_ctr.cap = 64 * sizeof(unsigned long long);
+        d_ctr.d = dev->alloc(d_ctr.cap);
+        if (!d_ctr.d) return kErrMemory;
+    }
+    return kOk;
+}
+
+// ------------------------------------------------------------------ SideDev
+SideDev::~SideDev() {
+    if (!dev) return;
+    dev->release(d_red, bytes_red);
+    dev->release(d_syn, bytes_syn);
+    for (auto& kv : lists) {
+        dev->release(kv.second.words, kv.second.bytes_w);
+        dev->release(kv.second.pc, kv.second.bytes_pc);
+    }
+}
+
+int SideDev::init(Device* d, Session* s, const Problem& p, const std::vector<InfoSet>& sets) {
+    dev = d;
+    n = p.n;
+    K = p.code_gen.rows;
+    ng = (int)sets.size();
+    count_all = p.count_all;
+    kcheck = p.count_all ? 0 : p.check.rows;
+    if (K > kBinomMaxN || ng > 255 || ng == 0) return kErrUnsupported;
+    int max_red = 1;
+    ranks.resize(ng);
+    nonpivot.resize(ng);
+    for (int g = 0; g < ng; ++g) {
+        ranks[g] = sets[g].rank;
+        std::vector<char> isp(n, 0);
+        for (int c : sets[g].pivots) isp[c] = 1;
+        for (int c = 0; c < n; ++c)
+            if (!isp[c]) nonpivot[g].push_back(c);
+        max_red = std::max(max_red, (int)nonpivot[g].size());
+    }
+    W32 = (max_red + 31) / 32;
+    SW = (kcheck + 31) / 32;
+    if (W32 > 32 || SW > 32) return kErrUnsupported;
+    const int swp = std::max(SW, 1);
+    std::vector<uint32_t> red((size_t)ng * K * W32, 0u), syn((size_t)ng * K * swp, 0u);
+    for (int g = 0; g < ng; ++g) {
+        const Mat& G = sets[g].g;
+        for (int r = 0; r < K; ++r) {
+            uint32_t* o = &red[((size_t)g * K + r) * W32];
+            const u64* row = G.row(r);
+            const std::vector<int>& np = nonpivot[g];
+            for (size_t i = 0; i < np.size(); ++i) {
+                const int c = np[i];
+                if ((row[c >> 6] >> (c & 63)) & 1u) o[i >> 5] |= 1u << (i & 31);
+            }
+            uint32_t* so = &syn[((size_t)g * K + r) * swp];
+            for (int c = 0; c < kcheck; ++c)
+                if (vec_dot(p.check.row(c), row, G.stride)) so[c >> 5] |= 1u << (c & 31);
+        }
+    }
+    bytes_red = red.size() * 4;
+    bytes_syn = syn.size() * 4;
+    d_red = (uint32_t*)dev->alloc(bytes_red);
+    d_syn = (uint32_t*)dev->alloc(bytes_syn);
+    if (!d_red || !d_syn) return kErrMemory;
+    if (cudaMemcpyAsync(d_red, red.data(), bytes_red, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaMemcpyAsync(d_syn, syn.data(), bytes_syn, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrDevice;
+    }
+    return kOk;
+}
+
+// ------------------------------------------------------------------ level runner
+namespace {
+
+// P(Binomial(bits, 1/2) <= t) -- survivor rate of a probe over `bits` random bits.
+double binom_cdf_half(int bits, int t) {
+    if (t < 0) return 0.0;
+    if (t >= bits) return 1.0;
+    double logp = -bits * std::log(2.0), acc = 0.0, lc = 0.0;
+    for (int i = 0; i <= t; ++i) {
+        if (i > 0) lc += std::log((double)(bits - i + 1) / i);
+        acc += std::exp(lc + logp);
+    }
+    return acc;
+}
+
+int words_of(int bits) { return (bits + 31) / 32; }
+
+// Initial witness key: weight field = bound + 1 (the strict bound), every other bit set.
+unsigned long long key_init(int bound) {
+    const int f = std::max(0, std::min(bound + 1, 4095));
+    return ((unsigned long long)f << kKeyWtShift) | ((1ull << kKeyWtShift) - 1);
+}
+
+struct Plan {
+    int req, g, a, b, H, HP, full;
+    unsigned long long pairs;
+    int p_lo, nterms;
+    std::vector<unsigned long long> term_jobs;
+    unsigned long long jobs;
+};
+
+}  // namespace
+
+unsigned long long level_pairs(const Device* dev, int K, int w) { return dev->binom(K, w); }
+
+int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelOut>& outs,
+               RunStats* stats) {
+    Device* dev = s->dev;
+    outs.assign(reqs.size(), LevelOut());
+    if (reqs.empty()) return kOk;
+
+    // 1) plan every (request, set)
+    std::vector<Plan> plans;
+    unsigned long long total_pairs = 0;
+    for (size_t r = 0; r < reqs.size(); ++r) {
+        const LevelReq& q = reqs[r];
+        SideDev* S = q.side;
+        const int K = S->K, w = q.w;
+        if (w < 1 || w > K || w > kBinomMaxK) return kErrUnsupported;
+        const unsigned long long pairs = dev->binom(K, w);
+        if (pairs == kSat || pairs >= (1ull << 62)) return kErrUnsupported;
+        int a, b;
+        if (pairs <= (1ull << 14)) { a = w; b = 0; }
+        else { a = (w + 1) / 2; b = w - a; }
+        for (int g = 0; g < q.active; ++g) {
+            Plan P;
+            P.req = (int)r; P.g = g; P.a = a; P.b = b;
+            const int rank = S->ranks[g];
+            const int nred = (int)S->nonpivot[g].size();
+            const int wg = std::max(1, words_of(nred));
+            P.HP = wg >= 3 ? 4 : wg;
+            P.full = rank == K;
+            // smallest probe width whose random-code survivor rate is negligible
+            const int T = std::max(0, std::min(q.bound + 1, 4095));
+            const int pcmin = std::max(0, w - (K - rank));
+            int H = std::min(wg, 4);
+            for (int h = std::min(wg, 2); h < std::min(wg, 4); ++h) {
+                if (binom_cdf_half(std::min(32 * h, nred), T - 1 - pcmin) <= 1e-6) { H = h; break; }
+            }
+            P.H = H;
+            P.pairs = pairs;
+            P.p_lo = a - 1;
+            P.nterms = K - b - a + 1;
+            total_pairs += pairs;
+            plans.push_back(std::move(P));
+        }
+    }
+    // loop tile: enough jobs to keep every resident warp busy several times over
+    const unsigned long long want_jobs = (unsigned long long)dev->num_sms * 16 * 4;
+    unsigned long long lt = total_pairs / ((unsigned long long)kRegTile * want_jobs);
+    lt = std::max<unsigned long long>(32, std::min<unsigned long long>(1024, lt));
+    const int loop_tile = (int)((lt + 31) / 32 * 32);
+
+    // 2) lists to build
+    struct GenReq { SideDev* S; int g, size, reflect, HP; };
+    std::vector<GenReq> gens;
+    for (const Plan& P : plans) {
+        SideDev* S = reqs[P.req].side;
+        for (int side = 0; side < 2; ++side) {
+            const int size = side == 0 ? P.a : P.b;
+            auto key = std::make_tuple(P.g, size, side);
+            ListBuf& L = S->lists[key];
+            if (L.ready || L.words) continue;
+            L.count = dev->binom(S->K, size);
+            L.bytes_w = (size_t)L.count * P.HP * 4;
+            L.words = (uint32_t*)dev->alloc(std::max<size_t>(L.bytes_w, 16));
+            if (!L.words) return kErrMemory;
+            if (!P.full) {
+                L.bytes_pc = std::max<size_t>((size_t)L.count, 16);
+                L.pc = (uint8_t*)dev->alloc(L.bytes_pc);
+                if (!L.pc) return kErrMemory;
+            }
+            S->list_bytes += L.bytes_w + L.bytes_pc;
+            gens.push_back({S, P.g, size, side, P.HP});
+        }
+    }
+
+    // 3) term tables and job counts
+    for (Plan& P : plans) {
+        const int K = reqs[P.req].side->K;
+        P.term_jobs.assign(P.nterms + 1, 0ull);
+        unsigned long long acc = 0;
+        for (int t = 0; t < P.nterms; ++t) {
+            const int p = P.p_lo + t;
+            const unsigned long long nx = dev->binom(p, P.a - 1);
+            const unsigned long long ny = dev->binom(K - 1 - p, P.b);
+            const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
+            P.term_jobs[t] = acc;
+            acc += ((rn + kRegTile - 1) / kRegTile) * ((ln + loop_tile - 1) / loop_tile);
+        }
+        P.term_jobs[P.nterms] = acc;
+        P.jobs = acc;
+    }
+
+    // variant groups: (H, full) -> plan indices
+    std::vector<int> order(plans.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return std::make_tuple(plans[x].H, plans[x].HP, plans[x].full) <
+               std::make_tuple(plans[y].H, plans[y].HP, plans[y].full);
+    });
+
+    // 4) staging layout
+    const size_t nplans = plans.size();
+    size_t off = 0;
+    const size_t off_gen = off;
+    off = align_up(off + gens.size() * sizeof(GenDesc), 64);
+    const size_t off_lvl = off;
+    off = align_up(off + nplans * sizeof(LevelDesc), 64);
+    const size_t off_terms = off;
+    size_t terms_total = 0;
+    for (const Plan& P : plans) terms_total += P.term_jobs.size();
+    off = align_up(off + terms_total * 8, 64);
+    const size_t off_keys = off;
+    off = align_up(off + reqs.size() * 8, 64);
+    const size_t off_counts = off;
+    off = align_up(off + nplans * 8, 64);
+    const size_t total_bytes = off;
+    int rc = s->ensure(total_bytes, total_bytes);
+    if (rc != kOk) return rc;
+    char* h = (char*)s->h_stage.h;
+    char* d = (char*)s->d_stage.d;
+    std::memset(h, 0, total_bytes);
+
+    GenDesc* hg = (GenDesc*)(h + off_gen);
+    unsigned long long gen_total = 0;
+    for (size_t i = 0; i < gens.size(); ++i) {
+        const GenReq& G = gens[i];
+        ListBuf& L = G.S->lists[std::make_tuple(G.g, G.size, G.reflect)];
+        GenDesc& D = hg[i];
+        D.red = G.S->d_red + (size_t)G.g * G.S->K * G.S->W32;
+        D.out = L.words;
+        D.pc = L.pc;
+        D.entry_base = gen_total;
+        D.count = L.count;
+        D.K = G.S->K;
+        D.size = G.size;
+        D.W32 = G.S->W32;
+        D.HP = G.HP;
+        D.rank = G.S->ranks[G.g];
+        D.reflect = G.reflect;
+        gen_total += L.count;
+    }
+
+    unsigned long long* hkeys = (unsigned long long*)(h + off_keys);
+    for (size_t r = 0; r < reqs.size(); ++r)
+        hkeys[r] = key_init(reqs[r].bound);
+
+    LevelDesc* hl = (LevelDesc*)(h + off_lvl);
+    unsigned long long* hterms = (unsigned long long*)(h + off_terms);
+    size_t term_cursor = 0;
+    struct Group { int H, HP, full, first, count; unsigned long long jobs; };
+    std::vector<Group> groups;
+    for (size_t oi = 0; oi < order.size(); ++oi) {
+        const Plan& P = plans[order[oi]];
+        if (groups.empty() || groups.back().H != P.H || groups.back().HP != P.HP ||
+            groups.back().full != P.full)
+            groups.push_back({P.H, P.HP, P.full, (int)oi, 0, 0ull});
+        Group& Gp = groups.back();
+        SideDev* S = reqs[P.req].side;
+        LevelDesc& D = hl[oi];
+        const ListBuf& La = S->lists[std::make_tuple(P.g, P.a, 0)];
+        const ListBuf& Rb = S->lists[std::make_tuple(P.g, P.b, 1)];
+        D.red = S->d_red + (size_t)P.g * S->K * S->W32;
+        D.syn = S->d_syn + (size_t)P.g * S->K * std::max(S->SW, 1);
+        D.la = La.words;
+        D.pca = La.pc;
+        D.rb = Rb.words;
+        D.pcb = Rb.pc;
+        std::memcpy(hterms + term_cursor, P.term_jobs.data(), P.term_jobs.size() * 8);
+        D.term_jobs = (const uint64_t*)(d + off_terms + term_cursor * 8);
+        term_cursor += P.term_jobs.size();
+        D.key = (unsigned long long*)(d + off_keys + (size_t)P.req * 8);
+        D.count = (unsigned long long*)(d + off_counts + (size_t)order[oi] * 8);
+        D.job_base = Gp.jobs;
+        D.K = S->K; D.w = reqs[P.req].w; D.a = P.a; D.b = P.b;
+        D.W32 = S->W32; D.SW = S->SW; D.HP = P.HP;
+        D.rank = S->ranks[P.g];
+        D.g = P.g;
+        D.p_lo = P.p_lo;
+        D.nterms = P.nterms;
+        D.loop_tile = loop_tile;
+        int bits = 0;
+        while (bits < 64 && (P.pairs - 1) >> bits) ++bits;
+        D.rank_shift = std::max(0, bits - kKeyGShift);
+        D.count_all = S->count_all ? 1 : 0;
+        Gp.jobs += P.jobs;
+        Gp.count += 1;
+    }
+    if (groups.size() > 64) return kErrUnsupported;
+
+    // 5) launch
+    cudaStream_t st = s->stream;
+    if (cudaMemcpyAsync(d, h, total_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(s->d_ctr.d, 0, s->d_ctr.cap, st) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrDevice;
+    }
+    cudaEventRecord(s->ev0, st);
+    int launches = 0;
+    if (!gens.empty()) {
+        if (launch_gen_lists((const GenDesc*)(d + off_gen), (int)gens.size(), gen_total,
+                             dev->d_binom, dev->num_sms, st) != cudaSuccess)
+            return kErrDevice;
+        ++launches;
+    }
+    cudaEvent_t evm;
+    cudaEventCreate(&evm);
+    cudaEventRecord(evm, st);
+    unsigned long long all_jobs = 0;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& Gp = groups[gi];
+        if (launch_pairs(Gp.H, Gp.HP, Gp.full != 0, (const LevelDesc*)(d + off_lvl) + Gp.first, Gp.count,
+                         Gp.jobs, (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
+                         dev->num_sms, st) != cudaSuccess) {
+            cudaEventDestroy(evm);
+            return kErrDevice;
+        }
+        ++launches;
+        all_jobs += Gp.jobs;
+    }
+    cudaEventRecord(s->ev1, st);
+    if (cudaMemcpyAsync(h + off_keys, d + off_keys, off_counts + nplans * 8 - off_keys,
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        cudaEventDestroy(evm);
+        return kErrDevice;
+    }
+    for (const GenReq& G : gens) G.S->lists[std::make_tuple(G.g, G.size, G.reflect)].ready = true;
+
+    // 6) decode
+    unsigned long long* hcounts = (unsigned long long*)(h + off_counts);
+    unsigned long long cw = 0;
+    for (size_t r = 0; r < reqs.size(); ++r) {
+        LevelOut& O = outs[r];
+        O.counts.assign(reqs[r].active, 0ull);
+        const unsigned long long k0 = key_init(reqs[r].bound);
+        const unsigned long long k = hkeys[r];
+        if (k < k0) {
+            O.found = true;
+            O.wt = (int)(k >> kKeyWtShift) - 1;
+            O.g = (int)((k >> kKeyGShift) & 0xff);
+            O.rank = k & kKeyRankMask;
+        }
+    }
+    for (size_t oi = 0; oi < order.size(); ++oi) {
+        const Plan& P = plans[order[oi]];
+        outs[P.req].counts[P.g] = hcounts[order[oi]];
+        cw += hcounts[order[oi]];
+        const LevelDesc& D = hl[oi];
+        if (outs[P.req].found && outs[P.req].g == P.g) outs[P.req].rank_shift = D.rank_shift;
+    }
+    if (stats) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, s->ev0, evm);
+        cudaEventElapsedTime(&b, evm, s->ev1);
+        stats->ms_gen += a;
+        stats->ms_pairs += b;
+        stats->jobs += all_jobs;
+        stats->codewords += cw;
+        stats->launches += launches;
+    }
+    cudaEventDestroy(evm);
+    return kOk;
+}
+
+}  // namespace qsfb

@@ -1,0 +1,161 @@
+// Device side of the BZ engine: one context per process (device selected by
+// QSFB_DEVICE, default 0), a size-bucketed caching allocator, and pooled sessions (one
+// CUDA stream + staging buffers each) so that concurrent ABI calls never share a stream.
+//
+// A SideDev is the device image of one BZ subproblem: per information set the rows
+// restricted to the set's non-pivot columns, the per-row detector syndromes, and the
+// lazily built subset lists.  run_levels() enumerates any number of (side, level)
+// requests in ONE list-generation launch plus one pair-sweep launch per kernel variant,
+// which is what both the plain per-code path (one request) and the batched engine
+// (every unresolved side of a round) use.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "engine_types.hpp"
+#include "infoset.hpp"
+#include "problem.hpp"
+
+namespace qsfb {
+
+// Status codes shared with the C ABI (0..3 are the reference's own, capi.cpp).
+enum Status : int {
+    kOk = 0,
+    kErrNull = 1,
+    kErrShape = 2,
+    kErrMethod = 3,     // cc on non-CSS (reference rc 3)
+    kErrDevice = 4,     // no usable device, CUDA error, or device wait timeout
+    kErrUnsupported = 5,  // method/backend/size this engine does not run
+    kErrMemory = 6,     // admission / device memory exhausted
+};
+
+struct Session;
+
+class Device {
+public:
+    // The process-wide device context; nullptr (with *rc = kErrDevice) without a GPU.
+    static Device* get(int* rc);
+    static bool available();
+
+    int id = 0;
+    int num_sms = 0;
+    std::string name;
+    unsigned long long* d_binom = nullptr;   // (kBinomMaxN+1) x (kBinomMaxK+1), saturating
+
+    void* alloc(size_t bytes);               // caching; nullptr on failure
+    void release(void* p, size_t bytes);
+    size_t bytes_in_use() const { return in_use_; }
+    size_t bytes_cached() const { return cached_; }
+
+    Session* acquire();
+    void give_back(Session* s);
+
+    // Host-side binomial (same saturating table the kernels read).
+    unsigned long long binom(int n, int k) const;
+
+private:
+    Device() = default;
+    int init();
+    std::mutex mu_;
+    std::multimap<size_t, void*> free_;
+    size_t in_use_ = 0, cached_ = 0;
+    std::vector<Session*> idle_;
+    std::vector<unsigned long long> h_binom_;
+};
+
+// Grow-only device / pinned-host scratch owned by a session.
+struct DevScratch {
+    void* d = nullptr;
+    size_t cap = 0;
+};
+struct HostScratch {
+    void* h = nullptr;
+    size_t cap = 0;
+};
+
+struct Session {
+    Device* dev = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevScratch d_stage;    // descriptors + term tables + keys/counts
+    HostScratch h_stage;   // pinned mirror of d_stage
+    DevScratch d_ctr;      // job counters (one per kernel variant)
+    int ensure(size_t dbytes, size_t hbytes);
+};
+
+// RAII lease of a session from the device pool.
+struct SessionLease {
+    Device* dev;
+    Session* s;
+    explicit SessionLease(Device* d) : dev(d), s(d->acquire()) {}
+    ~SessionLease() { if (s) dev->give_back(s); }
+};
+
+struct ListBuf {
+    uint32_t* words = nullptr;
+    uint8_t* pc = nullptr;
+    unsigned long long count = 0;
+    size_t bytes_w = 0, bytes_pc = 0;
+    bool ready = false;
+};
+
+class SideDev {
+public:
+    SideDev() = default;
+    SideDev(const SideDev&) = delete;
+    SideDev& operator=(const SideDev&) = delete;
+    ~SideDev();
+
+    // Upload the information sets of problem `p`.  Returns a Status.
+    int init(Device* dev, Session* s, const Problem& p, const std::vector<InfoSet>& sets);
+
+    int n = 0, K = 0, ng = 0, W32 = 0, SW = 0, kcheck = 0;
+    bool count_all = false;
+    std::vector<int> ranks;
+    std::vector<std::vector<int>> nonpivot;   // per set: non-pivot columns (bit order of red)
+    Device* dev = nullptr;
+    uint32_t* d_red = nullptr;   // ng x K x W32
+    uint32_t* d_syn = nullptr;   // ng x K x max(SW,1)
+    size_t bytes_red = 0, bytes_syn = 0;
+    std::map<std::tuple<int, int, int>, ListBuf> lists;   // (g, size, reflect)
+    size_t list_bytes = 0;
+};
+
+struct LevelReq {
+    SideDev* side = nullptr;
+    int w = 0;
+    int active = 0;      // information sets [0, active) are enumerated
+    int bound = kWeightNone;  // current upper bound (candidates of weight <= bound count)
+};
+
+struct LevelOut {
+    bool found = false;  // some candidate of weight <= bound was seen
+    int wt = kWeightNone;
+    int g = -1;
+    unsigned long long rank = 0;   // lexicographic rank (shifted by rank_shift)
+    int rank_shift = 0;
+    std::vector<unsigned long long> counts;   // evaluated codewords per set [0, active)
+};
+
+struct RunStats {
+    double ms_gen = 0.0;     // device time of list generation
+    double ms_pairs = 0.0;   // device time of the pair sweep
+    unsigned long long jobs = 0;
+    unsigned long long codewords = 0;
+    int launches = 0;
+};
+
+// Enumerate every request; blocking.  Returns a Status.
+int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelOut>& outs,
+               RunStats* stats = nullptr);
+
+// Enumeration counts are the per-set C(K,w); used by tests of the job decomposition.
+unsigned long long level_pairs(const Device* dev, int K, int w);
+
+}  // namespace qsfb

@@ -1,0 +1,407 @@
+// sm_100a kernels of the BZ enumeration: list generation and the XOR-popcount pair sweep.
+//
+// Semantics kept from the reference (cpp/qsf/enum_core.hpp:74-88, 109-194): for every
+// active information set g and every w-subset S of its K rows, c = XOR of the rows; c is
+// a candidate if it is a logical (no detector, or odd overlap with some detector row) and
+// its full Hamming weight does not exceed the current bound; the level returns the
+// smallest candidate.  The traversal is this engine's own (engine_types.hpp): subsets are
+// split into a colex-ordered prefix list and a reflected-colex suffix list, so a level is
+// a set of rectangles of independent (prefix, suffix) pairs that a warp sweeps with the
+// prefix entries in registers and the suffix entries broadcast from L1.
+//
+// The hot loop is integer-issue bound: per pair H LOP3 (XOR), H POPC and one fused
+// add/min on the H probe words; the pivot columns never enter it (they contribute the
+// pivot-row count).  A pair whose probe sum reaches the bound is rejected there; the rare
+// survivors are re-evaluated over all words, tested against the detector syndromes and
+// folded into the side's packed witness key with one 64-bit atomicMin.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "engine_types.hpp"
+
+namespace qsfb {
+namespace dev {
+
+constexpr int kLd = kBinomMaxK + 1;
+constexpr int kMaxWords = 32;   // n <= 1024 bits after pivot removal; detector <= 1024 rows
+constexpr int kMaxW = 64;
+constexpr int RX = 8;           // register-side entries per lane
+constexpr int kChunk = 32;      // loop entries between survivor checks
+
+__device__ __forceinline__ unsigned long long binom(const unsigned long long* __restrict__ B,
+                                                    int n, int k) {
+    if (k < 0 || n < 0 || k > n) return 0ull;
+    return __ldg(B + (size_t)n * kLd + k);
+}
+
+// Colex unrank: the r-th s-subset of [0, hi) in colex order, written largest first into
+// c[0..s-1] (c[0] > c[1] > ...).  r = sum_i C(c_i, s - i).
+__device__ __forceinline__ void colex_unrank(const unsigned long long* __restrict__ B,
+                                             unsigned long long r, int s, int hi, int* c) {
+    for (int i = s; i >= 1; --i) {
+        // largest x in [i-1, hi-1] with C(x, i) <= r
+        int lo = i - 1, top = hi - 1;
+        while (lo < top) {
+            const int mid = (lo + top + 1) >> 1;
+            if (binom(B, mid, i) <= r) lo = mid; else top = mid - 1;
+        }
+        c[s - i] = lo;
+        r -= binom(B, lo, i);
+        hi = lo;
+    }
+}
+
+// Rows of entry e of a list: colex (reflect=0) rows ascending after reversal, or reflected
+// colex (reflect=1) rows K-1-c.  Writes rows ascending into rows[0..s-1].
+__device__ __forceinline__ void list_rows(const unsigned long long* __restrict__ B,
+                                          unsigned long long e, int s, int K, int reflect,
+                                          int* rows) {
+    int c[kMaxW];
+    colex_unrank(B, e, s, K, c);
+    for (int i = 0; i < s; ++i) rows[i] = reflect ? (K - 1 - c[i]) : c[s - 1 - i];
+}
+
+// ---------------------------------------------------------------- list generation
+__global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restrict__ descs,
+                                                        int ndesc, unsigned long long total,
+                                                        const unsigned long long* __restrict__ B) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long ge = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         ge < total; ge += stride) {
+        int lo = 0, hi = ndesc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (descs[mid].entry_base <= ge) lo = mid; else hi = mid - 1;
+        }
+        const GenDesc& D = descs[lo];
+        const unsigned long long e = ge - D.entry_base;
+        int rows[kMaxW];
+        list_rows(B, e, D.size, D.K, D.reflect, rows);
+        uint32_t acc[4] = {0u, 0u, 0u, 0u};
+        int pc = 0;
+        for (int i = 0; i < D.size; ++i) {
+            const uint32_t* r = D.red + (size_t)rows[i] * D.W32;
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+                if (h < D.HP && h < D.W32) acc[h] ^= __ldg(r + h);
+            pc += rows[i] < D.rank;
+        }
+        uint32_t* o = D.out + e * (unsigned long long)D.HP;
+        if (D.HP == 4) {
+            *reinterpret_cast<uint4*>(o) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+        } else if (D.HP == 2) {
+            *reinterpret_cast<uint2*>(o) = make_uint2(acc[0], acc[1]);
+        } else {
+            o[0] = acc[0];
+        }
+        if (D.pc) D.pc[e] = (uint8_t)pc;
+    }
+}
+
+// ---------------------------------------------------------------- survivors
+// Lexicographic rank of sorted positions (the reference's unrank order,
+// cpp/qsf/combinatorics.hpp:52-61): C(K,w) - 1 - sum_i C(K-1-s_i, w-i).
+__device__ unsigned long long lex_rank(const unsigned long long* __restrict__ B,
+                                       const int* s, int w, int K) {
+    unsigned long long acc = 0;
+    for (int i = 0; i < w; ++i) acc += binom(B, K - 1 - s[i], w - i);
+    return binom(B, K, w) - 1ull - acc;
+}
+
+// Full evaluation of register entry `ereg` against the loop entries [l0, l0+ln).  Each pair
+// is first re-screened on all stored probe words (a lower bound on its weight) and only
+// then rebuilt from its rows.  Returns the (possibly lowered) strict bound T.
+__device__ __noinline__ int survivor_scan(const LevelDesc& D, const unsigned long long* __restrict__ B,
+                                          int regX, unsigned long long xoff,
+                                          unsigned long long ereg, int pc_reg,
+                                          unsigned long long l0, int ln, int T) {
+    const int sreg = regX ? D.a : D.b;
+    const int sloop = regX ? D.b : D.a;
+    const uint32_t* regbase = regX ? D.la + xoff * (unsigned long long)D.HP : D.rb;
+    const uint32_t* lbase = regX ? D.rb : D.la + xoff * (unsigned long long)D.HP;
+    const uint8_t* lpc = regX ? D.pcb : (D.pca ? D.pca + xoff : nullptr);
+    uint32_t xr[4];
+    for (int h = 0; h < D.HP; ++h) xr[h] = __ldg(regbase + ereg * D.HP + h);
+
+    int rreg[kMaxW], rloop[kMaxW];
+    if (regX) list_rows(B, xoff + ereg, D.a, D.K, 0, rreg);
+    else list_rows(B, ereg, D.b, D.K, 1, rreg);
+    uint32_t fr[kMaxWords], sr[kMaxWords];
+    for (int h = 0; h < D.W32; ++h) fr[h] = 0u;
+    for (int h = 0; h < D.SW; ++h) sr[h] = 0u;
+    for (int i = 0; i < sreg; ++i) {
+        const uint32_t* r = D.red + (size_t)rreg[i] * D.W32;
+        for (int h = 0; h < D.W32; ++h) fr[h] ^= __ldg(r + h);
+        const uint32_t* s = D.syn + (size_t)rreg[i] * D.SW;
+        for (int h = 0; h < D.SW; ++h) sr[h] ^= __ldg(s + h);
+    }
+    for (int j = 0; j < ln; ++j) {
+        const unsigned long long el = l0 + (unsigned long long)j;
+        const int pcl = lpc ? (int)__ldg(lpc + el) : sloop;
+        int lb = pc_reg + pcl;
+        for (int h = 0; h < D.HP; ++h) lb += __popc(xr[h] ^ __ldg(lbase + el * D.HP + h));
+        if (lb >= T) continue;
+        if (regX) list_rows(B, el, D.b, D.K, 1, rloop);
+        else list_rows(B, xoff + el, D.a, D.K, 0, rloop);
+        int wt = pc_reg + pcl;
+        uint32_t fl[kMaxWords];
+        for (int h = 0; h < D.W32; ++h) fl[h] = 0u;
+        for (int i = 0; i < sloop; ++i) {
+            const uint32_t* r = D.red + (size_t)rloop[i] * D.W32;
+            for (int h = 0; h < D.W32; ++h) fl[h] ^= __ldg(r + h);
+        }
+        for (int h = 0; h < D.W32; ++h) wt += __popc(fr[h] ^ fl[h]);
+        if (wt >= T) continue;
+        bool logical = D.count_all != 0;
+        if (!logical) {
+            uint32_t acc = 0u;
+            for (int h = 0; h < D.SW; ++h) {
+                uint32_t s = sr[h];
+                for (int i = 0; i < sloop; ++i) s ^= __ldg(D.syn + (size_t)rloop[i] * D.SW + h);
+                acc |= s;
+            }
+            logical = acc != 0u;
+        }
+        if (!logical) continue;
+        // sorted positions: prefix rows (all <= p) then suffix rows (all > p)
+        int pos[kMaxW];
+        const int* pre = regX ? rreg : rloop;
+        const int* suf = regX ? rloop : rreg;
+        for (int i = 0; i < D.a; ++i) pos[i] = pre[i];
+        for (int i = 0; i < D.b; ++i) pos[D.a + i] = suf[i];
+        const unsigned long long rk = lex_rank(B, pos, D.w, D.K) >> D.rank_shift;
+        const unsigned long long key = ((unsigned long long)(wt + 1) << kKeyWtShift) |
+                                       ((unsigned long long)D.g << kKeyGShift) |
+                                       (rk & kKeyRankMask);
+        const unsigned long long old = atomicMin(D.key, key);
+        const unsigned long long cur = old < key ? old : key;
+        const int nb = (int)(cur >> kKeyWtShift);
+        if (nb < T) T = nb;
+    }
+    return T;
+}
+
+// ---------------------------------------------------------------- pair sweep
+template <int H>
+__device__ __forceinline__ int probe_sum(const uint32_t (&x)[H], const uint32_t (&y)[H]) {
+    int s = 0;
+#pragma unroll
+    for (int h = 0; h < H; ++h) s += __popc(x[h] ^ y[h]);
+    return s;
+}
+
+template <int H, int HP>
+__device__ __forceinline__ void load_entry(const uint32_t* __restrict__ p, uint32_t (&v)[H]) {
+    if constexpr (HP == 4) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(p));
+        const uint32_t t[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int h = 0; h < H; ++h) v[h] = t[h];
+    } else if constexpr (HP == 2) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2*>(p));
+        v[0] = q.x;
+        if constexpr (H > 1) v[1] = q.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+
+// m = min(m, popc-sum + extra) with the add folded into the DPX add-min where possible.
+template <int H>
+__device__ __forceinline__ int fold_min(const uint32_t (&x)[H], const uint32_t (&y)[H],
+                                        int extra, int m) {
+    if constexpr (H == 1) {
+        return __viaddmin_s32(__popc(x[0] ^ y[0]), extra, m);
+    } else if constexpr (H == 2) {
+        return __viaddmin_s32(__popc(x[0] ^ y[0]) + extra, __popc(x[1] ^ y[1]), m);
+    } else if constexpr (H == 3) {
+        return __viaddmin_s32(__popc(x[0] ^ y[0]) + __popc(x[1] ^ y[1]) + extra,
+                              __popc(x[2] ^ y[2]), m);
+    } else {
+        return __viaddmin_s32(__popc(x[0] ^ y[0]) + __popc(x[1] ^ y[1]) + __popc(x[2] ^ y[2]) + extra,
+                              __popc(x[3] ^ y[3]), m);
+    }
+}
+
+template <int H, int HP, bool FULL>
+__global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict__ descs,
+                                                    int ndesc, unsigned long long total_jobs,
+                                                    unsigned long long* __restrict__ job_counter,
+                                                    const unsigned long long* __restrict__ B) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long job = 0;
+        if (lane == 0) job = atomicAdd(job_counter, 1ull);
+        job = __shfl_sync(0xffffffffu, job, 0);
+        if (job >= total_jobs) break;
+
+        int lo = 0, hi = ndesc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (descs[mid].job_base <= job) lo = mid; else hi = mid - 1;
+        }
+        const LevelDesc& D = descs[lo];
+        const unsigned long long local = job - D.job_base;
+        // term t: largest t with term_jobs[t] <= local
+        int tl = 0, th = D.nterms - 1;
+        while (tl < th) {
+            const int mid = (tl + th + 1) >> 1;
+            if (__ldg(D.term_jobs + mid) <= local) tl = mid; else th = mid - 1;
+        }
+        const unsigned long long idx = local - __ldg(D.term_jobs + tl);
+        const int p = D.p_lo + tl;
+        const unsigned long long nx = binom(B, p, D.a - 1);
+        const unsigned long long ny = binom(B, D.K - 1 - p, D.b);
+        const unsigned long long xoff = binom(B, p, D.a);
+        const int regX = nx >= ny;
+        const unsigned long long reg_n = regX ? nx : ny;
+        const unsigned long long loop_n = regX ? ny : nx;
+        const unsigned long long njl = (loop_n + D.loop_tile - 1) / D.loop_tile;
+        const unsigned long long ri = idx / njl, li = idx - ri * njl;
+        const unsigned long long reg0 = ri * kRegTile;
+        const unsigned long long reg_cnt =
+            (reg_n - reg0) < (unsigned long long)kRegTile ? (reg_n - reg0) : kRegTile;
+        const unsigned long long loop0 = li * D.loop_tile;
+        const int loop_cnt = (int)((loop_n - loop0) < (unsigned long long)D.loop_tile
+                                       ? (loop_n - loop0) : (unsigned long long)D.loop_tile);
+        const uint32_t* regbase = regX ? D.la + xoff * HP : D.rb;
+        const uint8_t* regpc = regX ? (D.pca ? D.pca + xoff : nullptr) : D.pcb;
+        const uint32_t* loopbase = regX ? D.rb : D.la + xoff * HP;
+        const uint8_t* looppc = regX ? D.pcb : (D.pca ? D.pca + xoff : nullptr);
+
+        // strict bound: the key's weight field holds (best weight + 1)
+        int T = (int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
+
+        uint32_t x[RX][H];
+        int thr[RX], m[RX], pcr[RX];
+#pragma unroll
+        for (int i = 0; i < RX; ++i) {
+            const unsigned long long e = reg0 + lane + 32 * i;
+            const bool ok = (unsigned long long)(lane + 32 * i) < reg_cnt;
+            if (ok) {
+                load_entry<H, HP>(regbase + e * HP, x[i]);
+                pcr[i] = FULL ? (regX ? D.a : D.b) : (int)regpc[e];
+            } else {
+#pragma unroll
+                for (int h = 0; h < H; ++h) x[i][h] = 0u;
+                pcr[i] = 1 << 20;
+            }
+            thr[i] = T - pcr[i] - (FULL ? (regX ? D.b : D.a) : 0);
+            m[i] = 0x7fffffff;
+        }
+
+        // Sweep the loop entries in chunks of kChunk; after each chunk the (rare) lanes
+        // whose running minimum reached the bound rescan just that chunk.
+        const uint32_t* lp = loopbase + loop0 * HP;
+        const uint8_t* lpc = FULL ? nullptr : looppc + loop0;
+        for (int c0 = 0; c0 < loop_cnt; c0 += kChunk) {
+            const int cn = (loop_cnt - c0) < kChunk ? (loop_cnt - c0) : kChunk;
+            int j = c0;
+            const int cend = c0 + cn;
+            if (FULL) {
+                for (; j + 4 <= cend; j += 4) {
+                    uint32_t y0[H], y1[H], y2[H], y3[H];
+                    load_entry<H, HP>(lp + (j + 0) * HP, y0);
+                    load_entry<H, HP>(lp + (j + 1) * HP, y1);
+                    load_entry<H, HP>(lp + (j + 2) * HP, y2);
+                    load_entry<H, HP>(lp + (j + 3) * HP, y3);
+#pragma unroll
+                    for (int i = 0; i < RX; ++i) {
+                        int mm = m[i];
+                        mm = fold_min<H>(x[i], y0, 0, mm);
+                        mm = fold_min<H>(x[i], y1, 0, mm);
+                        mm = fold_min<H>(x[i], y2, 0, mm);
+                        mm = fold_min<H>(x[i], y3, 0, mm);
+                        m[i] = mm;
+                    }
+                }
+                for (; j < cend; ++j) {
+                    uint32_t y0[H];
+                    load_entry<H, HP>(lp + j * HP, y0);
+#pragma unroll
+                    for (int i = 0; i < RX; ++i) m[i] = fold_min<H>(x[i], y0, 0, m[i]);
+                }
+            } else {
+                for (; j < cend; ++j) {
+                    uint32_t y0[H];
+                    load_entry<H, HP>(lp + j * HP, y0);
+                    const int pcy = (int)__ldg(lpc + j);
+#pragma unroll
+                    for (int i = 0; i < RX; ++i) m[i] = fold_min<H>(x[i], y0, pcy, m[i]);
+                }
+            }
+            bool any = false;
+#pragma unroll
+            for (int i = 0; i < RX; ++i) any |= m[i] < thr[i];
+            if (any) {
+#pragma unroll 1
+                for (int i = 0; i < RX; ++i) {
+                    if (m[i] < thr[i]) {
+                        const unsigned long long e = reg0 + lane + 32 * i;
+                        T = survivor_scan(D, B, regX, xoff, e, pcr[i],
+                                          loop0 + (unsigned long long)c0, cn, T);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < RX; ++i)
+                    thr[i] = T - pcr[i] - (FULL ? (regX ? D.b : D.a) : 0);
+            }
+#pragma unroll
+            for (int i = 0; i < RX; ++i) m[i] = 0x7fffffff;
+        }
+        if (lane == 0) atomicAdd(D.count, reg_cnt * (unsigned long long)loop_cnt);
+    }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------- host launchers
+cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
+                             const unsigned long long* d_binom, int num_sms, cudaStream_t st) {
+    if (total == 0) return cudaSuccess;
+    unsigned long long blocks = (total + 255) / 256;
+    const unsigned long long cap = (unsigned long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    dev::gen_lists_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_descs, ndesc, total, d_binom);
+    return cudaGetLastError();
+}
+
+template <int H, int HP, bool FULL>
+static cudaError_t launch_pairs_t(const LevelDesc* d, int nd, unsigned long long jobs,
+                                  unsigned long long* ctr, const unsigned long long* B,
+                                  int num_sms, cudaStream_t st) {
+    static int blocks_per_sm = 0;
+    if (blocks_per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
+                                                      dev::pairs_kernel<H, HP, FULL>, 128, 0);
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+    }
+    unsigned long long blocks = (unsigned long long)num_sms * blocks_per_sm;
+    const unsigned long long need = (jobs + 3) / 4;   // 4 warps per block
+    if (need < blocks) blocks = need;
+    if (blocks < 1) blocks = 1;
+    dev::pairs_kernel<H, HP, FULL><<<(unsigned)blocks, 128, 0, st>>>(d, nd, jobs, ctr, B);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pairs(int H, int HP, bool full, const LevelDesc* d, int nd,
+                         unsigned long long jobs, unsigned long long* ctr,
+                         const unsigned long long* B, int num_sms, cudaStream_t st) {
+    if (jobs == 0) return cudaSuccess;
+    const int key = (H * 8 + HP) * 2 + (full ? 1 : 0);
+    switch (key) {
+        case (1 * 8 + 1) * 2: return launch_pairs_t<1, 1, false>(d, nd, jobs, ctr, B, num_sms, st);
+        case (1 * 8 + 1) * 2 + 1: return launch_pairs_t<1, 1, true>(d, nd, jobs, ctr, B, num_sms, st);
+        case (2 * 8 + 2) * 2: return launch_pairs_t<2, 2, false>(d, nd, jobs, ctr, B, num_sms, st);
+        case (2 * 8 + 2) * 2 + 1: return launch_pairs_t<2, 2, true>(d, nd, jobs, ctr, B, num_sms, st);
+        case (2 * 8 + 4) * 2: return launch_pairs_t<2, 4, false>(d, nd, jobs, ctr, B, num_sms, st);
+        case (2 * 8 + 4) * 2 + 1: return launch_pairs_t<2, 4, true>(d, nd, jobs, ctr, B, num_sms, st);
+        case (3 * 8 + 4) * 2: return launch_pairs_t<3, 4, false>(d, nd, jobs, ctr, B, num_sms, st);
+        case (3 * 8 + 4) * 2 + 1: return launch_pairs_t<3, 4, true>(d, nd, jobs, ctr, B, num_sms, st);
+        case (4 * 8 + 4) * 2: return launch_pairs_t<4, 4, false>(d, nd, jobs, ctr, B, num_sms, st);
+        case (4 * 8 + 4) * 2 + 1: return launch_pairs_t<4, 4, true>(d, nd, jobs, ctr, B, num_sms, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace qsfb

@@ -1,0 +1,159 @@
+"""Generate the golden vectors under tests/golden/ from the REFERENCE implementation.
+
+Runs only where the reference CPU library has been built from its sources
+(oracle/_ref/libqubitserf.so, see oracle/Makefile).  Outputs:
+
+* golden.npz   -- the input matrices (uint8), keyed by case name
+* golden.json  -- per case: the reference's distance / proven flag, and for the
+                  no-early-stop cases the reference's per-level (w, active, work) trace
+                  read from its DISTFIND_PROFILE lines (cpp/distfind/bz.cpp:193-201)
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import codes as C  # noqa: E402
+from qubitserf_b200 import workloads as W  # noqa: E402
+
+
+def cases():
+    """(name, kind, mats, extra) for every golden case."""
+    out = []
+    out.append(("cfg_classical_96", "classical", (W.single_classical_96(),), {}))
+    out.append(("cfg_classical_128", "classical", (W.single_classical_128(),), {}))
+    out.append(("cfg_css_128", "css", W.single_css_128(), {"which": "M"}))
+    for L in range(3, 7):
+        out.append((f"toric{L}", "css", C.toric(L), {"which": "M"}))
+    for L in range(3, 6):
+        out.append((f"surface{L}", "css", C.surface(L), {"which": "M"}))
+    out.append(("surface7", "css", C.surface(7), {"which": "M"}))
+    out.append(("toric7", "css", C.toric(7), {"which": "M"}))
+    out.append(("steane", "css", C.steane(), {"which": "M"}))
+    out.append(("shor", "css", C.shor(), {"which": "M"}))
+    out.append(("hgp_2x5", "css", C.hypergraph_product(C.repetition_parity(2),
+                                                       C.repetition_parity(5)), {"which": "M"}))
+    out.append(("hgp_3x4", "css", C.hypergraph_product(C.repetition_parity(3),
+                                                       C.repetition_parity(4)), {"which": "M"}))
+    for nm, (Hx, Hz) in (("toric4", C.toric(4)), ("hgp_2x5", C.hypergraph_product(
+            C.repetition_parity(2), C.repetition_parity(5)))):
+        out.append((nm + "_z", "css", (Hx, Hz), {"which": "Z"}))
+        out.append((nm + "_x", "css", (Hx, Hz), {"which": "X"}))
+    for n in range(3, 9):
+        out.append((f"rep{n}", "classical", (C.repetition_parity(n),), {}))
+    out.append(("hamming3", "classical", (C.hamming_parity(3),), {}))
+    out.append(("hamming4", "classical", (C.hamming_parity(4),), {}))
+    out.append(("qrm_1_9", "css", C.quantum_reed_muller(1, 9), {"which": "M"}))
+    out.append(("qrm_1_10", "css", C.quantum_reed_muller(1, 10), {"which": "M"}))
+    out.append(("bacon_shor3", "subsystem", C.bacon_shor(3), {"which": "M"}))
+    out.append(("bacon_shor4", "subsystem", C.bacon_shor(4), {"which": "M"}))
+    out.append(("five_qubit", "stabilizer", (C.five_qubit(),), {"which": "M"}))
+    rng = np.random.default_rng(0x5AB)
+    for i in range(6):
+        n = int(rng.integers(5, 11))
+        S = C.random_isotropic(rng, n, int(rng.integers(2, n)))
+        if S.shape[0]:
+            out.append((f"noncss_{i}", "stabilizer", (S,), {"which": "M"}))
+    rng = np.random.default_rng(0x09E12)
+    for i in range(8):
+        n = int(rng.integers(6, 16))
+        Hx, Hz = C.random_css(rng, n, int(rng.integers(1, max(2, n // 2))))
+        z = rng.integers(0, 2, n, dtype=np.uint8)
+        x = rng.integers(0, 2, n, dtype=np.uint8)
+        out.append((f"opw_{i}", "opweight", (Hx, Hz, z, x), {}))
+    # first codes of the 1024-code batch (both halves)
+    batch = W.batch_1024()
+    for i in list(range(0, 12)) + list(range(512, 524)):
+        cs = batch[i]
+        if cs.kind == "classical":
+            out.append((f"batch_{i}", "classical", cs.mats, {}))
+        else:
+            out.append((f"batch_{i}", "css", cs.mats, {"which": "M"}))
+    return out
+
+
+# Cases re-run with DISTFIND_NO_EARLY_STOP for the per-(information set, w) counts.
+COUNT_CASES = ["rep6", "rep8", "hamming4", "toric4_z", "toric4_x", "hgp_2x5_z", "hgp_2x5_x",
+               "batch_3"]
+COUNT_MAX_K = 24
+
+
+def run_reference(kind, mats, extra):
+    from oracle.refbind import Ref
+    ref = Ref()
+    if kind == "classical":
+        r = ref.classical(mats[0])
+        return {"distance": r.distance, "proven": r.proven}
+    if kind == "css":
+        r = ref.css(mats[0], mats[1], extra.get("which", "M"))
+        return {"distance": r.distance, "proven": r.proven}
+    if kind == "subsystem":
+        r = ref.subsystem(mats[0], mats[1], extra.get("which", "M"))
+        return {"distance": r.distance, "proven": r.proven}
+    if kind == "stabilizer":
+        rc, r = ref.stabilizer(mats[0], extra.get("which", "M"))
+        assert rc == 0
+        return {"distance": r.distance, "proven": r.proven}
+    if kind == "opweight":
+        r = ref.operator_weight(*mats)
+        return {"z_weight": r.z_weight, "x_weight": r.x_weight}
+    raise ValueError(kind)
+
+
+PROF = re.compile(r"\[prof \w+\] d=(\d+) K=(\d+) ng=(\d+)/(\d+) stride=\d+ total=(\d+) work=(\d+)")
+
+
+def count_trace(name):
+    """Run the reference in a child with no early stop + profiling; parse its level lines."""
+    code = (
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {str(ROOT)!r}); sys.path.insert(0, {str(HERE)!r})\n"
+        "import make_golden as M\n"
+        f"c = [c for c in M.cases() if c[0] == {name!r}][0]\n"
+        "M.run_reference(c[1], c[2], c[3])\n"
+    )
+    env = dict(os.environ, DISTFIND_NO_EARLY_STOP="1", DISTFIND_PROFILE="1")
+    p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       check=True)
+    levels = []
+    for m in PROF.finditer(p.stderr):
+        d, K, a, t, total, work = map(int, m.groups())
+        levels.append({"w": d, "K": K, "active": a, "num_sets": t, "total": total,
+                       "work": work})
+    return levels
+
+
+def main():
+    sys.path.insert(0, str(ROOT))
+    arrays = {}
+    results = {}
+    for name, kind, mats, extra in cases():
+        for i, m in enumerate(mats):
+            arrays[f"{name}__{i}"] = np.asarray(m, dtype=np.uint8)
+        res = run_reference(kind, mats, extra)
+        res.update({"kind": kind, "nmats": len(mats), **extra})
+        results[name] = res
+        print(name, res, flush=True)
+    for name in COUNT_CASES:
+        tr = count_trace(name)
+        if tr and max(lv["K"] for lv in tr) <= COUNT_MAX_K:
+            results[name]["no_early_stop_levels"] = tr
+    np.savez_compressed(HERE / "golden.npz", **arrays)
+    (HERE / "golden.json").write_text(json.dumps(results, indent=1, sort_keys=True))
+
+
+if __name__ == "__main__":
+    main()

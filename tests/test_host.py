@@ -1,0 +1,166 @@
+"""Host-side logic of the engine, no GPU needed: the library loads and exports the ABI,
+the host problem reduction reproduces the reference's information sets bit for bit, the
+dispatch rules and error codes, and the workload generators."""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    text = (ROOT / "include" / "qsf_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(distfind_\w+|qsfb_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(native):
+    names = header_functions()
+    assert len(names) >= 15
+    lib = native.lib()
+    for n in names:
+        assert hasattr(lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", str(native.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (\w+)", out))
+    assert set(names) <= exported
+    # every binding in the Python layer points at a declared function
+    assert {s[0] for s in native.SIGNATURES} == set(names)
+
+
+def test_struct_layouts_match_reference_abi(native):
+    # cpp/distfind/capi.h:12-19 and :39-45 (byte compatible with the reference ctypes)
+    assert ctypes.sizeof(native.DistfindResult) == 4 * 4 + 8 + 16
+    assert native.DistfindResult.seconds.offset == 16
+    assert ctypes.sizeof(native.DistfindOpResult) == 3 * 4 + 4 + 8 + 16
+    assert native.DistfindOpResult.seconds.offset == 16
+
+
+def test_version(native):
+    assert native.version() == "0.1.0"
+
+
+def _prep_cases(golden):
+    out = []
+    for name in ["cfg_classical_96", "cfg_classical_128", "hamming4", "rep6", "batch_0",
+                 "batch_5", "batch_11"]:
+        out.append((name, 0, golden.mats(name)))
+    for name in ["cfg_css_128", "toric4", "surface5", "steane", "shor", "hgp_2x5",
+                 "batch_512", "batch_515", "batch_520", "qrm_1_9"]:
+        m = golden.mats(name)
+        out.append((name + "_Z", 1, m))
+        out.append((name + "_X", 2, m))
+    for name in ["bacon_shor3", "bacon_shor4"]:
+        m = golden.mats(name)
+        out.append((name + "_Z", 3, m))
+        out.append((name + "_X", 4, m))
+    for name in ["five_qubit", "noncss_1", "noncss_4"]:
+        out.append((name, 5, golden.mats(name)))
+    return out
+
+
+def test_host_reduction_bit_exact_vs_reference(native, ref, golden):
+    """Information-set generators, ranks, detector, parity and seed bound equal the
+    reference's (cpp/distfind/bz.cpp:141-159) bit for bit."""
+    if ref is None:
+        pytest.skip("reference library not built here")
+    for name, kind, mats in _prep_cases(golden):
+        a = native.prepare_problem(kind, *mats)
+        b = ref.problem_gammas(kind, *mats)
+        for k in ("n", "K", "stride", "ranks", "even", "count_all", "seed_upper"):
+            assert a[k] == b[k], (name, k, a[k], b[k])
+        assert np.array_equal(a["gamma"], b["gamma"]), name
+        assert np.array_equal(a["check"], b["check"]), name
+
+
+def test_host_reduction_matches_oracle(native, orc, golden):
+    for name, kind, mats in _prep_cases(golden):
+        a = native.prepare_problem(kind, *mats)
+        b = orc.prepare(kind, *mats)
+        assert a["ranks"] == b["ranks"] or sorted(a["ranks"]) == sorted(b["ranks"]), name
+        for k in ("n", "K", "even", "count_all", "seed_upper"):
+            assert a[k] == b[k], (name, k)
+
+
+def test_matroid_partition_cases_bit_exact(native, ref):
+    """Classical codes where the greedy peel is suboptimal take the matroid partition
+    (cpp/distfind/css.cpp:417-447); the chosen sets must still agree exactly."""
+    if ref is None:
+        pytest.skip("reference library not built here")
+    from qubitserf_b200.workloads import classical_parity_from_rng
+    rng = np.random.default_rng(11)
+    hit = 0
+    for _ in range(60):
+        n = int(rng.integers(20, 60))
+        k = int(rng.integers(n // 4, n // 2 + 1))
+        H = classical_parity_from_rng(rng, n, k)
+        # sparsify some columns so the greedy peel leaves rank on the table
+        H[:, rng.integers(0, n, n // 5)] = 0
+        a = native.prepare_problem(0, H)
+        b = ref.problem_gammas(0, H)
+        assert a["ranks"] == b["ranks"]
+        assert np.array_equal(a["gamma"], b["gamma"])
+        hit += len(a["ranks"]) > 1
+    assert hit > 10
+
+
+def test_dispatch_rules_without_device(native, golden):
+    """No CPU path: without an sm_100 device every distance call fails with rc 4, and the
+    unsupported methods/backends with rc 5, before touching any device."""
+    lib = native.lib()
+    H = golden.mats("hamming3")[0]
+    a = native.as_u8(H)
+    out = native.DistfindResult()
+    p = a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    assert lib.distfind_classical_distance(p, a.shape[0], a.shape[1], b"mitm", b"gpu", 0, 0,
+                                           ctypes.byref(out)) == 5
+    assert lib.distfind_classical_distance(p, a.shape[0], a.shape[1], b"bz", b"cpu", 0, 0,
+                                           ctypes.byref(out)) == 5
+    assert lib.distfind_classical_distance(None, 1, 1, b"bz", b"gpu", 0, 0,
+                                           ctypes.byref(out)) == 1
+    S = np.zeros((1, 5), np.uint8)
+    assert lib.distfind_stabilizer_distance(
+        S.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), 1, 5, b"bz", b"M", b"gpu", 0, 0,
+        ctypes.byref(out)) == 2
+    if lib.qsfb_device_sms() == 0:
+        assert lib.distfind_backend_available(b"gpu") == 0
+        rc = lib.distfind_classical_distance(p, a.shape[0], a.shape[1], b"bz", b"gpu", 0, 0,
+                                             ctypes.byref(out))
+        assert rc == 4
+        with pytest.raises(RuntimeError):
+            native.classical_distance_raw(H, "bz", "auto", 0, False)
+    assert lib.distfind_backend_available(b"cpu") == 0
+    assert lib.distfind_backend_available(b"metal") == 0
+
+
+def test_api_argument_validation():
+    from qubitserf_b200 import api
+    Hx = np.ones((1, 4), np.uint8)
+    with pytest.raises(ValueError, match="auto/cpu/gpu"):
+        api.css_distance(Hx, Hx, backend="metal")
+    with pytest.raises(ValueError, match="min/z/x"):
+        api.css_distance(Hx, Hx, which="q")
+    with pytest.raises(ValueError):
+        api.stabilizer_distance(np.ones((2, 5), np.uint8))
+    z, x = api.parse_operator("IXYZ", 4)
+    assert list(z) == [0, 0, 1, 1] and list(x) == [0, 1, 1, 0]
+
+
+def test_workloads_are_deterministic():
+    from qubitserf_b200 import workloads as W
+    h = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+    H1 = W.single_classical_96()
+    assert H1.shape == (64, 96) and h(H1) == h(W.single_classical_96())
+    Hx, Hz = W.single_css_128()
+    assert Hx.shape == (40, 128) and Hz.shape == (40, 128)
+    assert not (W.gf2_matmul(Hx, Hz.T)).any()
+    assert W.gf2_rank(Hx) == 40 and W.gf2_rank(Hz) == 40
+    b = W.batch_1024(8)
+    assert [c.kind for c in b] == ["classical"] * 4 + ["css"] * 4

@@ -1,0 +1,124 @@
+"""The C oracle pinned against the reference: golden vectors (made by the reference,
+tests/golden/make_golden.py) and, where oracle/_ref is built, the reference library itself."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+# Golden cases too slow for the single-threaded oracle inside the CPU suite.
+SLOW = {"cfg_css_128", "qrm_1_10", "toric7", "surface7", "cfg_classical_128"}
+
+
+def _oracle_result(orc, kind, mats, extra, **kw):
+    if kind == "classical":
+        return orc.classical(mats[0], **kw)
+    if kind == "css":
+        return orc.css(mats[0], mats[1], extra.get("which", "M"), **kw)
+    if kind == "subsystem":
+        return orc.subsystem(mats[0], mats[1], extra.get("which", "M"), **kw)
+    if kind == "stabilizer":
+        return orc.stabilizer(mats[0], extra.get("which", "M"), **kw)
+    raise ValueError(kind)
+
+
+def test_oracle_matches_golden_distances(golden, orc):
+    bad = []
+    for name, res in golden.results.items():
+        if name in SLOW:
+            continue
+        mats = golden.mats(name)
+        if res["kind"] == "opweight":
+            got = orc.operator_weight(*mats)
+            if got != (res["z_weight"], res["x_weight"]):
+                bad.append((name, got, res))
+            continue
+        r = _oracle_result(orc, res["kind"], mats, res)
+        if r.distance != res["distance"] or r.proven != res["proven"]:
+            bad.append((name, r.distance, res["distance"]))
+    assert not bad, bad
+
+
+def test_oracle_no_early_stop_counts_match_reference(golden, orc):
+    """Per-level (w, active, C(K,w)*active) work with early termination disabled."""
+    seen = 0
+    for name, res in golden.results.items():
+        lv = res.get("no_early_stop_levels")
+        if not lv:
+            continue
+        mats = golden.mats(name)
+        r = _oracle_result(orc, res["kind"], mats, res, no_early_stop=True, trace_cap=256)
+        got = [(w, a) for (_side, w, a) in r.trace]
+        want = [(x["w"], x["active"]) for x in lv]
+        assert got == want, (name, got, want)
+        assert r.codewords == sum(x["work"] for x in lv), name
+        assert r.proven == 0
+        seen += 1
+    assert seen >= 5
+
+
+def _random_plan(rng, K, stride, d, ng, kcheck):
+    gamma = rng.integers(0, 2**63, (ng, K, stride), dtype=np.uint64)
+    check = rng.integers(0, 2**63, (kcheck, stride), dtype=np.uint64)
+    return gamma, check
+
+
+def test_oracle_enumerate_brute_vs_two_level(orc):
+    """The brute-force level (eval_combo order) and the two-level kernel agree."""
+    rng = np.random.default_rng(0xC0FFEE)
+    for _ in range(80):
+        K = int(rng.integers(4, 15))
+        stride = int(rng.integers(1, 4))
+        d = int(rng.integers(1, min(K, 5) + 1))
+        ng, kc = int(rng.integers(1, 4)), int(rng.integers(0, 4))
+        g, c = _random_plan(rng, K, stride, d, ng, kc)
+        cb = int(rng.choice([1 << 30, int(rng.integers(0, stride * 64 + 1))]))
+        a = orc.enumerate(stride * 64, K, d, g, c, cb)[0]
+        b = orc.enumerate_fast(stride * 64, K, d, g, c, cb)
+        assert a == b, (K, stride, d, ng, kc, cb, a, b)
+
+
+def test_oracle_enumerate_matches_reference_backend(orc, ref):
+    """cpu_enum_ref-style randomized plans (cpp/distfind/tests/cpu_enum_ref.cpp:78-133)
+    against the reference CPU backend itself, single- and multi-threaded."""
+    if ref is None:
+        pytest.skip("reference library not built here")
+    rng = np.random.default_rng(0xC0FFEE)
+    cases = []
+    for _ in range(50):
+        cases.append((int(rng.integers(4, 15)), int(rng.integers(1, 4)), int(rng.integers(1, 6)),
+                      int(rng.integers(1, 4)), int(rng.integers(0, 4)), 0))
+    cases += [(8, 1, 1, 1, 0, 0), (6, 2, 1, 2, 2, 0), (5, 1, 5, 1, 1, 0), (7, 2, 4, 2, 0, 0)]
+    for T in (2, 3, 8, 16):
+        cases += [(18, 2, 5, 2, 2, T), (16, 3, 6, 1, 1, T)]
+    for K, st, d, ng, kc, T in cases:
+        d = max(1, min(d, K))
+        g, c = _random_plan(rng, K, st, d, ng, kc)
+        for cb in (1 << 30, int(rng.integers(0, st * 64 + 1)), 0, 1):
+            want = ref.enumerate(st * 64, st, K, d, g, c, cb, threads=T)
+            got = orc.enumerate(st * 64, K, d, g, c, cb)[0]
+            assert got == want, (K, st, d, ng, kc, cb, got, want)
+
+
+def test_oracle_random_batch_codes_match_reference(orc, ref):
+    if ref is None:
+        pytest.skip("reference library not built here")
+    from qubitserf_b200 import workloads as W
+    codes = W.batch_1024(24)
+    for i, cs in enumerate(codes):
+        if cs.kind == "classical":
+            assert orc.classical(cs.mats[0]).distance == ref.classical(cs.mats[0]).distance, i
+        elif cs.n <= 80:
+            assert orc.css(*cs.mats).distance == ref.css(*cs.mats).distance, i
+
+
+def test_oracle_problem_ranks_match_reference(orc, ref, golden):
+    if ref is None:
+        pytest.skip("reference library not built here")
+    for name in ["cfg_classical_96", "cfg_classical_128", "toric5", "surface5", "hamming4",
+                 "batch_0", "batch_1", "batch_515"]:
+        mats = golden.mats(name)
+        kind = 0 if golden.results[name]["kind"] == "classical" else 1
+        a = orc.prepare(kind, *mats)
+        b = ref.problem_gammas(kind, *mats)
+        assert a["ranks"] == b["ranks"] and a["K"] == b["K"], name
+        assert a["seed_upper"] == b["seed_upper"] and a["even"] == b["even"], name
