@@ -142,6 +142,61 @@ int qsfb_last_witness(uint8_t* out, int cap);
  * number of records (written up to cap). */
 int qsfb_last_counts(int* side, int* w, int* g, unsigned long long* count, int cap);
 
+/* ---- batched engine: many queries certified together (no reference counterpart; the
+ * reference loops its per-code entry points).  Every query's levels of one round run in
+ * one list-generation launch plus one pair-sweep launch per kernel variant; host setup is
+ * spread over host_threads (0 = all cores).  Results equal the per-query entry points'. */
+typedef struct {
+    int kind;               /* 0 classical (A = H); 1 CSS distance (A = Hx, B = Hz);
+                               2 CSS operator weight (A = Gx, B = Gz, z_op, x_op) */
+    char which;             /* kind 1: 'Z', 'X' or 'M' (interleaved min) */
+    const uint8_t* A;
+    int a_rows, a_cols;
+    const uint8_t* B;
+    int b_rows, b_cols;
+    const uint8_t* z_op;    /* kind 2: length a_cols */
+    const uint8_t* x_op;
+} QsfbQuery;
+
+typedef struct {
+    int distance;           /* kinds 0/1: distance (-1 undefined); kind 2: max(z, x) */
+    int z_weight, x_weight; /* kind 2 */
+    int lower_bound;
+    int proven;
+    int levels;
+    int witness_ok;         /* 1: every certificate's witness verified on the host */
+} QsfbAnswer;
+
+typedef struct {
+    double seconds;              /* wall time of the call */
+    double host_setup_seconds;   /* problem reduction + information sets + seed bounds */
+    double device_ms;            /* list generation + pair sweeps (sum of kernel time) */
+    double device_span_ms;       /* CUDA-event span of all rounds, host gaps included */
+    double pair_ms;              /* pair-sweep kernel time alone */
+    unsigned long long codewords;
+    int rounds;
+    int kernel_launches;
+    int certificates;            /* BZ runs executed (a CSS 'M' query is one) */
+} QsfbBatchStats;
+
+/* One-shot: prepare + execute + free. */
+int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
+               QsfbBatchStats* stats);
+
+/* Two-phase form: prepare does the host reduction, information sets and seed bounds of
+ * every query and leaves the packed rows resident on the device; execute runs (or re-runs
+ * from the post-prepare state) all BZ rounds and fills out[nq]; free releases everything.
+ * A handle is used by one thread at a time. */
+typedef struct QsfbBatchHandle QsfbBatchHandle;
+int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
+                       QsfbBatchHandle** handle);
+int qsfb_batch_execute(QsfbBatchHandle* handle, QsfbAnswer* out, QsfbBatchStats* stats);
+void qsfb_batch_free(QsfbBatchHandle* handle);
+
+/* Overwrite a 256 MiB device buffer (more than the 126 MB L2) and wait; benchmarks call it
+ * between timed steps.  Returns 0, or 4 without a device. */
+int qsfb_flush_l2(void);
+
 /* Name of the device in use ("" without one) and its SM count. */
 const char* qsfb_device_name(void);
 int qsfb_device_sms(void);

@@ -49,6 +49,29 @@ class QsfbReport(ctypes.Structure):
                 ("codewords", ctypes.c_ulonglong)]
 
 
+class QsfbQuery(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("which", ctypes.c_char),
+                ("A", ctypes.POINTER(ctypes.c_uint8)), ("a_rows", ctypes.c_int),
+                ("a_cols", ctypes.c_int), ("B", ctypes.POINTER(ctypes.c_uint8)),
+                ("b_rows", ctypes.c_int), ("b_cols", ctypes.c_int),
+                ("z_op", ctypes.POINTER(ctypes.c_uint8)), ("x_op", ctypes.POINTER(ctypes.c_uint8))]
+
+
+class QsfbAnswer(ctypes.Structure):
+    _fields_ = [("distance", ctypes.c_int), ("z_weight", ctypes.c_int),
+                ("x_weight", ctypes.c_int), ("lower_bound", ctypes.c_int),
+                ("proven", ctypes.c_int), ("levels", ctypes.c_int),
+                ("witness_ok", ctypes.c_int)]
+
+
+class QsfbBatchStats(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("host_setup_seconds", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("device_span_ms", ctypes.c_double),
+                ("pair_ms", ctypes.c_double), ("codewords", ctypes.c_ulonglong),
+                ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),
+                ("certificates", ctypes.c_int)]
+
+
 # (name, restype, argtypes) of every exported function; tests check the export list.
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -74,6 +97,14 @@ SIGNATURES = [
     ("qsfb_last_report", _i, [ctypes.POINTER(QsfbReport)]),
     ("qsfb_last_witness", _i, [_u8p, _i]),
     ("qsfb_last_counts", _i, [_ip, _ip, _ip, _ullp, _i]),
+    ("qsfb_batch", _i, [ctypes.POINTER(QsfbQuery), _i, _i, ctypes.POINTER(QsfbAnswer),
+                        ctypes.POINTER(QsfbBatchStats)]),
+    ("qsfb_batch_prepare", _i, [ctypes.POINTER(QsfbQuery), _i, _i,
+                                ctypes.POINTER(ctypes.c_void_p)]),
+    ("qsfb_batch_execute", _i, [ctypes.c_void_p, ctypes.POINTER(QsfbAnswer),
+                                ctypes.POINTER(QsfbBatchStats)]),
+    ("qsfb_batch_free", None, [ctypes.c_void_p]),
+    ("qsfb_flush_l2", _i, []),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
 ]
@@ -283,3 +314,76 @@ def last_counts():
     cnt = (ctypes.c_ulonglong * max(n, 1))()
     lib().qsfb_last_counts(side, w, g, cnt, n)
     return [(side[i], w[i], g[i], int(cnt[i])) for i in range(n)]
+
+
+class Batch:
+    """Queries prepared once (contiguous uint8 host matrices) and certified together with
+    qsfb_batch.  Each item: ("classical", H) | ("css", Hx, Hz[, which]) |
+    ("opweight", Gx, Gz, z, x)."""
+
+    KINDS = {"classical": 0, "css": 1, "opweight": 2}
+
+    def __init__(self, items):
+        self._keep = []
+        self.n = len(items)
+        self.q = (QsfbQuery * max(1, self.n))()
+        self.host_bytes = 0
+        for i, it in enumerate(items):
+            kind = it[0]
+            Q = self.q[i]
+            Q.kind = self.KINDS[kind]
+            A = as_u8(it[1])
+            self._keep.append(A)
+            Q.A, Q.a_rows, Q.a_cols = _p(A), A.shape[0], A.shape[1]
+            self.host_bytes += A.size
+            Q.which = b"M"
+            if kind in ("css", "opweight"):
+                B = as_u8(it[2])
+                self._keep.append(B)
+                Q.B, Q.b_rows, Q.b_cols = _p(B), B.shape[0], B.shape[1]
+                self.host_bytes += B.size
+            if kind == "css" and len(it) > 3:
+                Q.which = it[3].encode()[:1]
+            if kind == "opweight":
+                z, x = as_u8_vec(it[3]), as_u8_vec(it[4])
+                self._keep += [z, x]
+                Q.z_op, Q.x_op = _p(z), _p(x)
+                self.host_bytes += z.size + x.size
+        self.out = (QsfbAnswer * max(1, self.n))()
+
+    def run(self, host_threads=0):
+        """One-shot certification from the host matrices (prepare + execute + free)."""
+        st = QsfbBatchStats()
+        rc = lib().qsfb_batch(self.q, self.n, int(host_threads), self.out, ctypes.byref(st))
+        _check(rc, "qsfb_batch")
+        return [self.out[i] for i in range(self.n)], st
+
+    def prepare(self, host_threads=0):
+        """Host setup + upload; returns a handle for execute()/free()."""
+        h = ctypes.c_void_p()
+        rc = lib().qsfb_batch_prepare(self.q, self.n, int(host_threads), ctypes.byref(h))
+        _check(rc, "qsfb_batch_prepare")
+        return h
+
+    def execute(self, handle):
+        st = QsfbBatchStats()
+        rc = lib().qsfb_batch_execute(handle, self.out, ctypes.byref(st))
+        _check(rc, "qsfb_batch_execute")
+        return [self.out[i] for i in range(self.n)], st
+
+    @staticmethod
+    def free(handle):
+        lib().qsfb_batch_free(handle)
+
+
+def batch_items(codes):
+    """workloads.CodeSpec list -> Batch items (CSS codes with which='min')."""
+    items = []
+    for cs in codes:
+        if cs.kind == "classical":
+            items.append(("classical", cs.mats[0]))
+        elif cs.kind == "css":
+            items.append(("css", cs.mats[0], cs.mats[1], "M"))
+        else:
+            items.append(("opweight",) + tuple(cs.mats))
+    return items

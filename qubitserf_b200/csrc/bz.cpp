@@ -1,10 +1,11 @@
 // BZ schedule on the device engine.  Bounds, termination, verbose lines and the Z/X
-// interleave keep the reference's semantics line for line (cpp/distfind/bz.cpp:118-403,
+// interleave keep the reference's semantics (cpp/distfind/bz.cpp:118-403,
 // cpp/distfind/progress.hpp:12-33) so that distance, lower_bound, proven and levels agree
 // with the reference run on the same host; the enumeration itself runs on the GPU.
 #include "bz.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -14,13 +15,12 @@
 
 namespace qsfb {
 
-namespace {
-
-using clk = std::chrono::steady_clock;
-
-double since(clk::time_point t) {
-    return std::chrono::duration<double>(clk::now() - t).count();
+double now_seconds() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
+
+namespace {
 
 void fprint_elapsed(double secs) {
     if (secs < 1.0) std::fprintf(stderr, "Elapsed:[%dms]\n", (int)(secs * 1000.0 + 0.5));
@@ -37,17 +37,15 @@ void verbose_final(int d, double secs, const char* tag) {
     fprint_elapsed(secs);
 }
 
-bool env_flag(const char* name) { return std::getenv(name) != nullptr; }
-
 }  // namespace
 
 // ------------------------------------------------------------------ seed
-int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, int /*threads*/,
+int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, bool parallel,
                    std::vector<u64>* word) {
     const int n = p.n;
     const int K = p.code_gen.rows;
     const int stride = p.code_gen.stride;
-    if (K == 0) return init_best;
+    if (K == 0 || trials <= 0) return init_best;
     int nth = (int)std::thread::hardware_concurrency();
     if (nth < 1) nth = 1;
     if (nth > trials) nth = trials;
@@ -76,19 +74,19 @@ int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, i
         }
         return o;
     };
-    std::vector<Out> res;
-    if (nth == 1) {
-        res.push_back(run(0, trials, seed));
+    std::vector<Out> res(nth);
+    auto chunk = [&](int t) {
+        const int lo = (int)((long)trials * t / nth);
+        const int hi = (int)((long)trials * (t + 1) / nth);
+        // one stream: the reference's single-thread case uses `seed` itself
+        const unsigned ts = nth == 1 ? seed : seed + 0x9e3779b9u * (unsigned)(t + 1);
+        res[t] = run(lo, hi, ts);
+    };
+    if (!parallel || nth == 1) {
+        for (int t = 0; t < nth; ++t) chunk(t);
     } else {
-        res.resize(nth);
         std::vector<std::thread> pool;
-        for (int t = 0; t < nth; ++t) {
-            const int lo = (int)((long)trials * t / nth);
-            const int hi = (int)((long)trials * (t + 1) / nth);
-            pool.emplace_back([&, t, lo, hi]() {
-                res[t] = run(lo, hi, seed + 0x9e3779b9u * (unsigned)(t + 1));
-            });
-        }
+        for (int t = 0; t < nth; ++t) pool.emplace_back(chunk, t);
         for (auto& th : pool) th.join();
     }
     int best = init_best;
@@ -101,13 +99,13 @@ int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, i
 }
 
 // ------------------------------------------------------------------ side
-int BzSide::setup(Device* d, Session* s, const Problem& p, const BzOptions& opt, const char* t) {
+int BzSide::setup_host(const Problem& p, const BzOptions& opt, const char* t) {
     tag = t;
     prob = &p;
     K = p.code_gen.rows;
     even = p.even;
     has_logicals = !(K == 0 || (!p.count_all && p.check.rows == 0));
-    if (!has_logicals) { resolved = true; return kOk; }
+    if (!has_logicals) { resolved = resolved0 = true; return kOk; }
     sets = information_sets(p.code_gen);
     ng = (int)sets.size();
     ranks.resize(ng);
@@ -115,10 +113,23 @@ int BzSide::setup(Device* d, Session* s, const Problem& p, const BzOptions& opt,
     inner = p.seed_upper > 0 ? p.seed_upper : kWeightNone;
     if (p.seed_upper > 0) best_word = p.seed_word;
     std::vector<u64> w;
-    const int seeded = random_is_seed(p, inner, opt.seed_trials, 0x9e3779b9u, opt.threads, &w);
+    const int seeded = random_is_seed(p, inner, opt.seed_trials, 0x9e3779b9u, opt.parallel_seed, &w);
     if (seeded < inner) { inner = seeded; best_word = w; }
     maxw = K;
-    return dev.init(d, s, p, sets);
+    inner0 = inner;
+    resolved0 = resolved;
+    return dev.prepare(p, sets);
+}
+
+void BzSide::reset() {
+    inner = inner0;
+    resolved = resolved0;
+    outer = 0;
+    level = 0;
+    proven = false;
+    best_from_level = false;
+    best_g = -1;
+    for (auto& kv : dev.lists) kv.second.ready = false;
 }
 
 int BzSide::active_at(int w) const {
@@ -153,7 +164,7 @@ bool BzSide::witness(std::vector<u64>& out) const {
         return !out.empty();
     }
     if (best_shift != 0 || best_g < 0 || best_g >= ng) return false;
-    // Unrank the lexicographic rank (cpp/qsf/combinatorics.hpp:52-61 order).
+    // Unrank the lexicographic rank (the order of cpp/qsf/combinatorics.hpp:52-61).
     std::vector<std::vector<unsigned long long>> C(K + 1, std::vector<unsigned long long>(best_w + 1, 0));
     for (int n = 0; n <= K; ++n) {
         C[n][0] = 1;
@@ -182,27 +193,128 @@ bool BzSide::witness(std::vector<u64>& out) const {
     return true;
 }
 
-// ------------------------------------------------------------------ drivers
-namespace {
+// ------------------------------------------------------------------ job
+BzJob::BzJob(Problem p0, const BzOptions& o) : pair(false), opt(o) { p[0] = std::move(p0); }
 
-int run_one(Session* s, BzSide& S, int w, LevelOut& o, BzResult& r, int side_idx) {
-    std::vector<LevelReq> q(1);
-    q[0].side = &S.dev;
-    q[0].w = w;
-    q[0].active = S.active_at(w);
-    q[0].bound = S.inner;
-    std::vector<LevelOut> outs;
-    if (q[0].active == 0) {
-        o = LevelOut();
-    } else {
-        const int rc = run_levels(s, q, outs, &r.stats);
+BzJob::BzJob(Problem pz, Problem px, const BzOptions& o) : pair(true), opt(o) {
+    p[0] = std::move(pz);
+    p[1] = std::move(px);
+}
+
+int BzJob::setup_host() {
+    t0_ = tl_ = now_seconds();
+    const int nsides = pair ? 2 : 1;
+    for (int i = 0; i < nsides; ++i) {
+        const int rc = s[i].setup_host(p[i], opt, pair ? (i == 0 ? "Z" : "X") : "");
         if (rc != kOk) return rc;
-        o = outs[0];
     }
-    r.trace.push_back({side_idx, w, q[0].active, o.counts});
+    if (!pair) {
+        done_ = !s[0].has_logicals;
+        maxw_ = s[0].maxw;
+        no_stop_ = opt.no_early_stop || std::getenv("DISTFIND_NO_EARLY_STOP") != nullptr;
+    } else {
+        for (int i = 0; i < 2; ++i)
+            if (s[i].has_logicals) {
+                best_ = std::min(best_, s[i].inner);
+                maxw_ = std::max(maxw_, s[i].maxw);
+            }
+        done_ = s[0].resolved && s[1].resolved;
+    }
     return kOk;
 }
 
+void BzJob::reset() {
+    for (int i = 0; i < (pair ? 2 : 1); ++i) s[i].reset();
+    w_ = 0;
+    stats = RunStats();
+    trace.clear();
+    t0_ = tl_ = now_seconds();
+    if (!pair) {
+        done_ = !s[0].has_logicals;
+    } else {
+        best_ = kWeightNone;
+        for (int i = 0; i < 2; ++i)
+            if (s[i].has_logicals) best_ = std::min(best_, s[i].inner);
+        done_ = s[0].resolved && s[1].resolved;
+    }
+}
+
+std::vector<SideDev*> BzJob::device_sides() {
+    std::vector<SideDev*> v;
+    for (int i = 0; i < (pair ? 2 : 1); ++i)
+        if (s[i].has_logicals) v.push_back(&s[i].dev);
+    return v;
+}
+
+void BzJob::requests(std::vector<LevelReq>& q, std::vector<int>& side) {
+    if (done_) return;
+    const int w = w_ + 1;
+    for (int i = 0; i < (pair ? 2 : 1); ++i) {
+        BzSide& S = s[i];
+        if (pair && (S.resolved || w > S.maxw || S.outer >= best_)) continue;
+        const int active = S.active_at(w);
+        if (active == 0) continue;
+        LevelReq r;
+        r.side = &S.dev;
+        r.w = w;
+        r.active = active;
+        // candidates must beat the side's upper bound strictly; ties among new finds stay
+        // inside the level so that its witness is deterministic
+        r.bound = S.inner >= kWeightNone ? kWeightNone : S.inner - 1;
+        q.push_back(r);
+        side.push_back(i);
+    }
+}
+
+void BzJob::apply(const std::vector<const LevelOut*>& outs, const std::vector<int>& side) {
+    if (done_) return;
+    const int w = ++w_;
+    const double now = now_seconds();
+    auto out_for = [&](int i) -> LevelOut {
+        for (size_t k = 0; k < side.size(); ++k)
+            if (side[k] == i) return *outs[k];
+        return LevelOut();
+    };
+    auto record = [&](int i, const LevelOut& o) {
+        trace.push_back({i, w, s[i].active_at(w), o.counts});
+    };
+    if (!pair) {
+        BzSide& S = s[0];
+        const LevelOut o = out_for(0);
+        S.absorb(w, o);
+        record(0, o);
+        if (S.inner <= S.outer && !no_stop_) {
+            S.proven = true;
+            done_ = true;
+            if (opt.verbose) verbose_final(S.inner, now - t0_, "");
+        } else if (opt.verbose) {
+            verbose_bound(std::max(0, S.outer - 1), now - tl_, "");
+        }
+        if (w >= maxw_) done_ = true;
+    } else {
+        for (int i = 0; i < 2; ++i) {
+            BzSide& S = s[i];
+            if (S.resolved || w > S.maxw) continue;
+            if (S.outer >= best_) { S.resolved = true; continue; }
+            const LevelOut o = out_for(i);
+            S.absorb(w, o);
+            record(i, o);
+            best_ = std::min(best_, S.inner);
+            if (S.inner <= S.outer) {
+                S.proven = true;
+                S.resolved = true;
+                if (opt.verbose) verbose_final(S.inner, now - t0_, S.tag);
+            } else {
+                if (opt.verbose) verbose_bound(std::max(0, S.outer - 1), now - tl_, S.tag);
+                if (S.outer >= best_) S.resolved = true;
+            }
+        }
+        if ((s[0].resolved && s[1].resolved) || w >= maxw_) done_ = true;
+    }
+    tl_ = now;
+}
+
+namespace {
 void finish_witness(const BzSide& S, const Problem& p, BzResult& r, int side_idx) {
     std::vector<u64> c;
     r.witness_side = side_idx;
@@ -211,97 +323,170 @@ void finish_witness(const BzSide& S, const Problem& p, BzResult& r, int side_idx
         r.witness_ok = verify_witness(p, c.data(), r.distance);
     }
 }
-
 }  // namespace
 
-int bz_distance(Device* dev, const Problem& p, const BzOptions& opt, BzResult& r) {
-    const auto t0 = clk::now();
-    r = BzResult();
-    const int K = p.code_gen.rows;
-    if (K == 0 || (!p.count_all && p.check.rows == 0)) {
-        r.distance = -1;
-        r.seconds = since(t0);
-        return kOk;
+BzResult BzJob::result() {
+    BzResult r;
+    r.stats = stats;
+    r.trace = trace;
+    r.seconds = now_seconds() - t0_;
+    if (!pair) {
+        const BzSide& S = s[0];
+        if (!S.has_logicals) return r;
+        r.distance = S.inner >= kWeightNone ? -1 : S.inner;
+        r.levels = S.level;
+        r.lower_bound = S.outer;
+        r.proven = S.proven;
+        finish_witness(S, p[0], r, 0);
+        return r;
     }
+    auto v = [](const BzSide& S) { return S.has_logicals ? S.inner : kWeightNone; };
+    const int dist = std::min(v(s[0]), v(s[1]));
+    r.distance = dist >= kWeightNone ? -1 : dist;
+    const int lb = std::min(s[0].has_logicals ? s[0].outer : kWeightNone,
+                            s[1].has_logicals ? s[1].outer : kWeightNone);
+    r.lower_bound = lb >= kWeightNone ? 0 : lb;
+    r.levels = std::max(s[0].level, s[1].level);
+    r.proven = s[0].resolved && s[1].resolved && dist < kWeightNone;
+    if (r.distance >= 0) {
+        if (v(s[0]) <= v(s[1])) finish_witness(s[0], p[0], r, 0);
+        else finish_witness(s[1], p[1], r, 1);
+    }
+    return r;
+}
+
+// ------------------------------------------------------------------ rounds
+int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
+               int host_threads, RunStats* stats) {
+    const double th0 = now_seconds();
+    int nth = host_threads > 0 ? host_threads : (int)std::thread::hardware_concurrency();
+    nth = std::max(1, std::min<int>(nth, (int)jobs.size()));
+    std::atomic<size_t> next{0};
+    std::atomic<int> err{kOk};
+    auto worker = [&]() {
+        for (;;) {
+            const size_t i = next.fetch_add(1);
+            if (i >= jobs.size()) break;
+            const int rc = jobs[i]->setup_host();
+            if (rc != kOk) err.store(rc);
+        }
+    };
+    if (nth == 1) {
+        worker();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nth; ++t) pool.emplace_back(worker);
+        for (auto& th : pool) th.join();
+    }
+    if (err.load() != kOk) return err.load();
+    if (stats) stats->host_setup_s += now_seconds() - th0;
+    std::vector<SideDev*> sides;
+    for (BzJob* j : jobs)
+        for (SideDev* sd : j->device_sides()) sides.push_back(sd);
+    return upload_sides(dev, s, arena, sides);
+}
+
+int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* rounds,
+               double* span_ms) {
+    int nround = 0;
+    std::vector<LevelReq> q;
+    std::vector<int> side, owner;
+    std::vector<LevelOut> outs;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (span_ms) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s->stream);
+    }
+    int rc = kOk;
+    for (;;) {
+        bool any = false;
+        q.clear(); side.clear(); owner.clear();
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            if (jobs[j]->done()) continue;
+            any = true;
+            const size_t before = q.size();
+            jobs[j]->requests(q, side);
+            for (size_t k = before; k < q.size(); ++k) owner.push_back((int)j);
+        }
+        if (!any) break;
+        ++nround;
+        RunStats rs;
+        outs.clear();
+        if (!q.empty()) {
+            rc = run_levels(s, q, outs, &rs);
+            if (rc != kOk) break;
+        }
+        // per-job slices (requests of one job are contiguous)
+        size_t k = 0;
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            if (jobs[j]->done()) continue;
+            std::vector<const LevelOut*> o;
+            std::vector<int> sd;
+            unsigned long long cw = 0;
+            while (k < q.size() && owner[k] == (int)j) {
+                o.push_back(&outs[k]);
+                sd.push_back(side[k]);
+                for (unsigned long long c : outs[k].counts) cw += c;
+                ++k;
+            }
+            jobs[j]->stats.codewords += cw;
+            jobs[j]->apply(o, sd);
+        }
+        if (stats) {
+            stats->ms_gen += rs.ms_gen;
+            stats->ms_pairs += rs.ms_pairs;
+            stats->jobs += rs.jobs;
+            stats->codewords += rs.codewords;
+            stats->launches += rs.launches;
+        }
+        if (jobs.size() == 1) {
+            // a single job owns the whole device time of its rounds
+            jobs[0]->stats.ms_gen += rs.ms_gen;
+            jobs[0]->stats.ms_pairs += rs.ms_pairs;
+            jobs[0]->stats.launches += rs.launches;
+            jobs[0]->stats.jobs += rs.jobs;
+        }
+    }
+    if (span_ms) {
+        cudaEventRecord(e1, s->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        *span_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (rounds) *rounds = nround;
+    return rc;
+}
+
+int run_jobs(Device* dev, std::vector<BzJob*>& jobs, int host_threads, RunStats* stats,
+             int* rounds) {
     SessionLease lease(dev);
     if (!lease.s) return kErrDevice;
-    BzSide S;
-    int rc = S.setup(dev, lease.s, p, opt, "");
+    Arena arena(dev);
+    int rc = setup_jobs(dev, lease.s, &arena, jobs, host_threads, stats);
     if (rc != kOk) return rc;
-    const bool no_stop = opt.no_early_stop || env_flag("DISTFIND_NO_EARLY_STOP");
-    for (int w = 1; w <= S.maxw; ++w) {
-        const auto te0 = clk::now();
-        LevelOut o;
-        rc = run_one(lease.s, S, w, o, r, 0);
-        if (rc != kOk) return rc;
-        S.absorb(w, o);
-        if (S.inner <= S.outer && !no_stop) {
-            S.proven = true;
-            if (opt.verbose) verbose_final(S.inner, since(t0), "");
-            break;
-        }
-        if (opt.verbose) verbose_bound(std::max(0, S.outer - 1), since(te0), "");
-    }
-    r.distance = S.inner >= kWeightNone ? -1 : S.inner;
-    r.levels = S.level;
-    r.lower_bound = S.outer;
-    r.proven = S.proven;
-    finish_witness(S, p, r, 0);
-    r.seconds = since(t0);
+    return run_rounds(lease.s, jobs, stats, rounds);
+}
+
+int bz_distance(Device* dev, const Problem& p, const BzOptions& opt, BzResult& r) {
+    BzJob job(p, opt);
+    std::vector<BzJob*> jobs{&job};
+    const int rc = run_jobs(dev, jobs, 1, nullptr);
+    if (rc != kOk) return rc;
+    r = job.result();
     return kOk;
 }
 
 int bz_min_interleaved(Device* dev, const Problem& pz, const Problem& px, const BzOptions& opt,
                        BzResult& r) {
-    const auto t0 = clk::now();
-    r = BzResult();
-    SessionLease lease(dev);
-    if (!lease.s) return kErrDevice;
-    BzSide Z, X;
-    int rc = Z.setup(dev, lease.s, pz, opt, "Z");
+    BzJob job(pz, px, opt);
+    std::vector<BzJob*> jobs{&job};
+    const int rc = run_jobs(dev, jobs, 1, nullptr);
     if (rc != kOk) return rc;
-    rc = X.setup(dev, lease.s, px, opt, "X");
-    if (rc != kOk) return rc;
-    BzSide* sides[2] = {&Z, &X};
-    int best = kWeightNone;
-    if (Z.has_logicals) best = std::min(best, Z.inner);
-    if (X.has_logicals) best = std::min(best, X.inner);
-    const int maxw = std::max(Z.has_logicals ? Z.maxw : 0, X.has_logicals ? X.maxw : 0);
-    for (int w = 1; w <= maxw; ++w) {
-        for (int si = 0; si < 2; ++si) {
-            BzSide* S = sides[si];
-            if (S->resolved) continue;
-            if (w > S->maxw) continue;
-            if (S->outer >= best) { S->resolved = true; continue; }
-            const auto te0 = clk::now();
-            LevelOut o;
-            rc = run_one(lease.s, *S, w, o, r, si);
-            if (rc != kOk) return rc;
-            S->absorb(w, o);
-            best = std::min(best, S->inner);
-            if (S->inner <= S->outer) {
-                S->proven = true;
-                S->resolved = true;
-                if (opt.verbose) verbose_final(S->inner, since(t0), S->tag);
-            } else {
-                if (opt.verbose) verbose_bound(std::max(0, S->outer - 1), since(te0), S->tag);
-                if (S->outer >= best) S->resolved = true;
-            }
-        }
-        if (Z.resolved && X.resolved) break;
-    }
-    auto v = [](const BzSide& S) { return S.has_logicals ? S.inner : kWeightNone; };
-    const int dist = std::min(v(Z), v(X));
-    r.distance = dist >= kWeightNone ? -1 : dist;
-    const int lb = std::min(Z.has_logicals ? Z.outer : kWeightNone, X.has_logicals ? X.outer : kWeightNone);
-    r.lower_bound = lb >= kWeightNone ? 0 : lb;
-    r.levels = std::max(Z.level, X.level);
-    r.proven = Z.resolved && X.resolved && dist < kWeightNone;
-    if (r.distance >= 0) {
-        if (v(Z) <= v(X)) finish_witness(Z, pz, r, 0);
-        else finish_witness(X, px, r, 1);
-    }
-    r.seconds = since(t0);
+    r = job.result();
     return kOk;
 }
 

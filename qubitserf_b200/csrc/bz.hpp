@@ -1,9 +1,18 @@
-// Brouwer-Zimmermann schedule on the device engine: information sets, the random
-// information-set upper bound, the weight-level loop with the BZ lower bound
-//   outer(w) = sum_g max(0, (w+1) - (K - rank_g))   (+1 if odd and every codeword is even)
-// and the early stop inner <= outer (reference cpp/distfind/bz.cpp:118-228), the Z/X
-// interleave with the cap-to-min (cpp/distfind/bz.cpp:242-403), and witness tracking.
+// Brouwer-Zimmermann schedule on the device engine.
+//
+// A BzJob is one certificate: a single subproblem (classical, one CSS side, a coset, the
+// non-CSS isometry) or an interleaved Z/X pair (CSS which='min').  Jobs are stepped one
+// weight level per ROUND; every unresolved job of a round contributes its level to ONE
+// run_levels() call, so a single code (the plain drop-in) and a batch of a thousand codes
+// run through the same code path.  Bounds, termination and the Z/X cap keep the
+// reference's semantics (cpp/distfind/bz.cpp:118-403):
+//   outer(w) = sum_g max(0, (w+1) - (K - rank_g))  (+1 if odd and every codeword is even)
+//   stop when inner <= outer; a pair side is capped once its outer reaches the best found.
+// In a pair both sides' level w run in the same round; the X result is folded in only if
+// the sequential Z-then-X order would have stepped X (capped levels are discarded), which
+// leaves every reported number identical to the sequential schedule.
 #pragma once
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -15,9 +24,9 @@ namespace qsfb {
 
 struct BzOptions {
     bool verbose = false;
-    int threads = 0;          // host threads for the seed trials (0 = hardware concurrency)
-    bool no_early_stop = false;  // enumerate every level up to K (count parity)
+    bool no_early_stop = false;  // enumerate every level up to K (single sides; count parity)
     int seed_trials = 256;
+    bool parallel_seed = true;   // seed trials on hardware_concurrency threads (plain path)
 };
 
 // One enumerated level, for the per-(information set, w) count record.
@@ -42,15 +51,16 @@ struct BzResult {
 };
 
 // Upper bound from `trials` random column orders (reference cpp/distfind/bz.cpp:70-116):
-// same generator, seeds and thread split, so the bound matches the reference run on the
-// same host.  `word` receives the logical row that achieved it.
-int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, int threads,
+// same generator, seeds and split of the trials over hardware_concurrency() streams, so
+// the bound equals the reference's on the same host.  parallel=false replays the streams
+// one after another (same result).  `word` receives a logical row achieving the bound.
+int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, bool parallel,
                    std::vector<u64>* word);
 
-// One BZ subproblem stepped level by level on the device.
+// One BZ subproblem stepped level by level.
 class BzSide {
 public:
-    int setup(Device* dev, Session* s, const Problem& p, const BzOptions& opt, const char* tag);
+    int setup_host(const Problem& p, const BzOptions& opt, const char* tag);
     bool has_logicals = false;
     int K = 0, ng = 0, maxw = 0;
     bool even = false;
@@ -71,14 +81,65 @@ public:
     int active_at(int w) const;
     int outer_at(int w) const;
     void absorb(int w, const LevelOut& o);
-    // Rebuild the witness codeword (problem columns) from the recorded source.
     bool witness(std::vector<u64>& out) const;
+    // state right after setup_host (for re-execution)
+    int inner0 = kWeightNone;
+    bool resolved0 = false;
+    void reset();
 };
+
+class BzJob {
+public:
+    // Single subproblem, or (pair=true) the interleaved min over two.
+    BzJob(Problem p0, const BzOptions& opt);
+    BzJob(Problem pz, Problem px, const BzOptions& opt);
+    BzJob(const BzJob&) = delete;
+    BzJob& operator=(const BzJob&) = delete;
+
+    int setup_host();                       // information sets, seeds, packed rows
+    std::vector<SideDev*> device_sides();   // sides that need device data
+    // Level requests of this round (w = next level); side index per request.
+    void requests(std::vector<LevelReq>& q, std::vector<int>& side);
+    // Fold the round's results (one per request, in order) into the schedule.
+    void apply(const std::vector<const LevelOut*>& outs, const std::vector<int>& side);
+    bool done() const { return done_; }
+    void reset();                           // back to the post-setup state
+    BzResult result();                      // final numbers + verified witness
+
+    bool pair = false;
+    Problem p[2];
+    BzSide s[2];
+    BzOptions opt;
+    RunStats stats;
+    std::vector<LevelRecord> trace;
+
+private:
+    int w_ = 0;                // last stepped level
+    int maxw_ = 0;
+    int best_ = kWeightNone;   // pair: best distance found so far
+    bool done_ = false;
+    double t0_ = 0.0, tl_ = 0.0;
+    bool no_stop_ = false;
+};
+
+// Run jobs to completion on one device: host setup on `host_threads` threads (0 = all
+// cores), one bulk upload, then rounds.  Per-job results in `out`.  Returns a Status.
+int run_jobs(Device* dev, std::vector<BzJob*>& jobs, int host_threads, RunStats* stats,
+             int* rounds = nullptr);
+
+// The two halves of run_jobs, for callers that keep the device data resident and run the
+// rounds repeatedly: host setup of every job + one upload into `arena`, then the rounds.
+int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
+               int host_threads, RunStats* stats);
+int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* rounds,
+               double* span_ms = nullptr);
 
 int bz_distance(Device* dev, const Problem& p, const BzOptions& opt, BzResult& r);
 int bz_min_interleaved(Device* dev, const Problem& pz, const Problem& px, const BzOptions& opt,
                        BzResult& r);
 // Non-CSS: isometry to a 3q-column Hamming problem, BZ, then halve.
 int symplectic_bz_distance(Device* dev, const Problem& sp, const BzOptions& opt, BzResult& r);
+
+double now_seconds();
 
 }  // namespace qsfb

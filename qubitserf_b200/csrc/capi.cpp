@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -161,6 +162,25 @@ int symplectic_driver(const Mat& gauge, bool subsystem, const char* method, char
 }
 
 }  // namespace
+
+struct QsfbBatchHandle {
+    Device* dev = nullptr;
+    std::vector<int> kinds;
+    struct Map { int job0 = -1, job1 = -1; int zw = -1, xw = -1; };
+    std::vector<Map> map;
+    std::vector<std::unique_ptr<BzJob>> jobs;
+    std::vector<BzJob*> ptrs;
+    // declared after the jobs so that the arena outlives nothing that points into it
+    std::unique_ptr<Arena> arena;
+    std::unique_ptr<SessionLease> lease;
+    RunStats setup;
+    bool executed = false;
+    ~QsfbBatchHandle() {
+        jobs.clear();
+        arena.reset();
+        lease.reset();
+    }
+};
 
 extern "C" {
 
@@ -324,15 +344,18 @@ int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const ui
     int rc = kOk;
     Device* dev = device_or(&rc);
     if (!dev) return rc;
+    // The reference weighs every bit of the `stride` words (cpp/qsf/bits.hpp:29-33), so a
+    // raw plan is enumerated over stride*64 columns.
+    const int ncols = stride * 64;
     Problem p;
-    p.n = n;
+    p.n = ncols;
     p.count_all = kcheck == 0;
-    p.code_gen = Mat(K, n);
-    p.check = Mat(kcheck, n);
+    p.code_gen = Mat(K, ncols);
+    p.check = Mat(kcheck, ncols);
     if (kcheck > 0) std::copy(check, check + (size_t)kcheck * stride, p.check.w.begin());
     std::vector<InfoSet> sets(num_gamma);
     for (int g = 0; g < num_gamma; ++g) {
-        sets[g].g = Mat(K, n);
+        sets[g].g = Mat(K, ncols);
         std::copy(gamma + (size_t)g * K * stride, gamma + (size_t)(g + 1) * K * stride,
                   sets[g].g.w.begin());
         sets[g].rank = 0;   // raw rows: no pivot structure is assumed
@@ -340,7 +363,8 @@ int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const ui
     SessionLease lease(dev);
     if (!lease.s) return kErrDevice;
     SideDev S;
-    rc = S.init(dev, lease.s, p, sets);
+    rc = S.prepare(p, sets);
+    if (rc == kOk) rc = S.upload(dev, lease.s);
     if (rc != kOk) return rc;
     std::vector<LevelReq> q(1);
     q[0].side = &S;
@@ -421,6 +445,143 @@ int qsfb_last_counts(int* side, int* w, int* g, unsigned long long* count, int c
         if (count) count[i] = g_last.count[i];
     }
     return n;
+}
+
+int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
+                       QsfbBatchHandle** handle) {
+    if ((!queries && nq > 0) || !handle) return kErrNull;
+    *handle = nullptr;
+    int rc = kOk;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    auto* H = new QsfbBatchHandle();
+    H->dev = dev;
+    H->kinds.resize(nq);
+    H->map.resize(nq);
+    BzOptions opt;
+    opt.parallel_seed = false;   // the batch parallelizes over codes instead
+    auto& jobs = H->jobs;
+    for (int i = 0; i < nq; ++i) {
+        const QsfbQuery& q = queries[i];
+        H->kinds[i] = q.kind;
+        if (!q.A || (q.kind != 0 && !q.B)) { delete H; return kErrNull; }
+        Mat A = from_dense(q.A, q.a_rows, q.a_cols);
+        auto& m = H->map[i];
+        if (q.kind == 0) {
+            m.job0 = (int)jobs.size();
+            jobs.emplace_back(new BzJob(classical_problem(A), opt));
+        } else if (q.kind == 1) {
+            Mat B = from_dense(q.B, q.b_rows, q.b_cols);
+            m.job0 = (int)jobs.size();
+            if (q.which == 'Z' || q.which == 'X')
+                jobs.emplace_back(new BzJob(css_problem(A, B, q.which), opt));
+            else
+                jobs.emplace_back(new BzJob(css_problem(A, B, 'Z'), css_problem(A, B, 'X'), opt));
+        } else if (q.kind == 2) {
+            if (!q.z_op || !q.x_op) { delete H; return kErrNull; }
+            Mat B = from_dense(q.B, q.b_rows, q.b_cols);
+            // Z part modulo rowspace(Gz), X part modulo rowspace(Gx) (op_weight.cpp:22-41)
+            if (in_rowspace(B, q.z_op)) m.zw = 0;
+            else { m.job0 = (int)jobs.size(); jobs.emplace_back(new BzJob(coset_problem(B, q.z_op), opt)); }
+            if (in_rowspace(A, q.x_op)) m.xw = 0;
+            else { m.job1 = (int)jobs.size(); jobs.emplace_back(new BzJob(coset_problem(A, q.x_op), opt)); }
+        } else {
+            delete H;
+            return kErrShape;
+        }
+    }
+    for (auto& j : jobs) H->ptrs.push_back(j.get());
+    H->lease.reset(new SessionLease(dev));
+    if (!H->lease->s) { delete H; return kErrDevice; }
+    H->arena.reset(new Arena(dev));
+    rc = setup_jobs(dev, H->lease->s, H->arena.get(), H->ptrs, host_threads, &H->setup);
+    if (rc != kOk) { delete H; return rc; }
+    *handle = H;
+    return kOk;
+}
+
+int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats) {
+    if (!H || (!out && !H->map.empty())) return kErrNull;
+    const double t0 = now_seconds();
+    if (H->executed)
+        for (BzJob* j : H->ptrs) j->reset();
+    H->executed = true;
+    RunStats rs;
+    int rounds = 0;
+    double span = 0.0;
+    int rc = run_rounds(H->lease->s, H->ptrs, &rs, &rounds, &span);
+    if (rc != kOk) return rc;
+    auto& jobs = H->jobs;
+    for (size_t i = 0; i < H->map.size(); ++i) {
+        QsfbAnswer& a = out[i];
+        std::memset(&a, 0, sizeof(a));
+        const auto& m = H->map[i];
+        if (H->kinds[i] == 2) {
+            BzResult rz, rx;
+            int zw = m.zw, xw = m.xw;
+            bool ok = true, proven = true;
+            if (m.job0 >= 0) { rz = jobs[m.job0]->result(); zw = rz.distance; ok &= rz.witness_ok || zw <= 0; proven &= rz.proven; }
+            if (m.job1 >= 0) { rx = jobs[m.job1]->result(); xw = rx.distance; ok &= rx.witness_ok || xw <= 0; proven &= rx.proven; }
+            a.z_weight = zw;
+            a.x_weight = xw;
+            a.distance = std::max(zw, xw);
+            a.proven = proven ? 1 : 0;
+            a.witness_ok = ok ? 1 : 0;
+            a.levels = std::max(m.job0 >= 0 ? rz.levels : 0, m.job1 >= 0 ? rx.levels : 0);
+        } else {
+            BzResult r = jobs[m.job0]->result();
+            a.distance = r.distance;
+            a.lower_bound = r.lower_bound;
+            a.proven = r.proven ? 1 : 0;
+            a.levels = r.levels;
+            a.witness_ok = (r.witness_ok || r.distance < 0) ? 1 : 0;
+            a.z_weight = a.x_weight = -1;
+        }
+    }
+    if (stats) {
+        stats->seconds = now_seconds() - t0;
+        stats->host_setup_seconds = H->setup.host_setup_s;
+        stats->device_ms = rs.ms_gen + rs.ms_pairs;
+        stats->device_span_ms = span;
+        stats->pair_ms = rs.ms_pairs;
+        stats->codewords = rs.codewords;
+        stats->rounds = rounds;
+        stats->kernel_launches = rs.launches;
+        stats->certificates = (int)jobs.size();
+    }
+    return kOk;
+}
+
+void qsfb_batch_free(QsfbBatchHandle* H) { delete H; }
+
+int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
+               QsfbBatchStats* stats) {
+    const double t0 = now_seconds();
+    QsfbBatchHandle* H = nullptr;
+    int rc = qsfb_batch_prepare(queries, nq, host_threads, &H);
+    if (rc != kOk) return rc;
+    rc = qsfb_batch_execute(H, out, stats);
+    qsfb_batch_free(H);
+    if (stats) stats->seconds = now_seconds() - t0;
+    return rc;
+}
+
+int qsfb_flush_l2(void) {
+    int rc = kOk;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    static void* buf = nullptr;
+    const size_t bytes = 256ull << 20;
+    if (!buf) buf = dev->alloc(bytes);
+    if (!buf) return kErrMemory;
+    SessionLease lease(dev);
+    if (!lease.s) return kErrDevice;
+    if (cudaMemsetAsync(buf, 0x5a, bytes, lease.s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(lease.s->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrDevice;
+    }
+    return kOk;
 }
 
 const char* qsfb_device_name(void) {

@@ -10,7 +10,7 @@ namespace qsfb {
 
 cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
                              const unsigned long long* d_binom, int num_sms, cudaStream_t st);
-cudaError_t launch_pairs(int H, int HP, bool full, const LevelDesc* d, int nd,
+cudaError_t launch_pairs(int H, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
 
@@ -179,19 +179,41 @@ int Session::ensure(size_t dbytes, size_t hbytes) {
     return kOk;
 }
 
+// ------------------------------------------------------------------ Arena
+Arena::~Arena() {
+    for (auto& c : chunks_) dev_->release(c.first, c.second);
+}
+
+void* Arena::alloc(size_t bytes) {
+    bytes = align_up(std::max<size_t>(bytes, 16), 256);
+    if (chunks_.empty() || used_ + bytes > chunks_.back().second) {
+        const size_t sz = round_bucket(std::max<size_t>(bytes, 64ull << 20));
+        char* p = (char*)dev_->alloc(sz);
+        if (!p) return nullptr;
+        chunks_.push_back({p, sz});
+        used_ = 0;
+        total_ += sz;
+    }
+    char* p = chunks_.back().first + used_;
+    used_ += bytes;
+    return p;
+}
+
 // ------------------------------------------------------------------ SideDev
 SideDev::~SideDev() {
     if (!dev) return;
-    dev->release(d_red, bytes_red);
-    dev->release(d_syn, bytes_syn);
+    if (owns) {
+        dev->release(d_red, bytes_red);
+        dev->release(d_syn, bytes_syn);
+    }
     for (auto& kv : lists) {
+        if (kv.second.arena) continue;
         dev->release(kv.second.words, kv.second.bytes_w);
         dev->release(kv.second.pc, kv.second.bytes_pc);
     }
 }
 
-int SideDev::init(Device* d, Session* s, const Problem& p, const std::vector<InfoSet>& sets) {
-    dev = d;
+int SideDev::prepare(const Problem& p, const std::vector<InfoSet>& sets) {
     n = p.n;
     K = p.code_gen.rows;
     ng = (int)sets.size();
@@ -200,7 +222,7 @@ int SideDev::init(Device* d, Session* s, const Problem& p, const std::vector<Inf
     if (K > kBinomMaxN || ng > 255 || ng == 0) return kErrUnsupported;
     int max_red = 1;
     ranks.resize(ng);
-    nonpivot.resize(ng);
+    nonpivot.assign(ng, {});
     for (int g = 0; g < ng; ++g) {
         ranks[g] = sets[g].rank;
         std::vector<char> isp(n, 0);
@@ -213,29 +235,65 @@ int SideDev::init(Device* d, Session* s, const Problem& p, const std::vector<Inf
     SW = (kcheck + 31) / 32;
     if (W32 > 32 || SW > 32) return kErrUnsupported;
     const int swp = std::max(SW, 1);
-    std::vector<uint32_t> red((size_t)ng * K * W32, 0u), syn((size_t)ng * K * swp, 0u);
+    h_red.assign((size_t)ng * K * W32, 0u);
+    h_syn.assign((size_t)ng * K * swp, 0u);
     for (int g = 0; g < ng; ++g) {
         const Mat& G = sets[g].g;
+        const std::vector<int>& np = nonpivot[g];
         for (int r = 0; r < K; ++r) {
-            uint32_t* o = &red[((size_t)g * K + r) * W32];
+            uint32_t* o = &h_red[((size_t)g * K + r) * W32];
             const u64* row = G.row(r);
-            const std::vector<int>& np = nonpivot[g];
             for (size_t i = 0; i < np.size(); ++i) {
                 const int c = np[i];
                 if ((row[c >> 6] >> (c & 63)) & 1u) o[i >> 5] |= 1u << (i & 31);
             }
-            uint32_t* so = &syn[((size_t)g * K + r) * swp];
+            uint32_t* so = &h_syn[((size_t)g * K + r) * swp];
             for (int c = 0; c < kcheck; ++c)
                 if (vec_dot(p.check.row(c), row, G.stride)) so[c >> 5] |= 1u << (c & 31);
         }
     }
-    bytes_red = red.size() * 4;
-    bytes_syn = syn.size() * 4;
+    bytes_red = h_red.size() * 4;
+    bytes_syn = h_syn.size() * 4;
+    return kOk;
+}
+
+int SideDev::upload(Device* d, Session* s) {
+    dev = d;
+    owns = true;
     d_red = (uint32_t*)dev->alloc(bytes_red);
     d_syn = (uint32_t*)dev->alloc(bytes_syn);
     if (!d_red || !d_syn) return kErrMemory;
-    if (cudaMemcpyAsync(d_red, red.data(), bytes_red, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
-        cudaMemcpyAsync(d_syn, syn.data(), bytes_syn, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+    if (cudaMemcpyAsync(d_red, h_red.data(), bytes_red, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaMemcpyAsync(d_syn, h_syn.data(), bytes_syn, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrDevice;
+    }
+    return kOk;
+}
+
+int upload_sides(Device* dev, Session* s, Arena* arena, const std::vector<SideDev*>& sides) {
+    size_t total = 0;
+    for (SideDev* S : sides) total += align_up(S->bytes_red, 256) + align_up(S->bytes_syn, 256);
+    if (total == 0) return kOk;
+    char* d = (char*)arena->alloc(total);
+    if (!d) return kErrMemory;
+    int rc = s->ensure(0, total);
+    if (rc != kOk) return rc;
+    char* h = (char*)s->h_stage.h;
+    size_t off = 0;
+    for (SideDev* S : sides) {
+        S->dev = dev;
+        S->arena = arena;
+        S->owns = false;
+        std::memcpy(h + off, S->h_red.data(), S->bytes_red);
+        S->d_red = (uint32_t*)(d + off);
+        off += align_up(S->bytes_red, 256);
+        std::memcpy(h + off, S->h_syn.data(), S->bytes_syn);
+        S->d_syn = (uint32_t*)(d + off);
+        off += align_up(S->bytes_syn, 256);
+    }
+    if (cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
         cudaStreamSynchronize(s->stream) != cudaSuccess) {
         cudaGetLastError();
         return kErrDevice;
@@ -267,7 +325,7 @@ unsigned long long key_init(int bound) {
 }
 
 struct Plan {
-    int req, g, a, b, H, HP, full;
+    int req, g, a, b, H, HP, full, mode;
     unsigned long long pairs;
     int p_lo, nterms;
     std::vector<unsigned long long> term_jobs;
@@ -305,6 +363,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             const int wg = std::max(1, words_of(nred));
             P.HP = wg >= 3 ? 4 : wg;
             P.full = rank == K;
+            // mode: 0 rank-deficient, 1 full rank, 2 full rank with no room above the
+            // pivot bits (every candidate needs an all-zero non-pivot part)
             // smallest probe width whose random-code survivor rate is negligible
             const int T = std::max(0, std::min(q.bound + 1, 4095));
             const int pcmin = std::max(0, w - (K - rank));
@@ -313,6 +373,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 if (binom_cdf_half(std::min(32 * h, nred), T - 1 - pcmin) <= 1e-6) { H = h; break; }
             }
             P.H = H;
+            P.mode = !P.full ? 0 : (T - 1 - w <= 0 ? 2 : 1);
             P.pairs = pairs;
             P.p_lo = a - 1;
             P.nterms = K - b - a + 1;
@@ -335,14 +396,22 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             const int size = side == 0 ? P.a : P.b;
             auto key = std::make_tuple(P.g, size, side);
             ListBuf& L = S->lists[key];
-            if (L.ready || L.words) continue;
+            if (L.ready) continue;
+            if (L.words) {   // allocated by an earlier execution: regenerate in place
+                bool dup = false;
+                for (const GenReq& G : gens)
+                    dup |= G.S == S && G.g == P.g && G.size == size && G.reflect == side;
+                if (!dup) gens.push_back({S, P.g, size, side, P.HP});
+                continue;
+            }
             L.count = dev->binom(S->K, size);
-            L.bytes_w = (size_t)L.count * P.HP * 4;
-            L.words = (uint32_t*)dev->alloc(std::max<size_t>(L.bytes_w, 16));
+            L.bytes_w = std::max<size_t>((size_t)L.count * P.HP * 4, 16);
+            L.arena = S->arena != nullptr;
+            L.words = (uint32_t*)(L.arena ? S->arena->alloc(L.bytes_w) : dev->alloc(L.bytes_w));
             if (!L.words) return kErrMemory;
             if (!P.full) {
                 L.bytes_pc = std::max<size_t>((size_t)L.count, 16);
-                L.pc = (uint8_t*)dev->alloc(L.bytes_pc);
+                L.pc = (uint8_t*)(L.arena ? S->arena->alloc(L.bytes_pc) : dev->alloc(L.bytes_pc));
                 if (!L.pc) return kErrMemory;
             }
             S->list_bytes += L.bytes_w + L.bytes_pc;
@@ -371,8 +440,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     std::vector<int> order(plans.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return std::make_tuple(plans[x].H, plans[x].HP, plans[x].full) <
-               std::make_tuple(plans[y].H, plans[y].HP, plans[y].full);
+        return std::make_tuple(plans[x].H, plans[x].HP, plans[x].mode) <
+               std::make_tuple(plans[y].H, plans[y].HP, plans[y].mode);
     });
 
     // 4) staging layout
@@ -424,13 +493,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     LevelDesc* hl = (LevelDesc*)(h + off_lvl);
     unsigned long long* hterms = (unsigned long long*)(h + off_terms);
     size_t term_cursor = 0;
-    struct Group { int H, HP, full, first, count; unsigned long long jobs; };
+    struct Group { int H, HP, mode, first, count; unsigned long long jobs; };
     std::vector<Group> groups;
     for (size_t oi = 0; oi < order.size(); ++oi) {
         const Plan& P = plans[order[oi]];
         if (groups.empty() || groups.back().H != P.H || groups.back().HP != P.HP ||
-            groups.back().full != P.full)
-            groups.push_back({P.H, P.HP, P.full, (int)oi, 0, 0ull});
+            groups.back().mode != P.mode)
+            groups.push_back({P.H, P.HP, P.mode, (int)oi, 0, 0ull});
         Group& Gp = groups.back();
         SideDev* S = reqs[P.req].side;
         LevelDesc& D = hl[oi];
@@ -485,7 +554,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     unsigned long long all_jobs = 0;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& Gp = groups[gi];
-        if (launch_pairs(Gp.H, Gp.HP, Gp.full != 0, (const LevelDesc*)(d + off_lvl) + Gp.first, Gp.count,
+        if (launch_pairs(Gp.H, Gp.HP, Gp.mode, (const LevelDesc*)(d + off_lvl) + Gp.first, Gp.count,
                          Gp.jobs, (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
                          dev->num_sms, st) != cudaSuccess) {
             cudaEventDestroy(evm);

@@ -103,6 +103,24 @@ struct ListBuf {
     unsigned long long count = 0;
     size_t bytes_w = 0, bytes_pc = 0;
     bool ready = false;
+    bool arena = false;   // carved from an Arena (released with it)
+};
+
+// Bump allocator over device chunks taken from the caching allocator; everything carved
+// from it is released together when the arena is destroyed (one batch).
+class Arena {
+public:
+    explicit Arena(Device* d) : dev_(d) {}
+    Arena(const Arena&) = delete;
+    Arena& operator=(const Arena&) = delete;
+    ~Arena();
+    void* alloc(size_t bytes);
+    size_t bytes() const { return total_; }
+
+private:
+    Device* dev_;
+    std::vector<std::pair<char*, size_t>> chunks_;
+    size_t used_ = 0, total_ = 0;
 };
 
 class SideDev {
@@ -112,20 +130,29 @@ public:
     SideDev& operator=(const SideDev&) = delete;
     ~SideDev();
 
-    // Upload the information sets of problem `p`.  Returns a Status.
-    int init(Device* dev, Session* s, const Problem& p, const std::vector<InfoSet>& sets);
+    // Host half: pack every information set's rows over its non-pivot columns and the
+    // per-row detector syndromes.  Returns a Status (no device work).
+    int prepare(const Problem& p, const std::vector<InfoSet>& sets);
+    // Device half for a single side: own allocation + copy on the session stream.
+    int upload(Device* dev, Session* s);
 
     int n = 0, K = 0, ng = 0, W32 = 0, SW = 0, kcheck = 0;
     bool count_all = false;
     std::vector<int> ranks;
     std::vector<std::vector<int>> nonpivot;   // per set: non-pivot columns (bit order of red)
+    std::vector<uint32_t> h_red, h_syn;       // host images (ng x K x W32, ng x K x max(SW,1))
     Device* dev = nullptr;
-    uint32_t* d_red = nullptr;   // ng x K x W32
-    uint32_t* d_syn = nullptr;   // ng x K x max(SW,1)
+    Arena* arena = nullptr;      // list storage (null: caching allocator per list)
+    bool owns = false;           // d_red/d_syn allocated by upload()
+    uint32_t* d_red = nullptr;
+    uint32_t* d_syn = nullptr;
     size_t bytes_red = 0, bytes_syn = 0;
     std::map<std::tuple<int, int, int>, ListBuf> lists;   // (g, size, reflect)
     size_t list_bytes = 0;
 };
+
+// Upload many prepared sides with one allocation (from `arena`) and one host->device copy.
+int upload_sides(Device* dev, Session* s, Arena* arena, const std::vector<SideDev*>& sides);
 
 struct LevelReq {
     SideDev* side = nullptr;
@@ -149,6 +176,7 @@ struct RunStats {
     unsigned long long jobs = 0;
     unsigned long long codewords = 0;
     int launches = 0;
+    double host_setup_s = 0.0;
 };
 
 // Enumerate every request; blocking.  Returns a Status.

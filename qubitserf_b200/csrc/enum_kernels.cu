@@ -223,11 +223,26 @@ __device__ __forceinline__ int fold_min(const uint32_t (&x)[H], const uint32_t (
     }
 }
 
-template <int H, int HP, bool FULL>
+// Zero test: running unsigned minimum of the OR of the XORed probe words (no POPC); a
+// pair can only be a candidate when every probe word of its XOR is zero.
+template <int H>
+__device__ __forceinline__ uint32_t fold_zero(const uint32_t (&x)[H], const uint32_t (&y)[H],
+                                              uint32_t m) {
+    uint32_t v = x[0] ^ y[0];
+#pragma unroll
+    for (int h = 1; h < H; ++h) v |= x[h] ^ y[h];
+    return v < m ? v : m;
+}
+
+// MODE 0: rank-deficient set (per-entry pivot counts); 1: full-rank set, popcount bound;
+// 2: full-rank set whose bound leaves no room for any non-pivot bit (zero test).
+template <int H, int HP, int MODE>
 __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict__ descs,
                                                     int ndesc, unsigned long long total_jobs,
                                                     unsigned long long* __restrict__ job_counter,
                                                     const unsigned long long* __restrict__ B) {
+    constexpr bool FULL = MODE != 0;
+    constexpr bool ZERO = MODE == 2;
     const int lane = threadIdx.x & 31;
     for (;;) {
         unsigned long long job = 0;
@@ -287,7 +302,7 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                 pcr[i] = 1 << 20;
             }
             thr[i] = T - pcr[i] - (FULL ? (regX ? D.b : D.a) : 0);
-            m[i] = 0x7fffffff;
+            m[i] = ZERO ? -1 : 0x7fffffff;
         }
 
         // Sweep the loop entries in chunks of kChunk; after each chunk the (rare) lanes
@@ -307,19 +322,31 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                     load_entry<H, HP>(lp + (j + 3) * HP, y3);
 #pragma unroll
                     for (int i = 0; i < RX; ++i) {
-                        int mm = m[i];
-                        mm = fold_min<H>(x[i], y0, 0, mm);
-                        mm = fold_min<H>(x[i], y1, 0, mm);
-                        mm = fold_min<H>(x[i], y2, 0, mm);
-                        mm = fold_min<H>(x[i], y3, 0, mm);
-                        m[i] = mm;
+                        if constexpr (ZERO) {
+                            uint32_t mm = (uint32_t)m[i];
+                            mm = fold_zero<H>(x[i], y0, mm);
+                            mm = fold_zero<H>(x[i], y1, mm);
+                            mm = fold_zero<H>(x[i], y2, mm);
+                            mm = fold_zero<H>(x[i], y3, mm);
+                            m[i] = (int)mm;
+                        } else {
+                            int mm = m[i];
+                            mm = fold_min<H>(x[i], y0, 0, mm);
+                            mm = fold_min<H>(x[i], y1, 0, mm);
+                            mm = fold_min<H>(x[i], y2, 0, mm);
+                            mm = fold_min<H>(x[i], y3, 0, mm);
+                            m[i] = mm;
+                        }
                     }
                 }
                 for (; j < cend; ++j) {
                     uint32_t y0[H];
                     load_entry<H, HP>(lp + j * HP, y0);
 #pragma unroll
-                    for (int i = 0; i < RX; ++i) m[i] = fold_min<H>(x[i], y0, 0, m[i]);
+                    for (int i = 0; i < RX; ++i) {
+                        if constexpr (ZERO) m[i] = (int)fold_zero<H>(x[i], y0, (uint32_t)m[i]);
+                        else m[i] = fold_min<H>(x[i], y0, 0, m[i]);
+                    }
                 }
             } else {
                 for (; j < cend; ++j) {
@@ -332,11 +359,11 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
             }
             bool any = false;
 #pragma unroll
-            for (int i = 0; i < RX; ++i) any |= m[i] < thr[i];
+            for (int i = 0; i < RX; ++i) any |= ZERO ? (m[i] == 0 && thr[i] > 0) : m[i] < thr[i];
             if (any) {
 #pragma unroll 1
                 for (int i = 0; i < RX; ++i) {
-                    if (m[i] < thr[i]) {
+                    if (ZERO ? (m[i] == 0 && thr[i] > 0) : m[i] < thr[i]) {
                         const unsigned long long e = reg0 + lane + 32 * i;
                         T = survivor_scan(D, B, regX, xoff, e, pcr[i],
                                           loop0 + (unsigned long long)c0, cn, T);
@@ -347,7 +374,7 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                     thr[i] = T - pcr[i] - (FULL ? (regX ? D.b : D.a) : 0);
             }
 #pragma unroll
-            for (int i = 0; i < RX; ++i) m[i] = 0x7fffffff;
+            for (int i = 0; i < RX; ++i) m[i] = ZERO ? -1 : 0x7fffffff;
         }
         if (lane == 0) atomicAdd(D.count, reg_cnt * (unsigned long long)loop_cnt);
     }
@@ -366,42 +393,41 @@ cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long lo
     return cudaGetLastError();
 }
 
-template <int H, int HP, bool FULL>
+template <int H, int HP, int MODE>
 static cudaError_t launch_pairs_t(const LevelDesc* d, int nd, unsigned long long jobs,
                                   unsigned long long* ctr, const unsigned long long* B,
                                   int num_sms, cudaStream_t st) {
     static int blocks_per_sm = 0;
     if (blocks_per_sm == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
-                                                      dev::pairs_kernel<H, HP, FULL>, 128, 0);
+                                                      dev::pairs_kernel<H, HP, MODE>, 128, 0);
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     unsigned long long blocks = (unsigned long long)num_sms * blocks_per_sm;
     const unsigned long long need = (jobs + 3) / 4;   // 4 warps per block
     if (need < blocks) blocks = need;
     if (blocks < 1) blocks = 1;
-    dev::pairs_kernel<H, HP, FULL><<<(unsigned)blocks, 128, 0, st>>>(d, nd, jobs, ctr, B);
+    dev::pairs_kernel<H, HP, MODE><<<(unsigned)blocks, 128, 0, st>>>(d, nd, jobs, ctr, B);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pairs(int H, int HP, bool full, const LevelDesc* d, int nd,
+#define QSFB_PAIRS_CASE(H, HP, M) \
+    case ((H) * 8 + (HP)) * 4 + (M): \
+        return launch_pairs_t<H, HP, M>(d, nd, jobs, ctr, B, num_sms, st);
+
+cudaError_t launch_pairs(int H, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st) {
     if (jobs == 0) return cudaSuccess;
-    const int key = (H * 8 + HP) * 2 + (full ? 1 : 0);
-    switch (key) {
-        case (1 * 8 + 1) * 2: return launch_pairs_t<1, 1, false>(d, nd, jobs, ctr, B, num_sms, st);
-        case (1 * 8 + 1) * 2 + 1: return launch_pairs_t<1, 1, true>(d, nd, jobs, ctr, B, num_sms, st);
-        case (2 * 8 + 2) * 2: return launch_pairs_t<2, 2, false>(d, nd, jobs, ctr, B, num_sms, st);
-        case (2 * 8 + 2) * 2 + 1: return launch_pairs_t<2, 2, true>(d, nd, jobs, ctr, B, num_sms, st);
-        case (2 * 8 + 4) * 2: return launch_pairs_t<2, 4, false>(d, nd, jobs, ctr, B, num_sms, st);
-        case (2 * 8 + 4) * 2 + 1: return launch_pairs_t<2, 4, true>(d, nd, jobs, ctr, B, num_sms, st);
-        case (3 * 8 + 4) * 2: return launch_pairs_t<3, 4, false>(d, nd, jobs, ctr, B, num_sms, st);
-        case (3 * 8 + 4) * 2 + 1: return launch_pairs_t<3, 4, true>(d, nd, jobs, ctr, B, num_sms, st);
-        case (4 * 8 + 4) * 2: return launch_pairs_t<4, 4, false>(d, nd, jobs, ctr, B, num_sms, st);
-        case (4 * 8 + 4) * 2 + 1: return launch_pairs_t<4, 4, true>(d, nd, jobs, ctr, B, num_sms, st);
+    switch ((H * 8 + HP) * 4 + mode) {
+        QSFB_PAIRS_CASE(1, 1, 0) QSFB_PAIRS_CASE(1, 1, 1) QSFB_PAIRS_CASE(1, 1, 2)
+        QSFB_PAIRS_CASE(2, 2, 0) QSFB_PAIRS_CASE(2, 2, 1) QSFB_PAIRS_CASE(2, 2, 2)
+        QSFB_PAIRS_CASE(2, 4, 0) QSFB_PAIRS_CASE(2, 4, 1) QSFB_PAIRS_CASE(2, 4, 2)
+        QSFB_PAIRS_CASE(3, 4, 0) QSFB_PAIRS_CASE(3, 4, 1) QSFB_PAIRS_CASE(3, 4, 2)
+        QSFB_PAIRS_CASE(4, 4, 0) QSFB_PAIRS_CASE(4, 4, 1) QSFB_PAIRS_CASE(4, 4, 2)
         default: return cudaErrorInvalidValue;
     }
 }
+#undef QSFB_PAIRS_CASE
 
 }  // namespace qsfb
