@@ -193,6 +193,24 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
 int qsfb_batch_execute(QsfbBatchHandle* handle, QsfbAnswer* out, QsfbBatchStats* stats);
 void qsfb_batch_free(QsfbBatchHandle* handle);
 
+/* No counterpart in the reference.  qsfb_enumerate_plan for callers that cannot allocate
+ * device memory (a process whose own pool owns the device, or code that must not cause the
+ * device-wide synchronisation of a cudaMalloc).  Inputs and outputs are DEVICE pointers
+ * owned by the caller: d_gamma (num_gamma*K*stride u64), d_check (kcheck*stride u64),
+ * d_out_best (1 int), d_out_counts (num_gamma, may be NULL), d_out_g / d_out_rank (may be
+ * NULL).  Results equal qsfb_enumerate_plan's.  All scratch sits in one fixed 32 MiB device
+ * array inside the library (held on every GPU the library runs on until exit), shared by
+ * every call: calls that overlap on the GPU race, so serialise them.  The first call on a
+ * device sets the array up; make it before any stream capture.  Limits: K <= 128,
+ * num_gamma <= 8, kcheck <= 256, stride <= 16 and the level's subset lists within the
+ * array; beyond them it returns 8 without touching the device.  stream: a cudaStream_t
+ * (NULL = default stream); returns after the level has finished on that stream. */
+int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int num_gamma,
+                                const uint64_t* d_gamma, int kcheck, const uint64_t* d_check,
+                                int current_best, int* d_out_best,
+                                unsigned long long* d_out_counts, int* d_out_g,
+                                unsigned long long* d_out_rank, void* stream);
+
 /* Overwrite a 256 MiB device buffer (more than the 126 MB L2) and wait; benchmarks call it
  * between timed steps.  Returns 0, or 4 without a device. */
 int qsfb_flush_l2(void);

@@ -25,6 +25,7 @@ ERRORS = {
     5: "unsupported method/backend/size on the B200 engine",
     6: "device memory exhausted",
     7: "output buffer too small",
+    8: "beyond the fixed scratch of the no-allocation entry point",
 }
 
 
@@ -104,6 +105,9 @@ SIGNATURES = [
     ("qsfb_batch_execute", _i, [ctypes.c_void_p, ctypes.POINTER(QsfbAnswer),
                                 ctypes.POINTER(QsfbBatchStats)]),
     ("qsfb_batch_free", None, [ctypes.c_void_p]),
+    ("qsfb_enumerate_plan_noalloc", _i, [_i, _i, _i, _i, _i, ctypes.c_void_p, _i,
+                                         ctypes.c_void_p, _i, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("qsfb_flush_l2", _i, []),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
