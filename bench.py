@@ -169,12 +169,27 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--codes", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-resident", action="store_true",
+                    help="time only the resident-input rounds (profiling runs)")
+    ap.add_argument("--workload", default="batch",
+                    choices=["batch", "css128", "classical128", "classical96"],
+                    help="batch = the 1024-code batch; the others certify one code")
     args = ap.parse_args()
 
     rank, world, local, pg = dist_setup(args.gpus)
     from qubitserf_b200 import workloads as W
-    codes = W.batch_1024(args.codes)
-    config = {"workload": f"batch_{args.codes}_uneven_seed3", "codes": args.codes,
+    if args.workload == "batch":
+        codes = W.batch_1024(args.codes)
+        wname = f"batch_{args.codes}_uneven_seed3"
+    else:
+        one = {"css128": lambda: W.CodeSpec("css", W.single_css_128(), 128),
+               "classical128": lambda: W.CodeSpec("classical", (W.single_classical_128(),), 128),
+               "classical96": lambda: W.CodeSpec("classical", (W.single_classical_96(),), 96)}
+        codes = [one[args.workload]()]
+        args.codes = 1
+        wname = {"css128": "css_n128_rank40x40_seed1_min", "classical128": "classical_n128_k40_seed2",
+                 "classical96": "classical_n96_k32_seed0"}[args.workload]
+    config = {"workload": wname, "codes": args.codes,
               "classical": sum(c.kind == "classical" for c in codes),
               "css": sum(c.kind == "css" for c in codes), "n_range": [40, 128],
               "parallelism": f"replicas{world}",
@@ -234,6 +249,14 @@ def main():
     # algorithmic POPC of the full evaluation: per level work x 2W (W = 64-bit words)
     # (codewords of each code are not separated per code inside a batch: use the batch's
     #  codeword-weighted W from a plain pass below)
+
+    if args.only_resident:
+        if rank == 0:
+            print(json.dumps({"workload": wname, "certs_per_s": value,
+                              "ms_per_step": span_s / args.steps * 1000.0,
+                              "gcodewords_per_s": cw / max(pair_ms / 1000.0, 1e-12) / 1e9,
+                              "rounds": rounds, "launches": launches}), flush=True)
+        return
 
     # --- end to end: the one-shot public call from host matrices, K times
     e2e_t = []
