@@ -169,7 +169,9 @@ typedef struct {
 
 typedef struct {
     double seconds;              /* wall time of the call */
-    double host_setup_seconds;   /* problem reduction + information sets + seed bounds */
+    double prepare_seconds;      /* wall time of the prepare phase */
+    double host_setup_seconds;   /* problem reduction + information sets + seed orders */
+    double device_seed_seconds;  /* seed eliminations on the device (copy + kernel) */
     double device_ms;            /* list generation + pair sweeps (sum of kernel time) */
     double device_span_ms;       /* CUDA-event span of all rounds, host gaps included */
     double pair_ms;              /* pair-sweep kernel time alone */

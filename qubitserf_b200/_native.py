@@ -66,7 +66,8 @@ class QsfbAnswer(ctypes.Structure):
 
 
 class QsfbBatchStats(ctypes.Structure):
-    _fields_ = [("seconds", ctypes.c_double), ("host_setup_seconds", ctypes.c_double),
+    _fields_ = [("seconds", ctypes.c_double), ("prepare_seconds", ctypes.c_double),
+                ("host_setup_seconds", ctypes.c_double), ("device_seed_seconds", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("device_span_ms", ctypes.c_double),
                 ("pair_ms", ctypes.c_double), ("codewords", ctypes.c_ulonglong),
                 ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),

@@ -12,6 +12,9 @@
 #include <numeric>
 #include <random>
 #include <thread>
+#include <cstring>
+
+#include "seed_types.hpp"
 
 namespace qsfb {
 
@@ -98,6 +101,43 @@ int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, b
     return best;
 }
 
+std::vector<int> seed_orders(int n, int trials, unsigned seed, int only) {
+    int nth = (int)std::thread::hardware_concurrency();
+    if (nth < 1) nth = 1;
+    if (nth > trials) nth = trials;
+    std::vector<int> out;
+    out.reserve((size_t)(only >= 0 ? 1 : trials) * n);
+    std::vector<int> cols(n);
+    for (int t = 0; t < nth; ++t) {
+        const int lo = (int)((long)trials * t / nth);
+        const int hi = (int)((long)trials * (t + 1) / nth);
+        if (only >= 0 && (only < lo || only >= hi)) continue;
+        std::mt19937 rng(nth == 1 ? seed : seed + 0x9e3779b9u * (unsigned)(t + 1));
+        for (int it = lo; it < hi; ++it) {
+            std::iota(cols.begin(), cols.end(), 0);
+            std::shuffle(cols.begin(), cols.end(), rng);
+            if (only < 0 || it == only) out.insert(out.end(), cols.begin(), cols.end());
+            if (it == only) return out;
+        }
+    }
+    return out;
+}
+
+void BzSide::apply_device_seed(unsigned key) {
+    seed_pending = false;
+    seed_perm.clear();
+    seed_perm.shrink_to_fit();
+    if (key == 0xffffffffu) return;
+    const int w = (int)(key >> 15);
+    if (w < inner) {
+        inner = w;
+        inner0 = w;
+        seed_trial = (int)((key >> 7) & 0xff);
+        seed_row = (int)(key & 0x7f);
+        best_word.clear();
+    }
+}
+
 // ------------------------------------------------------------------ side
 int BzSide::setup_host(const Problem& p, const BzOptions& opt, const char* t) {
     tag = t;
@@ -112,9 +152,19 @@ int BzSide::setup_host(const Problem& p, const BzOptions& opt, const char* t) {
     for (int g = 0; g < ng; ++g) ranks[g] = sets[g].rank;
     inner = p.seed_upper > 0 ? p.seed_upper : kWeightNone;
     if (p.seed_upper > 0) best_word = p.seed_word;
-    std::vector<u64> w;
-    const int seeded = random_is_seed(p, inner, opt.seed_trials, 0x9e3779b9u, opt.parallel_seed, &w);
-    if (seeded < inner) { inner = seeded; best_word = w; }
+    if (opt.device_seed && K <= kSeedMaxK && p.n <= kSeedMaxN && opt.seed_trials <= 256 &&
+        opt.seed_trials > 0) {
+        // the eliminations run on the GPU (setup_jobs); draw the column orders here
+        seed_pending = true;
+        seed_trials = opt.seed_trials;
+        const std::vector<int> ord = seed_orders(p.n, seed_trials, 0x9e3779b9u);
+        seed_perm.assign(ord.begin(), ord.end());
+    } else {
+        std::vector<u64> w;
+        const int seeded = random_is_seed(p, inner, opt.seed_trials, 0x9e3779b9u,
+                                          opt.parallel_seed, &w);
+        if (seeded < inner) { inner = seeded; best_word = w; }
+    }
     maxw = K;
     inner0 = inner;
     resolved0 = resolved;
@@ -160,6 +210,15 @@ void BzSide::absorb(int w, const LevelOut& o) {
 
 bool BzSide::witness(std::vector<u64>& out) const {
     if (!best_from_level) {
+        if (best_word.empty() && seed_trial >= 0) {
+            // replay the winning trial's elimination on the host
+            const std::vector<int> ord = seed_orders(prob->n, seed_trials, 0x9e3779b9u, seed_trial);
+            Mat M = prob->code_gen;
+            restricted_rref(M, ord);
+            if (seed_row >= M.rows) return false;
+            out.assign(M.row(seed_row), M.row(seed_row) + M.stride);
+            return true;
+        }
         out = best_word;
         return !out.empty();
     }
@@ -201,18 +260,37 @@ BzJob::BzJob(Problem pz, Problem px, const BzOptions& o) : pair(true), opt(o) {
     p[1] = std::move(px);
 }
 
+BzJob::BzJob(Builder build, bool is_pair, const BzOptions& o)
+    : pair(is_pair), opt(o), build_(std::move(build)) {}
+
 int BzJob::setup_host() {
     t0_ = tl_ = now_seconds();
+    if (build_) {
+        zero = build_(p[0], p[1]) == 1;
+        build_ = nullptr;
+        if (zero) {
+            done_ = true;
+            return kOk;
+        }
+    }
     const int nsides = pair ? 2 : 1;
     for (int i = 0; i < nsides; ++i) {
         const int rc = s[i].setup_host(p[i], opt, pair ? (i == 0 ? "Z" : "X") : "");
         if (rc != kOk) return rc;
     }
+    finish_setup();
+    return kOk;
+}
+
+void BzJob::finish_setup() {
+    if (zero) return;
     if (!pair) {
         done_ = !s[0].has_logicals;
         maxw_ = s[0].maxw;
         no_stop_ = opt.no_early_stop || std::getenv("DISTFIND_NO_EARLY_STOP") != nullptr;
     } else {
+        best_ = kWeightNone;
+        maxw_ = 0;
         for (int i = 0; i < 2; ++i)
             if (s[i].has_logicals) {
                 best_ = std::min(best_, s[i].inner);
@@ -220,10 +298,10 @@ int BzJob::setup_host() {
             }
         done_ = s[0].resolved && s[1].resolved;
     }
-    return kOk;
 }
 
 void BzJob::reset() {
+    if (zero) return;
     for (int i = 0; i < (pair ? 2 : 1); ++i) s[i].reset();
     w_ = 0;
     stats = RunStats();
@@ -330,6 +408,12 @@ BzResult BzJob::result() {
     r.stats = stats;
     r.trace = trace;
     r.seconds = now_seconds() - t0_;
+    if (zero) {
+        r.distance = 0;
+        r.proven = true;
+        r.witness_ok = true;
+        return r;
+    }
     if (!pair) {
         const BzSide& S = s[0];
         if (!S.has_logicals) return r;
@@ -356,6 +440,86 @@ BzResult BzJob::result() {
 }
 
 // ------------------------------------------------------------------ rounds
+cudaError_t launch_seed_trials(int W, const SeedDesc* d_descs, int ndesc, int total_trials,
+                               cudaStream_t st);
+
+// Run every pending seed trial of every job in one launch per row width, then fold the
+// per-side keys into the bounds.
+int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
+                 RunStats* stats) {
+    std::vector<BzSide*> pend[3];   // by row words W = 1, 2
+    for (BzJob* j : jobs)
+        for (int i = 0; i < (j->pair ? 2 : 1); ++i)
+            if (j->s[i].seed_pending) pend[words_for(j->s[i].prob->n)].push_back(&j->s[i]);
+    const double t0 = now_seconds();
+    bool any = false;
+    for (int W = 1; W <= 2; ++W) {
+        std::vector<BzSide*>& v = pend[W];
+        if (v.empty()) continue;
+        any = true;
+        // layout: descs | keys | per side: gen, check, perm
+        size_t off = 0;
+        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+        const size_t off_desc = off;
+        off = al(off + v.size() * sizeof(SeedDesc));
+        const size_t off_keys = off;
+        off = al(off + v.size() * 4);
+        std::vector<size_t> og(v.size()), oc(v.size()), op(v.size());
+        for (size_t i = 0; i < v.size(); ++i) {
+            const Problem& p = *v[i]->prob;
+            og[i] = off; off = al(off + (size_t)p.code_gen.rows * W * 8);
+            oc[i] = off; off = al(off + (size_t)std::max(1, p.check.rows) * W * 8);
+            op[i] = off; off = al(off + v[i]->seed_perm.size());
+        }
+        char* d = (char*)arena->alloc(off);
+        if (!d) return kErrMemory;
+        int rc = s->ensure(0, off);
+        if (rc != kOk) return rc;
+        char* h = (char*)s->h_stage.h;
+        SeedDesc* hd = (SeedDesc*)(h + off_desc);
+        unsigned* hk = (unsigned*)(h + off_keys);
+        int trials = 0;
+        for (size_t i = 0; i < v.size(); ++i) {
+            const Problem& p = *v[i]->prob;
+            u64* g = (u64*)(h + og[i]);
+            for (int r = 0; r < p.code_gen.rows; ++r)
+                for (int w = 0; w < W; ++w) g[(size_t)r * W + w] = p.code_gen.row(r)[w];
+            u64* c = (u64*)(h + oc[i]);
+            for (int r = 0; r < p.check.rows; ++r)
+                for (int w = 0; w < W; ++w) c[(size_t)r * W + w] = p.check.row(r)[w];
+            std::memcpy(h + op[i], v[i]->seed_perm.data(), v[i]->seed_perm.size());
+            SeedDesc& D = hd[i];
+            D.gen = (const unsigned long long*)(d + og[i]);
+            D.check = (const unsigned long long*)(d + oc[i]);
+            D.perm = (const uint8_t*)(d + op[i]);
+            D.key = (unsigned*)(d + off_keys) + i;
+            D.trial_base = trials;
+            D.K = p.code_gen.rows;
+            D.n = p.n;
+            D.kcheck = p.count_all ? 0 : p.check.rows;
+            D.count_all = p.count_all ? 1 : 0;
+            D.init_best = v[i]->inner;
+            hk[i] = 0xffffffffu;
+            trials += v[i]->seed_trials;
+        }
+        if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+            launch_seed_trials(W, (const SeedDesc*)(d + off_desc), (int)v.size(), trials,
+                               s->stream) != cudaSuccess ||
+            cudaMemcpyAsync(h + off_keys, d + off_keys, v.size() * 4, cudaMemcpyDeviceToHost,
+                            s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return kErrDevice;
+        }
+        for (size_t i = 0; i < v.size(); ++i) v[i]->apply_device_seed(hk[i]);
+        if (stats) stats->launches += 1;
+    }
+    if (any)
+        for (BzJob* j : jobs) j->finish_setup();
+    if (stats) stats->device_seed_s += now_seconds() - t0;
+    return kOk;
+}
+
 int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
                int host_threads, RunStats* stats) {
     const double th0 = now_seconds();
@@ -380,11 +544,14 @@ int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
     }
     if (err.load() != kOk) return err.load();
     if (stats) stats->host_setup_s += now_seconds() - th0;
+    int rc = device_seeds(dev, s, arena, jobs, stats);
+    if (rc != kOk) return rc;
     std::vector<SideDev*> sides;
     for (BzJob* j : jobs)
         for (SideDev* sd : j->device_sides()) sides.push_back(sd);
     return upload_sides(dev, s, arena, sides);
 }
+
 
 int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* rounds,
                double* span_ms) {

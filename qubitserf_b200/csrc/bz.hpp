@@ -12,6 +12,7 @@
 // the sequential Z-then-X order would have stepped X (capped levels are discarded), which
 // leaves every reported number identical to the sequential schedule.
 #pragma once
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -26,7 +27,8 @@ struct BzOptions {
     bool verbose = false;
     bool no_early_stop = false;  // enumerate every level up to K (single sides; count parity)
     int seed_trials = 256;
-    bool parallel_seed = true;   // seed trials on hardware_concurrency threads (plain path)
+    bool parallel_seed = true;   // host seed trials on hardware_concurrency threads
+    bool device_seed = true;     // eliminations of the seed trials on the GPU when K, n <= 128
 };
 
 // One enumerated level, for the per-(information set, w) count record.
@@ -57,6 +59,10 @@ struct BzResult {
 int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, bool parallel,
                    std::vector<u64>* word);
 
+// The column orders of those trials (trials x n, trial-major), drawn exactly as the
+// reference draws them; `only` >= 0 returns just that trial's order.
+std::vector<int> seed_orders(int n, int trials, unsigned seed, int only = -1);
+
 // One BZ subproblem stepped level by level.
 class BzSide {
 public:
@@ -82,10 +88,16 @@ public:
     int outer_at(int w) const;
     void absorb(int w, const LevelOut& o);
     bool witness(std::vector<u64>& out) const;
-    // state right after setup_host (for re-execution)
+    // state right after setup (for re-execution)
     int inner0 = kWeightNone;
     bool resolved0 = false;
     void reset();
+    // device-seed bookkeeping: trials pending on the GPU, and the winning (trial, row)
+    bool seed_pending = false;
+    int seed_trials = 0;
+    int seed_trial = -1, seed_row = -1;
+    std::vector<uint8_t> seed_perm;   // trials x n, released after upload
+    void apply_device_seed(unsigned key);
 };
 
 class BzJob {
@@ -93,10 +105,17 @@ public:
     // Single subproblem, or (pair=true) the interleaved min over two.
     BzJob(Problem p0, const BzOptions& opt);
     BzJob(Problem pz, Problem px, const BzOptions& opt);
+    // Deferred construction: `build` fills p[0] (and p[1] for a pair) inside setup_host, on
+    // the worker thread; returning 1 marks a certificate that is trivially 0 (an operator
+    // already in the group) and needs no enumeration.
+    using Builder = std::function<int(Problem& p0, Problem& p1)>;
+    BzJob(Builder build, bool pair, const BzOptions& opt);
+    bool zero = false;                      // trivially weight 0 (see Builder)
     BzJob(const BzJob&) = delete;
     BzJob& operator=(const BzJob&) = delete;
 
     int setup_host();                       // information sets, seeds, packed rows
+    void finish_setup();                    // after the (device) seeds are in
     std::vector<SideDev*> device_sides();   // sides that need device data
     // Level requests of this round (w = next level); side index per request.
     void requests(std::vector<LevelReq>& q, std::vector<int>& side);
@@ -114,6 +133,7 @@ public:
     std::vector<LevelRecord> trace;
 
 private:
+    Builder build_;
     int w_ = 0;                // last stepped level
     int maxw_ = 0;
     int best_ = kWeightNone;   // pair: best distance found so far

@@ -174,6 +174,7 @@ struct QsfbBatchHandle {
     std::unique_ptr<Arena> arena;
     std::unique_ptr<SessionLease> lease;
     RunStats setup;
+    double prepare_s = 0.0;
     bool executed = false;
     ~QsfbBatchHandle() {
         jobs.clear();
@@ -451,6 +452,7 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
                        QsfbBatchHandle** handle) {
     if ((!queries && nq > 0) || !handle) return kErrNull;
     *handle = nullptr;
+    const double tp0 = now_seconds();
     int rc = kOk;
     Device* dev = device_or(&rc);
     if (!dev) return rc;
@@ -461,33 +463,52 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
     BzOptions opt;
     opt.parallel_seed = false;   // the batch parallelizes over codes instead
     auto& jobs = H->jobs;
+    // Problems are built inside the parallel job setup (deferred builders); the query's
+    // host matrices only need to live until prepare returns.
     for (int i = 0; i < nq; ++i) {
-        const QsfbQuery& q = queries[i];
+        const QsfbQuery q = queries[i];
         H->kinds[i] = q.kind;
-        if (!q.A || (q.kind != 0 && !q.B)) { delete H; return kErrNull; }
-        Mat A = from_dense(q.A, q.a_rows, q.a_cols);
+        if (!q.A || (q.kind != 0 && !q.B) || (q.kind == 2 && (!q.z_op || !q.x_op))) {
+            delete H;
+            return kErrNull;
+        }
+        if (q.kind < 0 || q.kind > 2) { delete H; return kErrShape; }
         auto& m = H->map[i];
         if (q.kind == 0) {
             m.job0 = (int)jobs.size();
-            jobs.emplace_back(new BzJob(classical_problem(A), opt));
+            jobs.emplace_back(new BzJob([q](Problem& p0, Problem&) {
+                p0 = classical_problem(from_dense(q.A, q.a_rows, q.a_cols));
+                return 0;
+            }, false, opt));
         } else if (q.kind == 1) {
-            Mat B = from_dense(q.B, q.b_rows, q.b_cols);
             m.job0 = (int)jobs.size();
-            if (q.which == 'Z' || q.which == 'X')
-                jobs.emplace_back(new BzJob(css_problem(A, B, q.which), opt));
-            else
-                jobs.emplace_back(new BzJob(css_problem(A, B, 'Z'), css_problem(A, B, 'X'), opt));
-        } else if (q.kind == 2) {
-            if (!q.z_op || !q.x_op) { delete H; return kErrNull; }
-            Mat B = from_dense(q.B, q.b_rows, q.b_cols);
-            // Z part modulo rowspace(Gz), X part modulo rowspace(Gx) (op_weight.cpp:22-41)
-            if (in_rowspace(B, q.z_op)) m.zw = 0;
-            else { m.job0 = (int)jobs.size(); jobs.emplace_back(new BzJob(coset_problem(B, q.z_op), opt)); }
-            if (in_rowspace(A, q.x_op)) m.xw = 0;
-            else { m.job1 = (int)jobs.size(); jobs.emplace_back(new BzJob(coset_problem(A, q.x_op), opt)); }
+            const bool single = q.which == 'Z' || q.which == 'X';
+            jobs.emplace_back(new BzJob([q, single](Problem& p0, Problem& p1) {
+                Mat A = from_dense(q.A, q.a_rows, q.a_cols), B = from_dense(q.B, q.b_rows, q.b_cols);
+                if (single) {
+                    p0 = css_problem(A, B, q.which);
+                } else {
+                    p0 = css_problem(A, B, 'Z');
+                    p1 = css_problem(A, B, 'X');
+                }
+                return 0;
+            }, !single, opt));
         } else {
-            delete H;
-            return kErrShape;
+            // Z part modulo rowspace(Gz), X part modulo rowspace(Gx) (op_weight.cpp:22-41)
+            m.job0 = (int)jobs.size();
+            jobs.emplace_back(new BzJob([q](Problem& p0, Problem&) {
+                Mat B = from_dense(q.B, q.b_rows, q.b_cols);
+                if (in_rowspace(B, q.z_op)) return 1;
+                p0 = coset_problem(B, q.z_op);
+                return 0;
+            }, false, opt));
+            m.job1 = (int)jobs.size();
+            jobs.emplace_back(new BzJob([q](Problem& p0, Problem&) {
+                Mat A = from_dense(q.A, q.a_rows, q.a_cols);
+                if (in_rowspace(A, q.x_op)) return 1;
+                p0 = coset_problem(A, q.x_op);
+                return 0;
+            }, false, opt));
         }
     }
     for (auto& j : jobs) H->ptrs.push_back(j.get());
@@ -496,6 +517,7 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
     H->arena.reset(new Arena(dev));
     rc = setup_jobs(dev, H->lease->s, H->arena.get(), H->ptrs, host_threads, &H->setup);
     if (rc != kOk) { delete H; return rc; }
+    H->prepare_s = now_seconds() - tp0;
     *handle = H;
     return kOk;
 }
@@ -540,7 +562,9 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
     }
     if (stats) {
         stats->seconds = now_seconds() - t0;
+        stats->prepare_seconds = H->prepare_s;
         stats->host_setup_seconds = H->setup.host_setup_s;
+        stats->device_seed_seconds = H->setup.device_seed_s;
         stats->device_ms = rs.ms_gen + rs.ms_pairs;
         stats->device_span_ms = span;
         stats->pair_ms = rs.ms_pairs;

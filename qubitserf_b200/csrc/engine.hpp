@@ -177,6 +177,7 @@ struct RunStats {
     unsigned long long codewords = 0;
     int launches = 0;
     double host_setup_s = 0.0;
+    double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)
 };
 
 // Enumerate every request; blocking.  Returns a Status.
