@@ -195,6 +195,37 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
 int qsfb_batch_execute(QsfbBatchHandle* handle, QsfbAnswer* out, QsfbBatchStats* stats);
 void qsfb_batch_free(QsfbBatchHandle* handle);
 
+/* ---- serving: continuous batching of queries that arrive over time (no reference
+ * counterpart).  submit() copies the query and returns at once; intake workers reduce it,
+ * run its seed eliminations and upload its rows on their own CUDA streams while the device
+ * keeps enumerating; an engine thread admits ready queries at every round boundary while
+ * at most max_active are in flight and their summed device footprint (rows + all subset
+ * lists their levels will build) stays within mem_budget_bytes (0 = 64 GiB), runs one
+ * fused round over all admitted queries' next levels, and completes each query as soon as
+ * it is proven.  Answers equal qsfb_batch's for the same query, alone or in any mix. */
+typedef struct QsfbServer QsfbServer;
+typedef struct {
+    double submit_s, ready_s, admit_s, done_s;   /* seconds since the server started */
+    double latency_s;                             /* done - submit */
+} QsfbTiming;
+typedef struct {
+    long long submitted, completed;
+    int active, pending;
+    double busy_s;                 /* wall time spent in enumeration rounds */
+    unsigned long long codewords;
+    int rounds;
+    long long peak_footprint_bytes;
+    double elapsed_s;
+} QsfbServeStats;
+int qsfb_server_start(int intake_threads, long long mem_budget_bytes, int max_active,
+                      QsfbServer** server);
+int qsfb_server_submit(QsfbServer* server, const QsfbQuery* query, long long* ticket);
+/* Blocks until the ticket's answer is ready; returns its status (0 ok). */
+int qsfb_server_wait(QsfbServer* server, long long ticket, QsfbAnswer* out, QsfbTiming* timing);
+int qsfb_server_stats(QsfbServer* server, QsfbServeStats* out);
+/* Stops the threads (call after every submitted ticket has been waited for). */
+int qsfb_server_stop(QsfbServer* server);
+
 /* No counterpart in the reference.  qsfb_enumerate_plan for callers that cannot allocate
  * device memory (a process whose own pool owns the device, or code that must not cause the
  * device-wide synchronisation of a cudaMalloc).  Inputs and outputs are DEVICE pointers

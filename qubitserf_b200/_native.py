@@ -74,6 +74,20 @@ class QsfbBatchStats(ctypes.Structure):
                 ("certificates", ctypes.c_int)]
 
 
+class QsfbTiming(ctypes.Structure):
+    _fields_ = [("submit_s", ctypes.c_double), ("ready_s", ctypes.c_double),
+                ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("latency_s", ctypes.c_double)]
+
+
+class QsfbServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("active", ctypes.c_int), ("pending", ctypes.c_int),
+                ("busy_s", ctypes.c_double), ("codewords", ctypes.c_ulonglong),
+                ("rounds", ctypes.c_int), ("peak_footprint_bytes", ctypes.c_longlong),
+                ("elapsed_s", ctypes.c_double)]
+
+
 # (name, restype, argtypes) of every exported function; tests check the export list.
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -109,6 +123,13 @@ SIGNATURES = [
     ("qsfb_enumerate_plan_noalloc", _i, [_i, _i, _i, _i, _i, ctypes.c_void_p, _i,
                                          ctypes.c_void_p, _i, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("qsfb_server_start", _i, [_i, ctypes.c_longlong, _i, ctypes.POINTER(ctypes.c_void_p)]),
+    ("qsfb_server_submit", _i, [ctypes.c_void_p, ctypes.POINTER(QsfbQuery),
+                                ctypes.POINTER(ctypes.c_longlong)]),
+    ("qsfb_server_wait", _i, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(QsfbAnswer),
+                              ctypes.POINTER(QsfbTiming)]),
+    ("qsfb_server_stats", _i, [ctypes.c_void_p, ctypes.POINTER(QsfbServeStats)]),
+    ("qsfb_server_stop", _i, [ctypes.c_void_p]),
     ("qsfb_flush_l2", _i, []),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
@@ -392,3 +413,45 @@ def batch_items(codes):
         else:
             items.append(("opweight",) + tuple(cs.mats))
     return items
+
+
+def make_query(item):
+    """One QsfbQuery (plus the arrays it points into) from a Batch-style item."""
+    b = Batch([item])
+    return b.q[0], b._keep
+
+
+class Server:
+    """Continuous-batching server (qsfb_server_*): submit() returns a ticket at once,
+    wait() blocks for that ticket's answer and timing."""
+
+    def __init__(self, intake_threads=0, mem_budget_bytes=0, max_active=0):
+        self.h = ctypes.c_void_p()
+        _check(lib().qsfb_server_start(int(intake_threads), int(mem_budget_bytes),
+                                       int(max_active), ctypes.byref(self.h)), "qsfb_server_start")
+
+    def submit(self, item):
+        q, keep = make_query(item)
+        t = ctypes.c_longlong()
+        _check(lib().qsfb_server_submit(self.h, ctypes.byref(q), ctypes.byref(t)),
+               "qsfb_server_submit")
+        del keep   # the server copied the matrices
+        return t.value
+
+    def wait(self, ticket):
+        a = QsfbAnswer()
+        tm = QsfbTiming()
+        _check(lib().qsfb_server_wait(self.h, ticket, ctypes.byref(a), ctypes.byref(tm)),
+               "qsfb_server_wait")
+        return a, tm
+
+    def stats(self):
+        st = QsfbServeStats()
+        lib().qsfb_server_stats(self.h, ctypes.byref(st))
+        return st
+
+    def stop(self):
+        if self.h:
+            rc = lib().qsfb_server_stop(self.h)
+            self.h = ctypes.c_void_p()
+            _check(rc, "qsfb_server_stop")
