@@ -63,7 +63,8 @@ def run_stream(reqs, intake_threads=0, mem_budget_bytes=64 << 30, max_active=0,
         "p99_ms": float(np.percentile(lat, 99) * 1e3),
         "max_ms": float(lat.max() * 1e3),
         "certs_per_s": len(reqs) / max(last - first, 1e-9),
-        "offered_rate": len(reqs) / max(reqs[-1].t - reqs[0].t, 1e-9) / time_scale,
+        "offered_rate": (len(reqs) / max(reqs[-1].t - reqs[0].t, 1e-9) / time_scale
+                         if time_scale > 0 else float("inf")),
         "rounds": st.rounds,
         "busy_s": st.busy_s,
         "span_s": last - first,
