@@ -89,33 +89,18 @@ class ClockSampler:
 
 
 def dist_setup(gpus):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        os.environ["QSFB_DEVICE"] = str(local)
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-        pg = dist
-    else:
-        os.environ.setdefault("QSFB_DEVICE", "0")
-    return rank, world, local, pg
+    from qubitserf_b200 import dist
+    return dist.init_from_env()
 
 
 def max_over_ranks(pg, x):
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    from qubitserf_b200 import dist
+    return dist.max_over_ranks(pg, x)
 
 
 def barrier(pg):
-    if pg is not None:
-        pg.barrier()
+    from qubitserf_b200 import dist
+    dist.barrier(pg)
 
 
 def run_plain(native, codes):
@@ -185,6 +170,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--codes", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=15.0,
+                    help="seconds of reference CPU work per reference-arm step")
     ap.add_argument("--only-resident", action="store_true",
                     help="time only the resident-input rounds (profiling runs)")
     ap.add_argument("--workload", default="batch",
@@ -216,10 +203,10 @@ def main():
         if rank != 0:
             return
         for _ in range(args.warmup):
-            cpu_baseline_sample(codes, budget_s=0.5)
+            cpu_baseline_sample(codes, budget_s=min(0.5, args.ref_budget))
         vals, b = [], None
         for k in range(args.steps):
-            b = cpu_baseline_sample(codes, budget_s=15.0, start=2 * k)
+            b = cpu_baseline_sample(codes, budget_s=args.ref_budget, start=2 * k)
             vals.append(b["value"])
         v = float(np.mean(vals))
         line = {"metric": METRIC, "value": v, "unit": "certs/s", "n_gpus": args.gpus,
