@@ -176,6 +176,8 @@ typedef struct {
     double device_span_ms;       /* CUDA-event span of all rounds, host gaps included */
     double pair_ms;              /* pair-sweep kernel time alone */
     unsigned long long codewords;
+    unsigned long long popc_issued;     /* POPC issued by the pair kernels */
+    unsigned long long zero_codewords;  /* codewords swept by the popcount-free zero test */
     int rounds;
     int kernel_launches;
     int certificates;            /* BZ runs executed (a CSS 'M' query is one) */
@@ -243,6 +245,10 @@ int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int num_gamma,
                                 int current_best, int* d_out_best,
                                 unsigned long long* d_out_counts, int* d_out_g,
                                 unsigned long long* d_out_rank, void* stream);
+
+/* Measured integer-pipe peak (ops/s over the whole device): which = 0 for 32-bit POPC
+ * (the XU pipe), 1 for LOP3 (the ALU pipe).  Roofline denominators of the pair kernel. */
+int qsfb_microbench(int which, double* ops_per_s);
 
 /* Overwrite a 256 MiB device buffer (more than the 126 MB L2) and wait; benchmarks call it
  * between timed steps.  Returns 0, or 4 without a device. */

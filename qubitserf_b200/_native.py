@@ -70,6 +70,7 @@ class QsfbBatchStats(ctypes.Structure):
                 ("host_setup_seconds", ctypes.c_double), ("device_seed_seconds", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("device_span_ms", ctypes.c_double),
                 ("pair_ms", ctypes.c_double), ("codewords", ctypes.c_ulonglong),
+                ("popc_issued", ctypes.c_ulonglong), ("zero_codewords", ctypes.c_ulonglong),
                 ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("certificates", ctypes.c_int)]
 
@@ -130,6 +131,7 @@ SIGNATURES = [
                               ctypes.POINTER(QsfbTiming)]),
     ("qsfb_server_stats", _i, [ctypes.c_void_p, ctypes.POINTER(QsfbServeStats)]),
     ("qsfb_server_stop", _i, [ctypes.c_void_p]),
+    ("qsfb_microbench", _i, [_i, ctypes.POINTER(ctypes.c_double)]),
     ("qsfb_flush_l2", _i, []),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
@@ -455,3 +457,10 @@ class Server:
             rc = lib().qsfb_server_stop(self.h)
             self.h = ctypes.c_void_p()
             _check(rc, "qsfb_server_stop")
+
+
+def microbench(which):
+    """Measured device-wide ops/s: 0 = POPC (XU pipe), 1 = LOP3 (ALU pipe)."""
+    v = ctypes.c_double()
+    _check(lib().qsfb_microbench(int(which), ctypes.byref(v)), "qsfb_microbench")
+    return v.value

@@ -605,6 +605,8 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             stats->ms_pairs += rs.ms_pairs;
             stats->jobs += rs.jobs;
             stats->codewords += rs.codewords;
+            stats->popc_issued += rs.popc_issued;
+            stats->zero_codewords += rs.zero_codewords;
             stats->launches += rs.launches;
         }
         if (jobs.size() == 1) {

@@ -16,6 +16,11 @@
 
 using namespace qsfb;
 
+namespace qsfb {
+cudaError_t microbench_peak(int which, int num_sms, uint32_t* d_out, cudaStream_t st,
+                            double* ops_per_s);
+}
+
 namespace {
 
 struct LastCall {
@@ -569,6 +574,8 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
         stats->device_span_ms = span;
         stats->pair_ms = rs.ms_pairs;
         stats->codewords = rs.codewords;
+        stats->popc_issued = rs.popc_issued;
+        stats->zero_codewords = rs.zero_codewords;
         stats->rounds = rounds;
         stats->kernel_launches = rs.launches;
         stats->certificates = (int)jobs.size();
@@ -588,6 +595,21 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     qsfb_batch_free(H);
     if (stats) stats->seconds = now_seconds() - t0;
     return rc;
+}
+
+int qsfb_microbench(int which, double* ops_per_s) {
+    if (!ops_per_s) return kErrNull;
+    int rc = kOk;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    SessionLease lease(dev);
+    if (!lease.s) return kErrDevice;
+    void* out = dev->alloc((size_t)dev->num_sms * 8 * 4);
+    if (!out) return kErrMemory;
+    const cudaError_t e = microbench_peak(which, dev->num_sms, (uint32_t*)out, lease.s->stream,
+                                          ops_per_s);
+    dev->release(out, (size_t)dev->num_sms * 8 * 4);
+    return e == cudaSuccess ? kOk : kErrDevice;
 }
 
 int qsfb_flush_l2(void) {

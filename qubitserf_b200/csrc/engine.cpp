@@ -382,7 +382,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         }
     }
     // loop tile: enough jobs to keep every resident warp busy several times over
-    const unsigned long long want_jobs = (unsigned long long)dev->num_sms * 16 * 4;
+    // ~16 jobs per resident warp: the launch tail (one job) stays a few % of the level
+    const unsigned long long want_jobs = (unsigned long long)dev->num_sms * 24 * 16;
     unsigned long long lt = total_pairs / ((unsigned long long)kRegTile * want_jobs);
     lt = std::max<unsigned long long>(32, std::min<unsigned long long>(1024, lt));
     const int loop_tile = (int)((lt + 31) / 32 * 32);
@@ -588,10 +589,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             O.rank = k & kKeyRankMask;
         }
     }
+    unsigned long long popc = 0, zcw = 0;
     for (size_t oi = 0; oi < order.size(); ++oi) {
         const Plan& P = plans[order[oi]];
         outs[P.req].counts[P.g] = hcounts[order[oi]];
         cw += hcounts[order[oi]];
+        if (P.mode == 2) zcw += hcounts[order[oi]];
+        else popc += hcounts[order[oi]] * (unsigned long long)P.H;
         const LevelDesc& D = hl[oi];
         if (outs[P.req].found && outs[P.req].g == P.g) outs[P.req].rank_shift = D.rank_shift;
     }
@@ -603,6 +607,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         stats->ms_pairs += b;
         stats->jobs += all_jobs;
         stats->codewords += cw;
+        stats->popc_issued += popc;
+        stats->zero_codewords += zcw;
         stats->launches += launches;
     }
     cudaEventDestroy(evm);

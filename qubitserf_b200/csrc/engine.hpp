@@ -175,6 +175,8 @@ struct RunStats {
     double ms_pairs = 0.0;   // device time of the pair sweep
     unsigned long long jobs = 0;
     unsigned long long codewords = 0;
+    unsigned long long popc_issued = 0;    // POPC the pair kernels issue (H per pair, 0 in zero mode)
+    unsigned long long zero_codewords = 0; // codewords swept by the zero-test mode
     int launches = 0;
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)

@@ -8,7 +8,8 @@ Runs only where the reference CPU library has been built from its sources
                   no-early-stop cases the reference's per-level (w, active, work) trace
                   read from its DISTFIND_PROFILE lines (cpp/distfind/bz.cpp:193-201)
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # golden.npz + golden.json
+    python tests/golden/make_golden.py --batch1024  # batch1024.json (all 1024 batch codes)
 """
 from __future__ import annotations
 
@@ -136,8 +137,27 @@ def count_trace(name):
     return levels
 
 
+def batch1024():
+    """Reference distance / levels / lower bound / proven for all 1024 batch codes (the
+    reference run on this host; levels depend on its core count through the seed streams)."""
+    from oracle.refbind import Ref
+    import time
+    ref = Ref()
+    out = []
+    t0 = time.perf_counter()
+    for c in W.batch_1024():
+        r = ref.classical(c.mats[0]) if c.kind == "classical" else ref.css(*c.mats)
+        out.append([int(r.distance), int(r.levels), int(r.lower_bound), int(r.proven)])
+    meta = {"host_cores": os.cpu_count(), "seconds": time.perf_counter() - t0,
+            "fields": ["distance", "levels", "lower_bound", "proven"]}
+    (HERE / "batch1024.json").write_text(json.dumps({"meta": meta, "codes": out}))
+
+
 def main():
     sys.path.insert(0, str(ROOT))
+    if "--batch1024" in sys.argv:
+        batch1024()
+        return
     arrays = {}
     results = {}
     for name, kind, mats, extra in cases():

@@ -80,3 +80,24 @@ def test_prepare_execute_repeatable(native):
     assert s2.device_span_ms > 0 and s2.pair_ms > 0
     a3, _ = b.run()
     assert [(a.distance, a.levels) for a in a3] == [x[:2] for x in d1]
+
+
+def test_full_1024_batch_matches_reference(native):
+    """All 1024 codes of the benchmark batch against the reference's own results
+    (tests/golden/batch1024.json, made by make_golden.py --batch1024)."""
+    import json
+    import os
+    from conftest import GOLDEN_DIR
+    from qubitserf_b200 import workloads as W
+    g = json.loads((GOLDEN_DIR / "batch1024.json").read_text())
+    codes = W.batch_1024()
+    ans, st = native.Batch(native.batch_items(codes)).run()
+    same_host = g["meta"]["host_cores"] == os.cpu_count()
+    bad = []
+    for i, (a, r) in enumerate(zip(ans, g["codes"])):
+        if a.distance != r[0] or a.proven != r[3] or not a.witness_ok:
+            bad.append((i, a.distance, r[0]))
+        if same_host and (a.levels, a.lower_bound) != (r[1], r[2]):
+            bad.append((i, "levels", a.levels, r[1]))
+    assert not bad, bad[:10]
+    assert st.certificates == 1024
