@@ -265,7 +265,8 @@ def main():
             print(json.dumps({"workload": wname, "certs_per_s": value,
                               "ms_per_step": span_s / args.steps * 1000.0,
                               "gcodewords_per_s": cw / max(pair_ms / 1000.0, 1e-12) / 1e9,
-                              "rounds": rounds, "launches": launches}), flush=True)
+                              "rounds": rounds, "launches": launches,
+                              "device_mb": st.device_bytes / 2**20}), flush=True)
         return
 
     # --- end to end: the one-shot public call from host matrices, K times

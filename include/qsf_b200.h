@@ -181,6 +181,7 @@ typedef struct {
     int rounds;
     int kernel_launches;
     int certificates;            /* BZ runs executed (a CSS 'M' query is one) */
+    long long device_bytes;      /* device memory held by the batch (rows, seeds, lists) */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free. */

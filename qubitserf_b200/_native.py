@@ -72,7 +72,7 @@ class QsfbBatchStats(ctypes.Structure):
                 ("pair_ms", ctypes.c_double), ("codewords", ctypes.c_ulonglong),
                 ("popc_issued", ctypes.c_ulonglong), ("zero_codewords", ctypes.c_ulonglong),
                 ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),
-                ("certificates", ctypes.c_int)]
+                ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong)]
 
 
 class QsfbTiming(ctypes.Structure):

@@ -579,6 +579,7 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
         stats->rounds = rounds;
         stats->kernel_launches = rs.launches;
         stats->certificates = (int)jobs.size();
+        stats->device_bytes = (long long)H->arena->bytes();
     }
     return kOk;
 }
