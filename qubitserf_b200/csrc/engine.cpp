@@ -85,6 +85,9 @@ unsigned long long Device::binom(int n, int k) const {
 }
 
 void* Device::alloc(size_t bytes) {
+    // Host-side fault injection for tests: QSFB_FAIL_ALLOC makes every allocation fail
+    // (cached blocks included), so callers exercise their out-of-memory paths.
+    if (std::getenv("QSFB_FAIL_ALLOC") != nullptr) return nullptr;
     const size_t b = round_bucket(bytes);
     {
         std::lock_guard<std::mutex> lk(mu_);
