@@ -132,9 +132,9 @@ int css_like(Device* dev, const Mat& A, const Mat& B, bool subsystem, char which
         if (rc == kOk) rc = bz_distance(dev, px, options(verbose), rx);
         if (rc == kOk) r = min_of(rz, rx);
     } else {
-        Problem pz = prob('Z'), px = prob('X');
-        nbits = pz.n;
-        rc = bz_min_interleaved(dev, pz, px, options(verbose), r);
+        auto pr = css_problem_pair(A, B);
+        nbits = pr.first.n;
+        rc = bz_min_interleaved(dev, pr.first, pr.second, options(verbose), r);
     }
     if (rc != kOk) return rc;
     fill(out, r);
@@ -493,8 +493,9 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
                 if (single) {
                     p0 = css_problem(A, B, q.which);
                 } else {
-                    p0 = css_problem(A, B, 'Z');
-                    p1 = css_problem(A, B, 'X');
+                    auto pr = css_problem_pair(A, B);
+                    p0 = std::move(pr.first);
+                    p1 = std::move(pr.second);
                 }
                 return 0;
             }, !single, opt));

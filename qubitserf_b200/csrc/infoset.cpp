@@ -36,62 +36,70 @@ std::vector<InfoSet> greedy_sets(const Mat& code_gen) {
     return seq;
 }
 
-// Sorted-list symmetric difference.
-std::vector<int> symdiff(const std::vector<int>& a, const std::vector<int>& b) {
-    std::vector<int> r;
-    r.reserve(a.size() + b.size());
-    std::set_symmetric_difference(a.begin(), a.end(), b.begin(), b.end(),
-                                  std::back_inserter(r));
-    return r;
-}
-
 // Express column z over the independent class `cls`: (in_span, circuit) where circuit is
 // the ascending list of class columns whose XOR is z (cpp/distfind/css.cpp:316-351).
+// Origins are kept as bitsets over the columns, so the reference's sorted-list symmetric
+// difference becomes an XOR and the circuit is read out in ascending order.
 struct Expr {
     bool in_span;
     std::vector<int> circuit;
 };
 
-Expr express(const std::vector<int>& cls, const std::vector<u64>& col, int kw, int z) {
-    std::vector<std::vector<u64>> basis;
+struct Expresser {
+    int kw = 0, nw = 0;
+    std::vector<u64> bv, bo;      // basis vectors (kw words) and origins (nw words)
     std::vector<int> bpiv;
-    std::vector<std::vector<int>> borig;
-    auto low = [&](const std::vector<u64>& v) {
-        for (int w = 0; w < kw; ++w)
-            if (v[w]) return w * 64 + __builtin_ctzll(v[w]);
-        return -1;
-    };
-    for (int idx : cls) {
-        std::vector<u64> v(col.begin() + (size_t)idx * kw, col.begin() + (size_t)idx * kw + kw);
-        std::vector<int> orig{idx};
-        for (size_t b = 0; b < basis.size(); ++b) {
-            const int p = bpiv[b];
-            if ((v[p >> 6] >> (p & 63)) & 1u) {
-                for (int w = 0; w < kw; ++w) v[w] ^= basis[b][w];
-                orig = symdiff(orig, borig[b]);
+    std::vector<u64> v, o;
+    Expresser(int kw_, int n) : kw(kw_), nw(words_for(n)) {}
+
+    Expr operator()(const std::vector<int>& cls, const std::vector<u64>& col, int z,
+                    bool want_circuit) {
+        const size_t cap = cls.size() + 1;
+        if (bpiv.size() < cap) {
+            bv.resize(cap * kw);
+            bo.resize(cap * nw);
+            bpiv.resize(cap);
+        }
+        v.assign(kw, 0);
+        o.assign(nw, 0);
+        int nb = 0;
+        auto reduce = [&]() {
+            for (int b = 0; b < nb; ++b) {
+                const int p = bpiv[b];
+                if ((v[p >> 6] >> (p & 63)) & 1u) {
+                    for (int w = 0; w < kw; ++w) v[w] ^= bv[(size_t)b * kw + w];
+                    for (int w = 0; w < nw; ++w) o[w] ^= bo[(size_t)b * nw + w];
+                }
+            }
+        };
+        for (int idx : cls) {
+            for (int w = 0; w < kw; ++w) v[w] = col[(size_t)idx * kw + w];
+            std::fill(o.begin(), o.end(), 0);
+            o[idx >> 6] |= 1ull << (idx & 63);
+            reduce();
+            int lb = -1;
+            for (int w = 0; w < kw; ++w)
+                if (v[w]) { lb = w * 64 + __builtin_ctzll(v[w]); break; }
+            if (lb >= 0) {
+                for (int w = 0; w < kw; ++w) bv[(size_t)nb * kw + w] = v[w];
+                for (int w = 0; w < nw; ++w) bo[(size_t)nb * nw + w] = o[w];
+                bpiv[nb] = lb;
+                ++nb;
             }
         }
-        const int lb = low(v);
-        if (lb >= 0) {
-            basis.push_back(v);
-            bpiv.push_back(lb);
-            borig.push_back(orig);
-        }
+        for (int w = 0; w < kw; ++w) v[w] = col[(size_t)z * kw + w];
+        std::fill(o.begin(), o.end(), 0);
+        reduce();
+        bool zero = true;
+        for (int w = 0; w < kw; ++w)
+            if (v[w]) { zero = false; break; }
+        Expr e{zero, {}};
+        if (zero && want_circuit)
+            for (int w = 0; w < nw; ++w)
+                for (u64 x = o[w]; x; x &= x - 1) e.circuit.push_back(w * 64 + __builtin_ctzll(x));
+        return e;
     }
-    std::vector<u64> v(col.begin() + (size_t)z * kw, col.begin() + (size_t)z * kw + kw);
-    std::vector<int> orig;
-    for (size_t b = 0; b < basis.size(); ++b) {
-        const int p = bpiv[b];
-        if ((v[p >> 6] >> (p & 63)) & 1u) {
-            for (int w = 0; w < kw; ++w) v[w] ^= basis[b][w];
-            orig = symdiff(orig, borig[b]);
-        }
-    }
-    bool zero = true;
-    for (int w = 0; w < kw; ++w)
-        if (v[w]) { zero = false; break; }
-    return {zero, zero ? orig : std::vector<int>{}};
-}
+};
 
 // cpp/distfind/css.cpp:355-409
 bool matroid_partition(const Mat& code_gen, std::vector<std::vector<int>>& out) {
@@ -107,14 +115,15 @@ bool matroid_partition(const Mat& code_gen, std::vector<std::vector<int>>& out) 
     }
     std::vector<std::vector<int>> cls;
     std::vector<char> visited(n, 0);
+    Expresser express(kw, n);
     std::function<bool(int, int)> place = [&](int z, int forbidden) -> bool {
         for (int c = 0; c < (int)cls.size(); ++c) {
             if (c == forbidden) continue;
-            if (!express(cls[c], col, kw, z).in_span) { cls[c].push_back(z); return true; }
+            if (!express(cls[c], col, z, false).in_span) { cls[c].push_back(z); return true; }
         }
         for (int c = 0; c < (int)cls.size(); ++c) {
             if (c == forbidden) continue;
-            Expr e = express(cls[c], col, kw, z);
+            Expr e = express(cls[c], col, z, true);
             if (!e.in_span) continue;
             for (int y : e.circuit) {
                 if (visited[y]) continue;

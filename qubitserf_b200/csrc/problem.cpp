@@ -89,6 +89,47 @@ std::vector<u64> pack_bytes(const u8* vec, int n) {
 
 }  // namespace
 
+namespace {
+// Rows of ko = nullspace(other) independent of rowspan(self) (cpp/distfind/css.cpp:175-186).
+Mat quotient_of(const Mat& self, const Mat& ko) {
+    Reducer basis(self.cols);
+    for (int i = 0; i < self.rows; ++i) {
+        std::vector<u64> t(self.row(i), self.row(i) + self.stride);
+        if (basis.reduce(t.data())) basis.add(t.data());
+    }
+    Mat out(0, self.cols);
+    for (int i = 0; i < ko.rows; ++i) {
+        std::vector<u64> t(ko.row(i), ko.row(i) + ko.stride);
+        if (!basis.reduce(t.data())) continue;
+        basis.add(t.data());
+        out.append_row(ko.row(i));
+    }
+    return out;
+}
+
+Problem from_parts(int n, Mat code_gen, Mat check, const Mat& logicals) {
+    Problem p;
+    p.n = n;
+    p.code_gen = std::move(code_gen);
+    p.check = std::move(check);
+    p.even = all_rows_even(p.code_gen);
+    auto mw = min_weight_row(logicals);
+    p.seed_upper = mw.first;
+    if (mw.second >= 0)
+        p.seed_word.assign(logicals.row(mw.second), logicals.row(mw.second) + logicals.stride);
+    return p;
+}
+}  // namespace
+
+std::pair<Problem, Problem> css_problem_pair(const Mat& Hx, const Mat& Hz) {
+    Mat nx = nullspace(Hx), nz = nullspace(Hz);
+    Mat qxz = quotient_of(Hx, nz);   // quotient_basis(Hx, Hz): Z detector, X logicals
+    Mat qzx = quotient_of(Hz, nx);   // quotient_basis(Hz, Hx): X detector, Z logicals
+    Problem pz = from_parts(Hx.cols, nx, qxz, qzx);
+    Problem px = from_parts(Hz.cols, nz, qzx, qxz);
+    return {std::move(pz), std::move(px)};
+}
+
 Mat quotient_basis(const Mat& self, const Mat& other) {
     Mat ko = nullspace(other);
     Reducer basis(self.cols);

@@ -29,6 +29,9 @@ struct Problem {
 Mat quotient_basis(const Mat& self, const Mat& other);
 // cpp/distfind/css.cpp:188-190 / 159-168
 Problem css_problem(const Mat& Hx, const Mat& Hz, char which);
+// Both sides of a CSS code at once: the same two problems as css_problem(·,'Z') and
+// css_problem(·,'X'), sharing the two nullspaces and the two quotient bases.
+std::pair<Problem, Problem> css_problem_pair(const Mat& Hx, const Mat& Hz);
 // cpp/distfind/css.cpp:192-201
 Problem classical_problem(const Mat& H);
 // cpp/distfind/css.cpp:203-214

@@ -121,8 +121,13 @@ struct QsfbServer {
             const bool single = q->which == 'Z' || q->which == 'X';
             r->jobs.emplace_back(new BzJob([q, single](Problem& p0, Problem& p1) {
                 Mat A = from_dense(q->A.data(), q->ar, q->ac), B = from_dense(q->B.data(), q->br, q->bc);
-                if (single) p0 = css_problem(A, B, q->which);
-                else { p0 = css_problem(A, B, 'Z'); p1 = css_problem(A, B, 'X'); }
+                if (single) {
+                    p0 = css_problem(A, B, q->which);
+                } else {
+                    auto pr = css_problem_pair(A, B);
+                    p0 = std::move(pr.first);
+                    p1 = std::move(pr.second);
+                }
                 return 0;
             }, !single, opt));
         } else {

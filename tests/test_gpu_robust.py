@@ -34,9 +34,10 @@ def test_concurrent_calls_from_host_threads(native, golden):
     names = ["toric3", "toric4", "surface4", "steane", "hamming4", "cfg_classical_96",
              "batch_2", "batch_514"]
     serial = {}
+    mats = {n: golden.mats(n) for n in names}   # npz reads are not thread-safe: load here
     for n in names:
         r = golden.results[n]
-        m = golden.mats(n)
+        m = mats[n]
         serial[n] = (native.classical_distance_raw(m[0], "bz", "gpu", 0, False).distance
                      if r["kind"] == "classical" else
                      native.css_distance_raw(m[0], m[1], "bz", "M", "gpu", 0, False).distance)
@@ -47,7 +48,7 @@ def test_concurrent_calls_from_host_threads(native, golden):
             for rep in range(3):
                 n = names[(k + rep) % len(names)]
                 r = golden.results[n]
-                m = golden.mats(n)
+                m = mats[n]
                 d = (native.classical_distance_raw(m[0], "bz", "gpu", 0, False).distance
                      if r["kind"] == "classical" else
                      native.css_distance_raw(m[0], m[1], "bz", "M", "gpu", 0, False).distance)
