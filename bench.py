@@ -266,7 +266,10 @@ def main():
                               "ms_per_step": span_s / args.steps * 1000.0,
                               "gcodewords_per_s": cw / max(pair_ms / 1000.0, 1e-12) / 1e9,
                               "rounds": rounds, "launches": launches,
-                              "device_mb": st.device_bytes / 2**20}), flush=True)
+                              "device_mb": st.device_bytes / 2**20,
+                              "pair_ms": st.pair_ms, "gen_ms": st.gen_ms,
+                              "host_plan_ms": st.host_plan_seconds * 1e3,
+                              "host_apply_ms": st.host_apply_seconds * 1e3}), flush=True)
         return
 
     # --- end to end: the one-shot public call from host matrices, K times

@@ -182,6 +182,9 @@ typedef struct {
     int kernel_launches;
     int certificates;            /* BZ runs executed (a CSS 'M' query is one) */
     long long device_bytes;      /* device memory held by the batch (rows, seeds, lists) */
+    double gen_ms;               /* list-generation kernel time */
+    double host_plan_seconds;    /* host planning of the rounds (before their launches) */
+    double host_apply_seconds;   /* host schedule updates after the rounds */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free. */

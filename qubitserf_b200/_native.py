@@ -72,7 +72,9 @@ class QsfbBatchStats(ctypes.Structure):
                 ("pair_ms", ctypes.c_double), ("codewords", ctypes.c_ulonglong),
                 ("popc_issued", ctypes.c_ulonglong), ("zero_codewords", ctypes.c_ulonglong),
                 ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),
-                ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong)]
+                ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong),
+                ("gen_ms", ctypes.c_double), ("host_plan_seconds", ctypes.c_double),
+                ("host_apply_seconds", ctypes.c_double)]
 
 
 class QsfbTiming(ctypes.Structure):

@@ -585,6 +585,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             if (rc != kOk) break;
         }
         // per-job slices (requests of one job are contiguous)
+        const double ta0 = now_seconds();
         size_t k = 0;
         for (size_t j = 0; j < jobs.size(); ++j) {
             if (jobs[j]->done()) continue;
@@ -600,7 +601,10 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             jobs[j]->stats.codewords += cw;
             jobs[j]->apply(o, sd);
         }
+        rs.host_apply_s += now_seconds() - ta0;
         if (stats) {
+            stats->host_plan_s += rs.host_plan_s;
+            stats->host_apply_s += rs.host_apply_s;
             stats->ms_gen += rs.ms_gen;
             stats->ms_pairs += rs.ms_pairs;
             stats->jobs += rs.jobs;

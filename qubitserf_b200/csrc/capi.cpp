@@ -4,6 +4,8 @@
 #include "../../include/qsf_b200.h"
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -540,6 +542,21 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
     int rc = run_rounds(H->lease->s, H->ptrs, &rs, &rounds, &span);
     if (rc != kOk) return rc;
     auto& jobs = H->jobs;
+    // Results (witness rebuild + host verification) are independent per job: spread them
+    // over the host cores.
+    std::vector<BzResult> res(jobs.size());
+    {
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (size_t k; (k = next.fetch_add(1)) < jobs.size();) res[k] = jobs[k]->result();
+        };
+        const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
+                                                  (int)jobs.size() / 8 + 1));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nth; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto& th : pool) th.join();
+    }
     for (size_t i = 0; i < H->map.size(); ++i) {
         QsfbAnswer& a = out[i];
         std::memset(&a, 0, sizeof(a));
@@ -548,8 +565,8 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
             BzResult rz, rx;
             int zw = m.zw, xw = m.xw;
             bool ok = true, proven = true;
-            if (m.job0 >= 0) { rz = jobs[m.job0]->result(); zw = rz.distance; ok &= rz.witness_ok || zw <= 0; proven &= rz.proven; }
-            if (m.job1 >= 0) { rx = jobs[m.job1]->result(); xw = rx.distance; ok &= rx.witness_ok || xw <= 0; proven &= rx.proven; }
+            if (m.job0 >= 0) { rz = res[m.job0]; zw = rz.distance; ok &= rz.witness_ok || zw <= 0; proven &= rz.proven; }
+            if (m.job1 >= 0) { rx = res[m.job1]; xw = rx.distance; ok &= rx.witness_ok || xw <= 0; proven &= rx.proven; }
             a.z_weight = zw;
             a.x_weight = xw;
             a.distance = std::max(zw, xw);
@@ -557,7 +574,7 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
             a.witness_ok = ok ? 1 : 0;
             a.levels = std::max(m.job0 >= 0 ? rz.levels : 0, m.job1 >= 0 ? rx.levels : 0);
         } else {
-            BzResult r = jobs[m.job0]->result();
+            const BzResult& r = res[m.job0];
             a.distance = r.distance;
             a.lower_bound = r.lower_bound;
             a.proven = r.proven ? 1 : 0;
@@ -581,6 +598,9 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
         stats->kernel_launches = rs.launches;
         stats->certificates = (int)jobs.size();
         stats->device_bytes = (long long)H->arena->bytes();
+        stats->gen_ms = rs.ms_gen;
+        stats->host_plan_seconds = rs.host_plan_s;
+        stats->host_apply_seconds = rs.host_apply_s;
     }
     return kOk;
 }

@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -342,6 +343,7 @@ unsigned long long level_pairs(const Device* dev, int K, int w) { return dev->bi
 int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelOut>& outs,
                RunStats* stats) {
     Device* dev = s->dev;
+    const auto tp0 = std::chrono::steady_clock::now();
     outs.assign(reqs.size(), LevelOut());
     if (reqs.empty()) return kOk;
 
@@ -538,6 +540,9 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     if (groups.size() > 64) return kErrUnsupported;
 
     // 5) launch
+    if (stats)
+        stats->host_plan_s +=
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
     cudaStream_t st = s->stream;
     if (cudaMemcpyAsync(d, h, total_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemsetAsync(s->d_ctr.d, 0, s->d_ctr.cap, st) != cudaSuccess) {

@@ -180,6 +180,8 @@ struct RunStats {
     int launches = 0;
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)
+    double host_plan_s = 0.0;     // run_levels host work before the launches
+    double host_apply_s = 0.0;    // schedule updates after each round
 };
 
 // Enumerate every request; blocking.  Returns a Status.
