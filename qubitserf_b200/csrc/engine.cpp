@@ -308,10 +308,23 @@ int upload_sides(Device* dev, Session* s, Arena* arena, const std::vector<SideDe
 // ------------------------------------------------------------------ level runner
 namespace {
 
-// P(Binomial(bits, 1/2) <= t) -- survivor rate of a probe over `bits` random bits.
+// P(Binomial(bits, 1/2) <= t) -- survivor rate of a probe over `bits` random bits
+// (bits <= 128; memoised, the planner asks the same few values every round).
 double binom_cdf_half(int bits, int t) {
     if (t < 0) return 0.0;
     if (t >= bits) return 1.0;
+    static thread_local std::vector<double> memo;
+    if (bits <= 128 && t <= 128) {
+        if (memo.empty()) memo.assign(129 * 129, -1.0);
+        double& m = memo[(size_t)bits * 129 + t];
+        if (m >= 0.0) return m;
+        double logp = -bits * std::log(2.0), acc = 0.0, lc = 0.0;
+        for (int i = 0; i <= t; ++i) {
+            if (i > 0) lc += std::log((double)(bits - i + 1) / i);
+            acc += std::exp(lc + logp);
+        }
+        return m = acc;
+    }
     double logp = -bits * std::log(2.0), acc = 0.0, lc = 0.0;
     for (int i = 0; i <= t; ++i) {
         if (i > 0) lc += std::log((double)(bits - i + 1) / i);
@@ -396,29 +409,35 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     // 2) lists to build
     struct GenReq { SideDev* S; int g, size, reflect, HP; };
     std::vector<GenReq> gens;
+    // the `queued` marks only live for this call, whatever path it leaves by
+    struct ClearQueued {
+        std::vector<GenReq>& g;
+        ~ClearQueued() {
+            for (const GenReq& G : g) G.S->lists[std::make_tuple(G.g, G.size, G.reflect)].queued = false;
+        }
+    } clear_queued{gens};
     for (const Plan& P : plans) {
         SideDev* S = reqs[P.req].side;
         for (int side = 0; side < 2; ++side) {
             const int size = side == 0 ? P.a : P.b;
             auto key = std::make_tuple(P.g, size, side);
             ListBuf& L = S->lists[key];
-            if (L.ready) continue;
+            if (L.ready || L.queued) continue;
             if (L.words) {   // allocated by an earlier execution: regenerate in place
-                bool dup = false;
-                for (const GenReq& G : gens)
-                    dup |= G.S == S && G.g == P.g && G.size == size && G.reflect == side;
-                if (!dup) gens.push_back({S, P.g, size, side, P.HP});
+                L.queued = true;
+                gens.push_back({S, P.g, size, side, P.HP});
                 continue;
             }
+            L.queued = true;
             L.count = dev->binom(S->K, size);
             L.bytes_w = std::max<size_t>((size_t)L.count * P.HP * 4, 16);
             L.arena = S->arena != nullptr;
             L.words = (uint32_t*)(L.arena ? S->arena->alloc(L.bytes_w) : dev->alloc(L.bytes_w));
-            if (!L.words) return kErrMemory;
+            if (!L.words) { L.queued = false; return kErrMemory; }
             if (!P.full) {
                 L.bytes_pc = std::max<size_t>((size_t)L.count, 16);
                 L.pc = (uint8_t*)(L.arena ? S->arena->alloc(L.bytes_pc) : dev->alloc(L.bytes_pc));
-                if (!L.pc) return kErrMemory;
+                if (!L.pc) { L.queued = false; return kErrMemory; }
             }
             S->list_bytes += L.bytes_w + L.bytes_pc;
             gens.push_back({S, P.g, size, side, P.HP});
@@ -580,7 +599,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         cudaEventDestroy(evm);
         return kErrDevice;
     }
-    for (const GenReq& G : gens) G.S->lists[std::make_tuple(G.g, G.size, G.reflect)].ready = true;
+    for (const GenReq& G : gens) {
+        ListBuf& L = G.S->lists[std::make_tuple(G.g, G.size, G.reflect)];
+        L.ready = true;
+        L.queued = false;
+    }
 
     // 6) decode
     unsigned long long* hcounts = (unsigned long long*)(h + off_counts);

@@ -104,6 +104,7 @@ struct ListBuf {
     size_t bytes_w = 0, bytes_pc = 0;
     bool ready = false;
     bool arena = false;   // carved from an Arena (released with it)
+    bool queued = false;  // scheduled for generation in the current run_levels call
 };
 
 // Bump allocator over device chunks taken from the caching allocator; everything carved
