@@ -392,6 +392,10 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             }
             P.H = H;
             P.mode = !P.full ? 0 : (T - 1 - w <= 0 ? 2 : 1);
+            // two-phase filter when one 32-bit word already rejects >= 94% of the pairs
+            if (P.mode == 1 && P.H >= 2 &&
+                binom_cdf_half(std::min(32, nred), T - 1 - w) <= 0.06)
+                P.mode = 3;
             P.pairs = pairs;
             P.p_lo = a - 1;
             P.nterms = K - b - a + 1;

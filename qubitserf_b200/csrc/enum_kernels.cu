@@ -235,7 +235,9 @@ __device__ __forceinline__ uint32_t fold_zero(const uint32_t (&x)[H], const uint
 }
 
 // MODE 0: rank-deficient set (per-entry pivot counts); 1: full-rank set, popcount bound;
-// 2: full-rank set whose bound leaves no room for any non-pivot bit (zero test).
+// 2: full-rank set whose bound leaves no room for any non-pivot bit (zero test);
+// 3: full-rank set, two-phase: a one-POPC filter on probe word 0 marks the few pairs whose
+//    first word stays under the bound, and only those get the other probe words.
 template <int H, int HP, int MODE>
 __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict__ descs,
                                                     int ndesc, unsigned long long total_jobs,
@@ -311,6 +313,49 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
         const uint8_t* lpc = FULL ? nullptr : looppc + loop0;
         for (int c0 = 0; c0 < loop_cnt; c0 += kChunk) {
             const int cn = (loop_cnt - c0) < kChunk ? (loop_cnt - c0) : kChunk;
+            if constexpr (MODE == 3) {
+                // Phase 1: one POPC per pair on probe word 0; a pair whose word-0 weight
+                // alone reaches the bound is rejected, the rest set bit jj of mask[i].
+                uint32_t mask[RX];
+#pragma unroll
+                for (int i = 0; i < RX; ++i) mask[i] = 0u;
+                if (cn == kChunk) {
+#pragma unroll
+                    for (int jj = 0; jj < kChunk; ++jj) {
+                        const uint32_t y0 = __ldg(lp + (size_t)(c0 + jj) * HP);
+#pragma unroll
+                        for (int i = 0; i < RX; ++i)
+                            if (__popc(x[i][0] ^ y0) < thr[i]) mask[i] |= 1u << jj;
+                    }
+                } else {
+                    for (int jj = 0; jj < cn; ++jj) {
+                        const uint32_t y0 = __ldg(lp + (size_t)(c0 + jj) * HP);
+#pragma unroll
+                        for (int i = 0; i < RX; ++i)
+                            if (__popc(x[i][0] ^ y0) < thr[i]) mask[i] |= 1u << jj;
+                    }
+                }
+                // Phase 2: the remaining probe words for the marked pairs only; a pair
+                // still within the bound gets the exact rescan.
+#pragma unroll
+                for (int i = 0; i < RX; ++i) {
+                    while (mask[i]) {
+                        const int jj = __ffs(mask[i]) - 1;
+                        mask[i] &= mask[i] - 1u;
+                        uint32_t y[H];
+                        load_entry<H, HP>(lp + (size_t)(c0 + jj) * HP, y);
+                        if (probe_sum<H>(x[i], y) < thr[i]) {
+                            const unsigned long long e = reg0 + lane + 32 * i;
+                            T = survivor_scan(D, B, regX, xoff, e, pcr[i],
+                                              loop0 + (unsigned long long)(c0 + jj), 1, T);
+#pragma unroll
+                            for (int q = 0; q < RX; ++q)
+                                thr[q] = T - pcr[q] - (regX ? D.b : D.a);
+                        }
+                    }
+                }
+                continue;
+            }
             int j = c0;
             const int cend = c0 + cn;
             if (FULL) {
@@ -422,9 +467,13 @@ cudaError_t launch_pairs(int H, int HP, int mode, const LevelDesc* d, int nd,
     switch ((H * 8 + HP) * 4 + mode) {
         QSFB_PAIRS_CASE(1, 1, 0) QSFB_PAIRS_CASE(1, 1, 1) QSFB_PAIRS_CASE(1, 1, 2)
         QSFB_PAIRS_CASE(2, 2, 0) QSFB_PAIRS_CASE(2, 2, 1) QSFB_PAIRS_CASE(2, 2, 2)
+        QSFB_PAIRS_CASE(2, 2, 3)
         QSFB_PAIRS_CASE(2, 4, 0) QSFB_PAIRS_CASE(2, 4, 1) QSFB_PAIRS_CASE(2, 4, 2)
+        QSFB_PAIRS_CASE(2, 4, 3)
         QSFB_PAIRS_CASE(3, 4, 0) QSFB_PAIRS_CASE(3, 4, 1) QSFB_PAIRS_CASE(3, 4, 2)
+        QSFB_PAIRS_CASE(3, 4, 3)
         QSFB_PAIRS_CASE(4, 4, 0) QSFB_PAIRS_CASE(4, 4, 1) QSFB_PAIRS_CASE(4, 4, 2)
+        QSFB_PAIRS_CASE(4, 4, 3)
         default: return cudaErrorInvalidValue;
     }
 }
