@@ -1,9 +1,9 @@
 // Host side of the device engine: context, allocator, side upload and the level runner.
 #include "engine.hpp"
+#include "filter_plan.hpp"
 
 #include <algorithm>
 #include <chrono>
-#include <cmath>
 #include <cstdlib>
 #include <cstring>
 
@@ -11,7 +11,7 @@ namespace qsfb {
 
 cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
                              const unsigned long long* d_binom, int num_sms, cudaStream_t st);
-cudaError_t launch_pairs(int H, int HP, int mode, const LevelDesc* d, int nd,
+cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
 
@@ -308,31 +308,6 @@ int upload_sides(Device* dev, Session* s, Arena* arena, const std::vector<SideDe
 // ------------------------------------------------------------------ level runner
 namespace {
 
-// P(Binomial(bits, 1/2) <= t) -- survivor rate of a probe over `bits` random bits
-// (bits <= 128; memoised, the planner asks the same few values every round).
-double binom_cdf_half(int bits, int t) {
-    if (t < 0) return 0.0;
-    if (t >= bits) return 1.0;
-    static thread_local std::vector<double> memo;
-    if (bits <= 128 && t <= 128) {
-        if (memo.empty()) memo.assign(129 * 129, -1.0);
-        double& m = memo[(size_t)bits * 129 + t];
-        if (m >= 0.0) return m;
-        double logp = -bits * std::log(2.0), acc = 0.0, lc = 0.0;
-        for (int i = 0; i <= t; ++i) {
-            if (i > 0) lc += std::log((double)(bits - i + 1) / i);
-            acc += std::exp(lc + logp);
-        }
-        return m = acc;
-    }
-    double logp = -bits * std::log(2.0), acc = 0.0, lc = 0.0;
-    for (int i = 0; i <= t; ++i) {
-        if (i > 0) lc += std::log((double)(bits - i + 1) / i);
-        acc += std::exp(lc + logp);
-    }
-    return acc;
-}
-
 int words_of(int bits) { return (bits + 31) / 32; }
 
 // Initial witness key: weight field = bound + 1 (the strict bound), every other bit set.
@@ -342,7 +317,7 @@ unsigned long long key_init(int bound) {
 }
 
 struct Plan {
-    int req, g, a, b, H, HP, full, mode;
+    int req, g, a, b, filt, popcs, HP, full, mode;
     unsigned long long pairs;
     int p_lo, nterms;
     std::vector<unsigned long long> term_jobs;
@@ -383,19 +358,12 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             P.full = rank == K;
             // mode: 0 rank-deficient, 1 full rank, 2 full rank with no room above the
             // pivot bits (every candidate needs an all-zero non-pivot part)
-            // smallest probe width whose random-code survivor rate is negligible
             const int T = std::max(0, std::min(q.bound + 1, 4095));
             const int pcmin = std::max(0, w - (K - rank));
-            int H = std::min(wg, 4);
-            for (int h = std::min(wg, 2); h < std::min(wg, 4); ++h) {
-                if (binom_cdf_half(std::min(32 * h, nred), T - 1 - pcmin) <= 1e-6) { H = h; break; }
-            }
-            P.H = H;
             P.mode = !P.full ? 0 : (T - 1 - w <= 0 ? 2 : 1);
-            // two-phase filter when one 32-bit word already rejects >= 94% of the pairs
-            if (P.mode == 1 && P.H >= 2 &&
-                binom_cdf_half(std::min(32, nred), T - 1 - w) <= 0.06)
-                P.mode = 3;
+            const FilterChoice fc = choose_filter(P.HP, nred, T - 1 - pcmin, P.mode == 2);
+            P.filt = fc.filt;
+            P.popcs = fc.popcs;
             P.pairs = pairs;
             P.p_lo = a - 1;
             P.nterms = K - b - a + 1;
@@ -469,8 +437,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     std::vector<int> order(plans.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return std::make_tuple(plans[x].H, plans[x].HP, plans[x].mode) <
-               std::make_tuple(plans[y].H, plans[y].HP, plans[y].mode);
+        return std::make_tuple(plans[x].filt, plans[x].HP, plans[x].mode) <
+               std::make_tuple(plans[y].filt, plans[y].HP, plans[y].mode);
     });
 
     // 4) staging layout
@@ -522,13 +490,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     LevelDesc* hl = (LevelDesc*)(h + off_lvl);
     unsigned long long* hterms = (unsigned long long*)(h + off_terms);
     size_t term_cursor = 0;
-    struct Group { int H, HP, mode, first, count; unsigned long long jobs; };
+    struct Group { int filt, HP, mode, first, count; unsigned long long jobs; };
     std::vector<Group> groups;
     for (size_t oi = 0; oi < order.size(); ++oi) {
         const Plan& P = plans[order[oi]];
-        if (groups.empty() || groups.back().H != P.H || groups.back().HP != P.HP ||
+        if (groups.empty() || groups.back().filt != P.filt || groups.back().HP != P.HP ||
             groups.back().mode != P.mode)
-            groups.push_back({P.H, P.HP, P.mode, (int)oi, 0, 0ull});
+            groups.push_back({P.filt, P.HP, P.mode, (int)oi, 0, 0ull});
         Group& Gp = groups.back();
         SideDev* S = reqs[P.req].side;
         LevelDesc& D = hl[oi];
@@ -586,7 +554,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     unsigned long long all_jobs = 0;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& Gp = groups[gi];
-        if (launch_pairs(Gp.H, Gp.HP, Gp.mode, (const LevelDesc*)(d + off_lvl) + Gp.first, Gp.count,
+        if (launch_pairs(Gp.filt, Gp.HP, Gp.mode, (const LevelDesc*)(d + off_lvl) + Gp.first, Gp.count,
                          Gp.jobs, (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
                          dev->num_sms, st) != cudaSuccess) {
             cudaEventDestroy(evm);
@@ -630,7 +598,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         outs[P.req].counts[P.g] = hcounts[order[oi]];
         cw += hcounts[order[oi]];
         if (P.mode == 2) zcw += hcounts[order[oi]];
-        else popc += hcounts[order[oi]] * (unsigned long long)P.H;
+        else popc += hcounts[order[oi]] * (unsigned long long)P.popcs;
         const LevelDesc& D = hl[oi];
         if (outs[P.req].found && outs[P.req].g == P.g) outs[P.req].rank_shift = D.rank_shift;
     }

@@ -9,11 +9,13 @@
 // a set of rectangles of independent (prefix, suffix) pairs that a warp sweeps with the
 // prefix entries in registers and the suffix entries broadcast from L1.
 //
-// The hot loop is integer-issue bound: per pair H LOP3 (XOR), H POPC and one fused
-// add/min on the H probe words; the pivot columns never enter it (they contribute the
-// pivot-row count).  A pair whose probe sum reaches the bound is rejected there; the rare
-// survivors are re-evaluated over all words, tested against the detector syndromes and
-// folded into the side's packed witness key with one 64-bit atomicMin.
+// The hot loop is bound by the POPC (XU) pipe: per pair a few LOP3s fold the XORed probe
+// words into one (or two) words whose popcount bounds the probe weight from below, one
+// POPC each and one fused add/min; the pivot columns never enter it (they contribute the
+// pivot-row count).  A chunk whose minimum stays at or above the bound is rejected there;
+// the rare chunks under it are rescanned exactly, their survivors re-evaluated over all
+// words, tested against the detector syndromes and folded into the side's packed witness
+// key with one 64-bit atomicMin.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -182,13 +184,14 @@ __device__ __noinline__ int survivor_scan(const LevelDesc& D, const unsigned lon
 }
 
 // ---------------------------------------------------------------- pair sweep
-template <int H>
-__device__ __forceinline__ int probe_sum(const uint32_t (&x)[H], const uint32_t (&y)[H]) {
-    int s = 0;
-#pragma unroll
-    for (int h = 0; h < H; ++h) s += __popc(x[h] ^ y[h]);
-    return s;
-}
+// Probe filters.  A filter maps the XORed probe words of a pair to a lower bound on their
+// popcount sum, at fewer POPCs (the XU pipe, the sweep's bottleneck) than the exact sum:
+//   FILT 1..4: popc(a | b | ...) over the first FILT words (one POPC);
+//   FILT 6:    carry-save over four words, popc(a^b^c^d) + 2 popc(maj(a,b,c) | (a^b^c)&d),
+//              exact except that a column set in all four words counts 2 (two POPCs).
+// Every pair whose exact sum is under the bound is under it on the filter as well, so the
+// filter only decides which chunks get the exact rescan.
+__host__ __device__ constexpr int filter_words(int filt) { return filt == 6 ? 4 : filt; }
 
 template <int H, int HP>
 __device__ __forceinline__ void load_entry(const uint32_t* __restrict__ p, uint32_t (&v)[H]) {
@@ -206,20 +209,20 @@ __device__ __forceinline__ void load_entry(const uint32_t* __restrict__ p, uint3
     }
 }
 
-// m = min(m, popc-sum + extra) with the add folded into the DPX add-min where possible.
-template <int H>
-__device__ __forceinline__ int fold_min(const uint32_t (&x)[H], const uint32_t (&y)[H],
-                                        int extra, int m) {
-    if constexpr (H == 1) {
-        return __viaddmin_s32(__popc(x[0] ^ y[0]), extra, m);
-    } else if constexpr (H == 2) {
-        return __viaddmin_s32(__popc(x[0] ^ y[0]) + extra, __popc(x[1] ^ y[1]), m);
-    } else if constexpr (H == 3) {
-        return __viaddmin_s32(__popc(x[0] ^ y[0]) + __popc(x[1] ^ y[1]) + extra,
-                              __popc(x[2] ^ y[2]), m);
+// m = min(m, filter + extra), the add folded into the DPX add-min.
+template <int FILT>
+__device__ __forceinline__ int fold_min(const uint32_t (&x)[filter_words(FILT)],
+                                        const uint32_t (&y)[filter_words(FILT)], int extra, int m) {
+    if constexpr (FILT == 6) {
+        const uint32_t a = x[0] ^ y[0], b = x[1] ^ y[1], c = x[2] ^ y[2], d = x[3] ^ y[3];
+        const uint32_t s = a ^ b ^ c;
+        const uint32_t mj = (a & b) | (c & (a | b));
+        return __viaddmin_s32(__popc(s ^ d) + extra, 2 * __popc(mj | (s & d)), m);
     } else {
-        return __viaddmin_s32(__popc(x[0] ^ y[0]) + __popc(x[1] ^ y[1]) + __popc(x[2] ^ y[2]) + extra,
-                              __popc(x[3] ^ y[3]), m);
+        uint32_t v = x[0] ^ y[0];
+#pragma unroll
+        for (int h = 1; h < FILT; ++h) v |= x[h] ^ y[h];
+        return __viaddmin_s32(__popc(v), extra, m);
     }
 }
 
@@ -235,16 +238,16 @@ __device__ __forceinline__ uint32_t fold_zero(const uint32_t (&x)[H], const uint
 }
 
 // MODE 0: rank-deficient set (per-entry pivot counts); 1: full-rank set, popcount bound;
-// 2: full-rank set whose bound leaves no room for any non-pivot bit (zero test);
-// 3: full-rank set, two-phase: a one-POPC filter on probe word 0 marks the few pairs whose
-//    first word stays under the bound, and only those get the other probe words.
-template <int H, int HP, int MODE>
+// 2: full-rank set whose bound leaves no room for any non-pivot bit (zero test).
+// FILT is the probe filter (filter_words(FILT) probe words of the HP stored per entry).
+template <int FILT, int HP, int MODE>
 __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict__ descs,
                                                     int ndesc, unsigned long long total_jobs,
                                                     unsigned long long* __restrict__ job_counter,
                                                     const unsigned long long* __restrict__ B) {
     constexpr bool FULL = MODE != 0;
     constexpr bool ZERO = MODE == 2;
+    constexpr int H = filter_words(FILT);
     const int lane = threadIdx.x & 31;
     for (;;) {
         unsigned long long job = 0;
@@ -313,49 +316,6 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
         const uint8_t* lpc = FULL ? nullptr : looppc + loop0;
         for (int c0 = 0; c0 < loop_cnt; c0 += kChunk) {
             const int cn = (loop_cnt - c0) < kChunk ? (loop_cnt - c0) : kChunk;
-            if constexpr (MODE == 3) {
-                // Phase 1: one POPC per pair on probe word 0; a pair whose word-0 weight
-                // alone reaches the bound is rejected, the rest set bit jj of mask[i].
-                uint32_t mask[RX];
-#pragma unroll
-                for (int i = 0; i < RX; ++i) mask[i] = 0u;
-                if (cn == kChunk) {
-#pragma unroll
-                    for (int jj = 0; jj < kChunk; ++jj) {
-                        const uint32_t y0 = __ldg(lp + (size_t)(c0 + jj) * HP);
-#pragma unroll
-                        for (int i = 0; i < RX; ++i)
-                            if (__popc(x[i][0] ^ y0) < thr[i]) mask[i] |= 1u << jj;
-                    }
-                } else {
-                    for (int jj = 0; jj < cn; ++jj) {
-                        const uint32_t y0 = __ldg(lp + (size_t)(c0 + jj) * HP);
-#pragma unroll
-                        for (int i = 0; i < RX; ++i)
-                            if (__popc(x[i][0] ^ y0) < thr[i]) mask[i] |= 1u << jj;
-                    }
-                }
-                // Phase 2: the remaining probe words for the marked pairs only; a pair
-                // still within the bound gets the exact rescan.
-#pragma unroll
-                for (int i = 0; i < RX; ++i) {
-                    while (mask[i]) {
-                        const int jj = __ffs(mask[i]) - 1;
-                        mask[i] &= mask[i] - 1u;
-                        uint32_t y[H];
-                        load_entry<H, HP>(lp + (size_t)(c0 + jj) * HP, y);
-                        if (probe_sum<H>(x[i], y) < thr[i]) {
-                            const unsigned long long e = reg0 + lane + 32 * i;
-                            T = survivor_scan(D, B, regX, xoff, e, pcr[i],
-                                              loop0 + (unsigned long long)(c0 + jj), 1, T);
-#pragma unroll
-                            for (int q = 0; q < RX; ++q)
-                                thr[q] = T - pcr[q] - (regX ? D.b : D.a);
-                        }
-                    }
-                }
-                continue;
-            }
             int j = c0;
             const int cend = c0 + cn;
             if (FULL) {
@@ -376,10 +336,10 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                             m[i] = (int)mm;
                         } else {
                             int mm = m[i];
-                            mm = fold_min<H>(x[i], y0, 0, mm);
-                            mm = fold_min<H>(x[i], y1, 0, mm);
-                            mm = fold_min<H>(x[i], y2, 0, mm);
-                            mm = fold_min<H>(x[i], y3, 0, mm);
+                            mm = fold_min<FILT>(x[i], y0, 0, mm);
+                            mm = fold_min<FILT>(x[i], y1, 0, mm);
+                            mm = fold_min<FILT>(x[i], y2, 0, mm);
+                            mm = fold_min<FILT>(x[i], y3, 0, mm);
                             m[i] = mm;
                         }
                     }
@@ -390,7 +350,7 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
 #pragma unroll
                     for (int i = 0; i < RX; ++i) {
                         if constexpr (ZERO) m[i] = (int)fold_zero<H>(x[i], y0, (uint32_t)m[i]);
-                        else m[i] = fold_min<H>(x[i], y0, 0, m[i]);
+                        else m[i] = fold_min<FILT>(x[i], y0, 0, m[i]);
                     }
                 }
             } else {
@@ -399,7 +359,7 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                     load_entry<H, HP>(lp + j * HP, y0);
                     const int pcy = (int)__ldg(lpc + j);
 #pragma unroll
-                    for (int i = 0; i < RX; ++i) m[i] = fold_min<H>(x[i], y0, pcy, m[i]);
+                    for (int i = 0; i < RX; ++i) m[i] = fold_min<FILT>(x[i], y0, pcy, m[i]);
                 }
             }
             bool any = false;
@@ -438,42 +398,39 @@ cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long lo
     return cudaGetLastError();
 }
 
-template <int H, int HP, int MODE>
+template <int FILT, int HP, int MODE>
 static cudaError_t launch_pairs_t(const LevelDesc* d, int nd, unsigned long long jobs,
                                   unsigned long long* ctr, const unsigned long long* B,
                                   int num_sms, cudaStream_t st) {
     static int blocks_per_sm = 0;
     if (blocks_per_sm == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm,
-                                                      dev::pairs_kernel<H, HP, MODE>, 128, 0);
+                                                      dev::pairs_kernel<FILT, HP, MODE>, 128, 0);
         if (blocks_per_sm < 1) blocks_per_sm = 1;
     }
     unsigned long long blocks = (unsigned long long)num_sms * blocks_per_sm;
     const unsigned long long need = (jobs + 3) / 4;   // 4 warps per block
     if (need < blocks) blocks = need;
     if (blocks < 1) blocks = 1;
-    dev::pairs_kernel<H, HP, MODE><<<(unsigned)blocks, 128, 0, st>>>(d, nd, jobs, ctr, B);
+    dev::pairs_kernel<FILT, HP, MODE><<<(unsigned)blocks, 128, 0, st>>>(d, nd, jobs, ctr, B);
     return cudaGetLastError();
 }
 
-#define QSFB_PAIRS_CASE(H, HP, M) \
-    case ((H) * 8 + (HP)) * 4 + (M): \
-        return launch_pairs_t<H, HP, M>(d, nd, jobs, ctr, B, num_sms, st);
+#define QSFB_PAIRS_CASE(F, HP, M) \
+    case ((F) * 8 + (HP)) * 4 + (M): \
+        return launch_pairs_t<F, HP, M>(d, nd, jobs, ctr, B, num_sms, st);
 
-cudaError_t launch_pairs(int H, int HP, int mode, const LevelDesc* d, int nd,
+cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st) {
     if (jobs == 0) return cudaSuccess;
-    switch ((H * 8 + HP) * 4 + mode) {
+    switch ((filt * 8 + HP) * 4 + mode) {
         QSFB_PAIRS_CASE(1, 1, 0) QSFB_PAIRS_CASE(1, 1, 1) QSFB_PAIRS_CASE(1, 1, 2)
         QSFB_PAIRS_CASE(2, 2, 0) QSFB_PAIRS_CASE(2, 2, 1) QSFB_PAIRS_CASE(2, 2, 2)
-        QSFB_PAIRS_CASE(2, 2, 3)
         QSFB_PAIRS_CASE(2, 4, 0) QSFB_PAIRS_CASE(2, 4, 1) QSFB_PAIRS_CASE(2, 4, 2)
-        QSFB_PAIRS_CASE(2, 4, 3)
-        QSFB_PAIRS_CASE(3, 4, 0) QSFB_PAIRS_CASE(3, 4, 1) QSFB_PAIRS_CASE(3, 4, 2)
-        QSFB_PAIRS_CASE(3, 4, 3)
-        QSFB_PAIRS_CASE(4, 4, 0) QSFB_PAIRS_CASE(4, 4, 1) QSFB_PAIRS_CASE(4, 4, 2)
-        QSFB_PAIRS_CASE(4, 4, 3)
+        QSFB_PAIRS_CASE(3, 4, 0) QSFB_PAIRS_CASE(3, 4, 1)
+        QSFB_PAIRS_CASE(4, 4, 0) QSFB_PAIRS_CASE(4, 4, 1)
+        QSFB_PAIRS_CASE(6, 4, 0) QSFB_PAIRS_CASE(6, 4, 1)
         default: return cudaErrorInvalidValue;
     }
 }

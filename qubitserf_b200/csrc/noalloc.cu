@@ -19,7 +19,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cmath>
 #include <cstdint>
 #include <cstddef>
 #include <cstring>
@@ -27,11 +26,12 @@
 
 #include "../../include/qsf_b200.h"
 #include "engine_types.hpp"
+#include "filter_plan.hpp"
 
 namespace qsfb {
 cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
                              const unsigned long long* d_binom, int num_sms, cudaStream_t st);
-cudaError_t launch_pairs(int H, int HP, int mode, const LevelDesc* d, int nd,
+cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
 }  // namespace qsfb
@@ -180,7 +180,7 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
         return kErrScratch;
     cudaStream_t st = (cudaStream_t)stream;
 
-    // ---- plan (the rules of the allocating path: prefix/suffix split, probe width)
+    // ---- plan (the rules of the allocating path: prefix/suffix split, probe filter)
     const unsigned long long pairs = host_binom(K, d);
     const int a = pairs <= (1ull << 14) ? d : (d + 1) / 2;
     const int b = d - a;
@@ -188,18 +188,7 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
     const int HP = W32 >= 3 ? 4 : W32;
     const int bound = current_best >= kWeightNone ? 4094 : current_best - 1;
     const int T = std::max(0, std::min(bound + 1, 4095));
-    int H = std::min(W32, 4);
-    for (int h = std::min(W32, 2); h < std::min(W32, 4); ++h) {
-        // survivor rate of an h-word probe over random bits (same rule as run_levels)
-        const int bits = 32 * h, t = T - 1;
-        double acc = 0.0, lc = 0.0;
-        const double lp = -bits * std::log(2.0);
-        for (int i = 0; i <= std::min(t, bits); ++i) {
-            if (i > 0) lc += std::log((double)(bits - i + 1) / i);
-            acc += std::exp(lc + lp);
-        }
-        if (t < 0 || acc <= 1e-6) { H = h; break; }
-    }
+    const int filt = choose_filter(HP, 32 * W32, T - 1, false).filt;
     const int SW = (kcheck + 31) / 32;
     const unsigned long long na = host_binom(K, a), nb = host_binom(K, b);
     const size_t list_a = (size_t)na * HP * 4, list_b = (size_t)nb * HP * 4;
@@ -295,7 +284,7 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
     }
     if (cudaGetLastError() != cudaSuccess ||
         launch_gen_lists((const GenDesc*)(dd + off_gen), ngen, gen_total, d_binom, slot->sms, st) != cudaSuccess ||
-        launch_pairs(H, HP, 0, (const LevelDesc*)(dd + off_lvl), num_gamma, job_total,
+        launch_pairs(filt, HP, 0, (const LevelDesc*)(dd + off_lvl), num_gamma, job_total,
                      (unsigned long long*)(dd + off_ctr), d_binom, slot->sms, st) != cudaSuccess) {
         cudaGetLastError();
         return 4;
