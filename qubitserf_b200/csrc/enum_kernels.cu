@@ -209,6 +209,32 @@ __device__ __forceinline__ void load_entry(const uint32_t* __restrict__ p, uint3
     }
 }
 
+// Filter value of one pair (no pivot rows).
+template <int FILT>
+__device__ __forceinline__ int filter_value(const uint32_t (&x)[filter_words(FILT)],
+                                            const uint32_t (&y)[filter_words(FILT)]) {
+    if constexpr (FILT == 6) {
+        const uint32_t a = x[0] ^ y[0], b = x[1] ^ y[1], c = x[2] ^ y[2], d = x[3] ^ y[3];
+        const uint32_t s = a ^ b ^ c;
+        const uint32_t mj = (a & b) | (c & (a | b));
+        return __popc(s ^ d) + 2 * __popc(mj | (s & d));
+    } else {
+        uint32_t v = x[0] ^ y[0];
+#pragma unroll
+        for (int h = 1; h < FILT; ++h) v |= x[h] ^ y[h];
+        return __popc(v);
+    }
+}
+
+// OR of the XORed probe words (zero exactly when every probe word of the pair's XOR is).
+template <int H>
+__device__ __forceinline__ uint32_t xor_or(const uint32_t (&x)[H], const uint32_t (&y)[H]) {
+    uint32_t v = x[0] ^ y[0];
+#pragma unroll
+    for (int h = 1; h < H; ++h) v |= x[h] ^ y[h];
+    return v;
+}
+
 // m = min(m, filter + extra), the add folded into the DPX add-min.
 template <int FILT>
 __device__ __forceinline__ int fold_min(const uint32_t (&x)[filter_words(FILT)],
@@ -327,19 +353,18 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                     load_entry<H, HP>(lp + (j + 3) * HP, y3);
 #pragma unroll
                     for (int i = 0; i < RX; ++i) {
+                        // two pairs per three-input DPX minimum
                         if constexpr (ZERO) {
                             uint32_t mm = (uint32_t)m[i];
-                            mm = fold_zero<H>(x[i], y0, mm);
-                            mm = fold_zero<H>(x[i], y1, mm);
-                            mm = fold_zero<H>(x[i], y2, mm);
-                            mm = fold_zero<H>(x[i], y3, mm);
+                            mm = __vimin3_u32(xor_or<H>(x[i], y0), xor_or<H>(x[i], y1), mm);
+                            mm = __vimin3_u32(xor_or<H>(x[i], y2), xor_or<H>(x[i], y3), mm);
                             m[i] = (int)mm;
                         } else {
                             int mm = m[i];
-                            mm = fold_min<FILT>(x[i], y0, 0, mm);
-                            mm = fold_min<FILT>(x[i], y1, 0, mm);
-                            mm = fold_min<FILT>(x[i], y2, 0, mm);
-                            mm = fold_min<FILT>(x[i], y3, 0, mm);
+                            mm = __vimin3_s32(filter_value<FILT>(x[i], y0),
+                                              filter_value<FILT>(x[i], y1), mm);
+                            mm = __vimin3_s32(filter_value<FILT>(x[i], y2),
+                                              filter_value<FILT>(x[i], y3), mm);
                             m[i] = mm;
                         }
                     }
