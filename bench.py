@@ -269,7 +269,8 @@ def main():
                               "device_mb": st.device_bytes / 2**20,
                               "pair_ms": st.pair_ms, "gen_ms": st.gen_ms,
                               "host_plan_ms": st.host_plan_seconds * 1e3,
-                              "host_apply_ms": st.host_apply_seconds * 1e3}), flush=True)
+                              "host_apply_ms": st.host_apply_seconds * 1e3,
+                              "tc_share": st.tc_codewords / max(st.codewords, 1)}), flush=True)
         return
 
     # --- end to end: the one-shot public call from host matrices, K times

@@ -185,6 +185,7 @@ typedef struct {
     double gen_ms;               /* list-generation kernel time */
     double host_plan_seconds;    /* host planning of the rounds (before their launches) */
     double host_apply_seconds;   /* host schedule updates after the rounds */
+    unsigned long long tc_codewords;    /* codewords swept by the tensor-core kernel */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free. */
@@ -253,6 +254,13 @@ int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int num_gamma,
 /* Measured integer-pipe peak (ops/s over the whole device): which = 0 for 32-bit POPC
  * (the XU pipe), 1 for LOP3 (the ALU pipe).  Roofline denominators of the pair kernel. */
 int qsfb_microbench(int which, double* ops_per_s);
+
+/* Operand-layout self-test of the tensor-core pair sweep (no reference counterpart):
+ * D = A * B^T over the first 32 * ksteps columns, with A 256 x 64 and B 128 x 64 int8
+ * (row-major; the sweep stores +1 / -1 / 0) and D 256 x 128 int32 (row-major), computed
+ * by the sweep's own copy, tcgen05 MMA and TMEM read-back path.  ksteps in 1..2.
+ * Returns 0, 1 (null), 2 (ksteps), 4 (device) or 6 (memory). */
+int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D);
 
 /* Overwrite a 256 MiB device buffer (more than the 126 MB L2) and wait; benchmarks call it
  * between timed steps.  Returns 0, or 4 without a device. */

@@ -74,7 +74,7 @@ class QsfbBatchStats(ctypes.Structure):
                 ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong),
                 ("gen_ms", ctypes.c_double), ("host_plan_seconds", ctypes.c_double),
-                ("host_apply_seconds", ctypes.c_double)]
+                ("host_apply_seconds", ctypes.c_double), ("tc_codewords", ctypes.c_ulonglong)]
 
 
 class QsfbTiming(ctypes.Structure):
@@ -135,6 +135,7 @@ SIGNATURES = [
     ("qsfb_server_stop", _i, [ctypes.c_void_p]),
     ("qsfb_microbench", _i, [_i, ctypes.POINTER(ctypes.c_double)]),
     ("qsfb_flush_l2", _i, []),
+    ("qsfb_tc_selftest", _i, [_i, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
 ]
@@ -466,3 +467,16 @@ def microbench(which):
     v = ctypes.c_double()
     _check(lib().qsfb_microbench(int(which), ctypes.byref(v)), "qsfb_microbench")
     return v.value
+
+
+def tc_selftest(ksteps, A, B):
+    """D = A[:, :32k] @ B[:, :32k].T (int32, 256 x 128) through the tensor-core sweep's own
+    copy / MMA / TMEM path; A is 256 x 64 and B 128 x 64 int8."""
+    A = np.ascontiguousarray(A, dtype=np.int8)
+    B = np.ascontiguousarray(B, dtype=np.int8)
+    if A.shape != (256, 64) or B.shape != (128, 64):
+        raise ValueError("tc_selftest: A must be 256 x 64 and B 128 x 64 int8")
+    D = np.zeros((256, 128), dtype=np.int32)
+    _check(lib().qsfb_tc_selftest(int(ksteps), A.ctypes.data, B.ctypes.data, D.ctypes.data),
+           "qsfb_tc_selftest")
+    return D

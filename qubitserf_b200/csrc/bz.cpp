@@ -179,7 +179,7 @@ void BzSide::reset() {
     proven = false;
     best_from_level = false;
     best_g = -1;
-    for (auto& kv : dev.lists) kv.second.ready = false;
+    for (auto& kv : dev.lists) kv.second.ready = kv.second.pm_ready = false;
 }
 
 int BzSide::active_at(int w) const {
@@ -611,6 +611,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             stats->codewords += rs.codewords;
             stats->popc_issued += rs.popc_issued;
             stats->zero_codewords += rs.zero_codewords;
+            stats->tc_codewords += rs.tc_codewords;
             stats->launches += rs.launches;
         }
         if (jobs.size() == 1) {

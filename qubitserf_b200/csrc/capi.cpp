@@ -19,6 +19,10 @@
 using namespace qsfb;
 
 namespace qsfb {
+cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int32_t* out,
+                               int* err, cudaStream_t st);
+int tc_tile_rows();
+int tc_tile_cols();
 cudaError_t microbench_peak(int which, int num_sms, uint32_t* d_out, cudaStream_t st,
                             double* ops_per_s);
 }
@@ -594,6 +598,7 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
         stats->codewords = rs.codewords;
         stats->popc_issued = rs.popc_issued;
         stats->zero_codewords = rs.zero_codewords;
+        stats->tc_codewords = rs.tc_codewords;
         stats->rounds = rounds;
         stats->kernel_launches = rs.launches;
         stats->certificates = (int)jobs.size();
@@ -632,6 +637,48 @@ int qsfb_microbench(int which, double* ops_per_s) {
                                           ops_per_s);
     dev->release(out, (size_t)dev->num_sms * 8 * 4);
     return e == cudaSuccess ? kOk : kErrDevice;
+}
+
+int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D) {
+    if (!A || !B || !D) return kErrNull;
+    if (ksteps < 1 || ksteps > kPmRowBytes / 32) return kErrShape;
+    int rc = kOk;
+    Device* dev = device_or(&rc);
+    if (!dev) return rc;
+    SessionLease lease(dev);
+    if (!lease.s) return kErrDevice;
+    const int rows_a = tc_tile_rows(), rows_b = tc_tile_cols();
+    const size_t bytes_a = (size_t)rows_a * kPmRowBytes, bytes_b = (size_t)rows_b * kPmRowBytes;
+    const size_t bytes_d = (size_t)rows_a * rows_b * 4;
+    // host swizzle: 16-byte chunk j of row e goes to chunk j ^ ((e >> 1) & 3)
+    std::vector<int8_t> h((size_t)(rows_a + rows_b) * kPmRowBytes);
+    auto put = [&](const int8_t* src, int rows, int8_t* dst) {
+        for (int e = 0; e < rows; ++e)
+            for (int j = 0; j < kPmRowBytes / 16; ++j)
+                std::memcpy(dst + (size_t)e * kPmRowBytes + (size_t)((j ^ ((e >> 1) & 3)) * 16),
+                            src + (size_t)e * kPmRowBytes + (size_t)j * 16, 16);
+    };
+    put(A, rows_a, h.data());
+    put(B, rows_b, h.data() + bytes_a);
+    const size_t total = bytes_a + bytes_b + bytes_d + 256;
+    char* buf = (char*)dev->alloc(total);
+    if (!buf) return kErrMemory;
+    int8_t* dA = (int8_t*)buf;
+    int8_t* dB = (int8_t*)(buf + bytes_a);
+    int32_t* dD = (int32_t*)(buf + bytes_a + bytes_b);
+    int* dErr = (int*)(buf + bytes_a + bytes_b + bytes_d);
+    cudaStream_t st = lease.s->stream;
+    int herr = 0;
+    bool ok = cudaMemcpyAsync(buf, h.data(), bytes_a + bytes_b, cudaMemcpyHostToDevice, st) ==
+                  cudaSuccess &&
+              cudaMemsetAsync(dErr, 0, sizeof(int), st) == cudaSuccess &&
+              launch_tc_selftest(dA, dB, ksteps, dD, dErr, st) == cudaSuccess &&
+              cudaMemcpyAsync(D, dD, bytes_d, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+              cudaMemcpyAsync(&herr, dErr, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+              cudaStreamSynchronize(st) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    dev->release(buf, total);
+    return ok && herr == 0 ? kOk : kErrDevice;
 }
 
 int qsfb_flush_l2(void) {

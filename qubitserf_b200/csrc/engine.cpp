@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -14,6 +15,13 @@ cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long lo
 cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
+cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_chunks,
+                             int num_sms, cudaStream_t st);
+cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
+                            const unsigned long long* B, int* err, int num_sms, cudaStream_t st);
+int tc_tile_rows();
+int tc_tile_cols();
+int tc_job_tiles();
 
 namespace {
 constexpr unsigned long long kSat = ~0ull;
@@ -214,6 +222,7 @@ SideDev::~SideDev() {
         if (kv.second.arena) continue;
         dev->release(kv.second.words, kv.second.bytes_w);
         dev->release(kv.second.pc, kv.second.bytes_pc);
+        dev->release(kv.second.pm, kv.second.bytes_pm);
     }
 }
 
@@ -316,9 +325,38 @@ unsigned long long key_init(int bound) {
     return ((unsigned long long)f << kKeyWtShift) | ((1ull << kKeyWtShift) - 1);
 }
 
+// Tensor-core sweep switch: QSFB_TENSOR=0 keeps every level on the CUDA-core kernels.
+bool tensor_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("QSFB_TENSOR");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// Tensor-core sweep for a full-rank set: worth it when the exact Hamming filter over the
+// first 64 non-pivot columns (two K = 32 MMA steps) is clearly cheaper than the CUDA-core
+// filter.  Costs are SM cycles per 32768 pairs (one 256 x 128 tile): the four MMAs take
+// ~262 cycles, a 64-column slice the filter passes costs ~1300 cycles of exact rescan on
+// one of the eight read-back warps; the CUDA-core sweep costs ~2048 cycles per POPC per
+// pair, ~1280 in zero-test mode.  Returns the MMA steps (2) or 0.
+int tc_depth(int n_enc, int t, int popcs, int* n_live) {
+    const int nl = std::min(n_enc, 64);
+    if (nl <= 32 || t >= nl / 2) return 0;   // the filter would reject (almost) nothing
+    const double pass = hamming_pass_rate(nl, t);
+    const double cost = 262.0 + 512.0 * 64.0 * pass * 1300.0 / 8.0;
+    const double cc = popcs > 0 ? 2048.0 * popcs : 1280.0;
+    if (cost >= 0.6 * cc) return 0;
+    *n_live = nl;
+    return 2;
+}
+
 struct Plan {
     int req, g, a, b, filt, popcs, HP, full, mode;
-    unsigned long long pairs;
+    bool tc = false;                 // tensor-core sweep of terms [p_lo, p_lo + nterms)
+    int ksteps = 0, n_live = 0;
+    unsigned long long pairs;        // C(K, w) of the level (witness rank width)
+    unsigned long long range_pairs;  // pairs of this plan's terms
     int p_lo, nterms;
     std::vector<unsigned long long> term_jobs;
     unsigned long long jobs;
@@ -334,10 +372,17 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     const auto tp0 = std::chrono::steady_clock::now();
     outs.assign(reqs.size(), LevelOut());
     if (reqs.empty()) return kOk;
+    const int tcM = tc_tile_rows(), tcN = tc_tile_cols(), tcJB = tc_job_tiles();
 
-    // 1) plan every (request, set)
+    // 1) plan every (request, set); a full-rank set may split into a tensor-core plan for
+    //    the terms whose rectangles fill the MMA tiles and CUDA-core plans for the rest
     std::vector<Plan> plans;
-    unsigned long long total_pairs = 0;
+    unsigned long long cc_pairs = 0;
+    auto range_pairs = [&](int K, int a, int b, int p0, int n) {
+        unsigned long long acc = 0;
+        for (int p = p0; p < p0 + n; ++p) acc += dev->binom(p, a - 1) * dev->binom(K - 1 - p, b);
+        return acc;
+    };
     for (size_t r = 0; r < reqs.size(); ++r) {
         const LevelReq& q = reqs[r];
         SideDev* S = q.side;
@@ -367,52 +412,115 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             P.pairs = pairs;
             P.p_lo = a - 1;
             P.nterms = K - b - a + 1;
-            total_pairs += pairs;
-            plans.push_back(std::move(P));
+            int ks = 0, nl = 0;
+            if (tensor_enabled() && P.full && P.HP >= 2 && b > 0)
+                ks = tc_depth(nred, T - 1 - w, P.popcs, &nl);
+            if (pairs > (1ull << 26) && std::getenv("QSFB_DEBUG") &&
+                std::getenv("QSFB_DEBUG")[0] == '2')
+                std::fprintf(stderr, "qsfb plan: K=%d w=%d a=%d b=%d nred=%d rank=%d HP=%d T=%d "
+                             "mode=%d filt=%d ks=%d\n", K, w, a, b, nred, rank, P.HP, T, P.mode,
+                             P.filt, ks);
+            int p1 = -1, p2 = -1;
+            if (ks > 0) {
+                // terms whose rectangles keep at least half of every tile busy
+                for (int p = P.p_lo; p < P.p_lo + P.nterms; ++p) {
+                    if (dev->binom(p, a - 1) >= (unsigned long long)(tcM / 2) &&
+                        dev->binom(K - 1 - p, b) >= (unsigned long long)(tcN / 2)) {
+                        if (p1 < 0) p1 = p;
+                        p2 = p;
+                    }
+                }
+            }
+            if (p1 < 0) {
+                P.range_pairs = pairs;
+                cc_pairs += pairs;
+                plans.push_back(std::move(P));
+                continue;
+            }
+            const int p_end = P.p_lo + P.nterms;   // one past the last term
+            Plan TP = P;
+            TP.tc = true;
+            TP.ksteps = ks;
+            TP.n_live = nl;
+            TP.p_lo = p1;
+            TP.nterms = p2 - p1 + 1;
+            TP.range_pairs = range_pairs(K, a, b, p1, TP.nterms);
+            if (p1 > P.p_lo) {
+                Plan L = P;
+                L.nterms = p1 - P.p_lo;
+                L.range_pairs = range_pairs(K, a, b, L.p_lo, L.nterms);
+                cc_pairs += L.range_pairs;
+                plans.push_back(std::move(L));
+            }
+            if (p2 + 1 < p_end) {
+                Plan R = P;
+                R.p_lo = p2 + 1;
+                R.nterms = p_end - R.p_lo;
+                R.range_pairs = range_pairs(K, a, b, R.p_lo, R.nterms);
+                cc_pairs += R.range_pairs;
+                plans.push_back(std::move(R));
+            }
+            plans.push_back(std::move(TP));
         }
     }
     // loop tile: enough jobs to keep every resident warp busy several times over
     // ~16 jobs per resident warp: the launch tail (one job) stays a few % of the level
     const unsigned long long want_jobs = (unsigned long long)dev->num_sms * 24 * 16;
-    unsigned long long lt = total_pairs / ((unsigned long long)kRegTile * want_jobs);
+    unsigned long long lt = cc_pairs / ((unsigned long long)kRegTile * want_jobs);
     lt = std::max<unsigned long long>(32, std::min<unsigned long long>(1024, lt));
     const int loop_tile = (int)((lt + 31) / 32 * 32);
 
-    // 2) lists to build
+    // 2) lists to build: packed probe words for every plan, +-1 rows for tensor plans
     struct GenReq { SideDev* S; int g, size, reflect, HP; };
+    struct ExpReq { SideDev* S; int g, size, reflect, HP, n_enc; };
     std::vector<GenReq> gens;
+    std::vector<ExpReq> exps;
     // the `queued` marks only live for this call, whatever path it leaves by
     struct ClearQueued {
         std::vector<GenReq>& g;
+        std::vector<ExpReq>& e;
         ~ClearQueued() {
             for (const GenReq& G : g) G.S->lists[std::make_tuple(G.g, G.size, G.reflect)].queued = false;
+            for (const ExpReq& E : e)
+                E.S->lists[std::make_tuple(E.g, E.size, E.reflect)].pm_queued = false;
         }
-    } clear_queued{gens};
+    } clear_queued{gens, exps};
     for (const Plan& P : plans) {
         SideDev* S = reqs[P.req].side;
         for (int side = 0; side < 2; ++side) {
-            const int size = side == 0 ? P.a : P.b;
+            const int size = side == 0 ? P.a : P.b;   // b = 0: one empty entry
             auto key = std::make_tuple(P.g, size, side);
             ListBuf& L = S->lists[key];
-            if (L.ready || L.queued) continue;
-            if (L.words) {   // allocated by an earlier execution: regenerate in place
-                L.queued = true;
-                gens.push_back({S, P.g, size, side, P.HP});
-                continue;
+            if (!(L.ready || L.queued)) {
+                if (L.words) {   // allocated by an earlier execution: regenerate in place
+                    L.queued = true;
+                    gens.push_back({S, P.g, size, side, P.HP});
+                } else {
+                    L.queued = true;
+                    L.count = dev->binom(S->K, size);
+                    L.bytes_w = std::max<size_t>((size_t)L.count * P.HP * 4, 16);
+                    L.arena = S->arena != nullptr;
+                    L.words = (uint32_t*)(L.arena ? S->arena->alloc(L.bytes_w) : dev->alloc(L.bytes_w));
+                    if (!L.words) { L.queued = false; return kErrMemory; }
+                    if (!P.full) {
+                        L.bytes_pc = std::max<size_t>((size_t)L.count, 16);
+                        L.pc = (uint8_t*)(L.arena ? S->arena->alloc(L.bytes_pc) : dev->alloc(L.bytes_pc));
+                        if (!L.pc) { L.queued = false; return kErrMemory; }
+                    }
+                    S->list_bytes += L.bytes_w + L.bytes_pc;
+                    gens.push_back({S, P.g, size, side, P.HP});
+                }
             }
-            L.queued = true;
-            L.count = dev->binom(S->K, size);
-            L.bytes_w = std::max<size_t>((size_t)L.count * P.HP * 4, 16);
-            L.arena = S->arena != nullptr;
-            L.words = (uint32_t*)(L.arena ? S->arena->alloc(L.bytes_w) : dev->alloc(L.bytes_w));
-            if (!L.words) { L.queued = false; return kErrMemory; }
-            if (!P.full) {
-                L.bytes_pc = std::max<size_t>((size_t)L.count, 16);
-                L.pc = (uint8_t*)(L.arena ? S->arena->alloc(L.bytes_pc) : dev->alloc(L.bytes_pc));
-                if (!L.pc) { L.queued = false; return kErrMemory; }
+            if (!P.tc || L.pm_ready || L.pm_queued) continue;
+            if (!L.pm) {
+                L.bytes_pm = (size_t)(L.count + kPmPadRows) * kPmRowBytes;
+                L.pm = (int8_t*)(L.arena ? S->arena->alloc(L.bytes_pm) : dev->alloc(L.bytes_pm));
+                if (!L.pm) return kErrMemory;
+                S->list_bytes += L.bytes_pm;
             }
-            S->list_bytes += L.bytes_w + L.bytes_pc;
-            gens.push_back({S, P.g, size, side, P.HP});
+            L.pm_queued = true;
+            const int nred = (int)S->nonpivot[P.g].size();
+            exps.push_back({S, P.g, size, side, P.HP, std::min(nred, kPmRowBytes)});
         }
     }
 
@@ -425,20 +533,28 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             const int p = P.p_lo + t;
             const unsigned long long nx = dev->binom(p, P.a - 1);
             const unsigned long long ny = dev->binom(K - 1 - p, P.b);
-            const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
             P.term_jobs[t] = acc;
-            acc += ((rn + kRegTile - 1) / kRegTile) * ((ln + loop_tile - 1) / loop_tile);
+            if (P.tc) {
+                // prefix tiles from the 8-aligned start of the block x suffix-tile chunks
+                const unsigned long long xoff = dev->binom(p, P.a);
+                const unsigned long long na = ((xoff & 7ull) + nx + tcM - 1) / tcM;
+                const unsigned long long nbt = (ny + tcN - 1) / tcN;
+                acc += na * ((nbt + tcJB - 1) / tcJB);
+            } else {
+                const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
+                acc += ((rn + kRegTile - 1) / kRegTile) * ((ln + loop_tile - 1) / loop_tile);
+            }
         }
         P.term_jobs[P.nterms] = acc;
         P.jobs = acc;
     }
 
-    // variant groups: (H, full) -> plan indices
+    // launch groups: CUDA-core variants (filter, HP, mode), then one tensor-core group
     std::vector<int> order(plans.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return std::make_tuple(plans[x].filt, plans[x].HP, plans[x].mode) <
-               std::make_tuple(plans[y].filt, plans[y].HP, plans[y].mode);
+        return std::make_tuple(plans[x].tc, plans[x].filt, plans[x].HP, plans[x].mode) <
+               std::make_tuple(plans[y].tc, plans[y].filt, plans[y].HP, plans[y].mode);
     });
 
     // 4) staging layout
@@ -446,6 +562,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     size_t off = 0;
     const size_t off_gen = off;
     off = align_up(off + gens.size() * sizeof(GenDesc), 64);
+    const size_t off_exp = off;
+    off = align_up(off + exps.size() * sizeof(ExpandDesc), 64);
     const size_t off_lvl = off;
     off = align_up(off + nplans * sizeof(LevelDesc), 64);
     const size_t off_terms = off;
@@ -455,7 +573,9 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     const size_t off_keys = off;
     off = align_up(off + reqs.size() * 8, 64);
     const size_t off_counts = off;
-    off = align_up(off + nplans * 8, 64);
+    off = off + nplans * 8;
+    const size_t off_err = off;
+    off = align_up(off + 8, 64);
     const size_t total_bytes = off;
     int rc = s->ensure(total_bytes, total_bytes);
     if (rc != kOk) return rc;
@@ -482,6 +602,21 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.reflect = G.reflect;
         gen_total += L.count;
     }
+    ExpandDesc* he = (ExpandDesc*)(h + off_exp);
+    unsigned long long exp_total = 0;
+    for (size_t i = 0; i < exps.size(); ++i) {
+        const ExpReq& E = exps[i];
+        ListBuf& L = E.S->lists[std::make_tuple(E.g, E.size, E.reflect)];
+        ExpandDesc& D = he[i];
+        D.words = L.words;
+        D.out = L.pm;
+        D.chunk_base = exp_total;
+        D.count = L.count;
+        D.rows = L.count + kPmPadRows;
+        D.HP = E.HP;
+        D.n_enc = E.n_enc;
+        exp_total += D.rows * (kPmRowBytes / 16);
+    }
 
     unsigned long long* hkeys = (unsigned long long*)(h + off_keys);
     for (size_t r = 0; r < reqs.size(); ++r)
@@ -490,13 +625,14 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     LevelDesc* hl = (LevelDesc*)(h + off_lvl);
     unsigned long long* hterms = (unsigned long long*)(h + off_terms);
     size_t term_cursor = 0;
-    struct Group { int filt, HP, mode, first, count; unsigned long long jobs; };
+    struct Group { bool tc; int filt, HP, mode, first, count; unsigned long long jobs; };
     std::vector<Group> groups;
     for (size_t oi = 0; oi < order.size(); ++oi) {
         const Plan& P = plans[order[oi]];
-        if (groups.empty() || groups.back().filt != P.filt || groups.back().HP != P.HP ||
-            groups.back().mode != P.mode)
-            groups.push_back({P.filt, P.HP, P.mode, (int)oi, 0, 0ull});
+        if (groups.empty() || groups.back().tc != P.tc ||
+            (!P.tc && (groups.back().filt != P.filt || groups.back().HP != P.HP ||
+                       groups.back().mode != P.mode)))
+            groups.push_back({P.tc, P.filt, P.HP, P.mode, (int)oi, 0, 0ull});
         Group& Gp = groups.back();
         SideDev* S = reqs[P.req].side;
         LevelDesc& D = hl[oi];
@@ -525,6 +661,12 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         while (bits < 64 && (P.pairs - 1) >> bits) ++bits;
         D.rank_shift = std::max(0, bits - kKeyGShift);
         D.count_all = S->count_all ? 1 : 0;
+        if (P.tc) {
+            D.ksteps = P.ksteps;
+            D.n_live = P.n_live;
+            D.xpm = La.pm;
+            D.ypm = Rb.pm;
+        }
         Gp.jobs += P.jobs;
         Gp.count += 1;
     }
@@ -548,15 +690,29 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             return kErrDevice;
         ++launches;
     }
+    if (!exps.empty()) {
+        if (launch_expand_pm((const ExpandDesc*)(d + off_exp), (int)exps.size(), exp_total,
+                             dev->num_sms, st) != cudaSuccess)
+            return kErrDevice;
+        ++launches;
+    }
     cudaEvent_t evm;
     cudaEventCreate(&evm);
     cudaEventRecord(evm, st);
     unsigned long long all_jobs = 0;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& Gp = groups[gi];
-        if (launch_pairs(Gp.filt, Gp.HP, Gp.mode, (const LevelDesc*)(d + off_lvl) + Gp.first, Gp.count,
-                         Gp.jobs, (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
-                         dev->num_sms, st) != cudaSuccess) {
+        const LevelDesc* gd = (const LevelDesc*)(d + off_lvl) + Gp.first;
+        const cudaError_t e =
+            Gp.tc ? launch_pairs_tc(gd, Gp.count, Gp.jobs, dev->d_binom, (int*)(d + off_err),
+                                    dev->num_sms, st)
+                  : launch_pairs(Gp.filt, Gp.HP, Gp.mode, gd, Gp.count, Gp.jobs,
+                                 (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
+                                 dev->num_sms, st);
+        if (e != cudaSuccess) {
+            if (std::getenv("QSFB_DEBUG"))
+                std::fprintf(stderr, "qsfb: pair launch failed: %s\n", cudaGetErrorString(e));
+            cudaGetLastError();
             cudaEventDestroy(evm);
             return kErrDevice;
         }
@@ -564,10 +720,20 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         all_jobs += Gp.jobs;
     }
     cudaEventRecord(s->ev1, st);
-    if (cudaMemcpyAsync(h + off_keys, d + off_keys, off_counts + nplans * 8 - off_keys,
-                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaError_t se = cudaMemcpyAsync(h + off_keys, d + off_keys, off_err + 8 - off_keys,
+                                     cudaMemcpyDeviceToHost, st);
+    if (se == cudaSuccess) se = cudaStreamSynchronize(st);
+    if (se != cudaSuccess) {
+        if (std::getenv("QSFB_DEBUG"))
+            std::fprintf(stderr, "qsfb: level run failed: %s\n", cudaGetErrorString(se));
         cudaGetLastError();
+        cudaEventDestroy(evm);
+        return kErrDevice;
+    }
+    if (*(const int*)(h + off_err) != 0) {   // a tensor-core wait ran out
+        if (std::getenv("QSFB_DEBUG"))
+            std::fprintf(stderr, "qsfb: tensor-core sweep wait ran out (role %d)\n",
+                         *(const int*)(h + off_err));
         cudaEventDestroy(evm);
         return kErrDevice;
     }
@@ -575,6 +741,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         ListBuf& L = G.S->lists[std::make_tuple(G.g, G.size, G.reflect)];
         L.ready = true;
         L.queued = false;
+    }
+    for (const ExpReq& E : exps) {
+        ListBuf& L = E.S->lists[std::make_tuple(E.g, E.size, E.reflect)];
+        L.pm_ready = true;
+        L.pm_queued = false;
     }
 
     // 6) decode
@@ -592,13 +763,15 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             O.rank = k & kKeyRankMask;
         }
     }
-    unsigned long long popc = 0, zcw = 0;
+    unsigned long long popc = 0, zcw = 0, tcw = 0;
     for (size_t oi = 0; oi < order.size(); ++oi) {
         const Plan& P = plans[order[oi]];
-        outs[P.req].counts[P.g] = hcounts[order[oi]];
-        cw += hcounts[order[oi]];
-        if (P.mode == 2) zcw += hcounts[order[oi]];
-        else popc += hcounts[order[oi]] * (unsigned long long)P.popcs;
+        const unsigned long long c = hcounts[order[oi]];
+        outs[P.req].counts[P.g] += c;
+        cw += c;
+        if (P.tc) tcw += c;
+        else if (P.mode == 2) zcw += c;
+        else popc += c * (unsigned long long)P.popcs;
         const LevelDesc& D = hl[oi];
         if (outs[P.req].found && outs[P.req].g == P.g) outs[P.req].rank_shift = D.rank_shift;
     }
@@ -612,6 +785,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         stats->codewords += cw;
         stats->popc_issued += popc;
         stats->zero_codewords += zcw;
+        stats->tc_codewords += tcw;
         stats->launches += launches;
     }
     cudaEventDestroy(evm);

@@ -100,11 +100,14 @@ struct SessionLease {
 struct ListBuf {
     uint32_t* words = nullptr;
     uint8_t* pc = nullptr;
+    int8_t* pm = nullptr;  // +-1 rows for the tensor-core sweep (count + kPmPadRows rows)
     unsigned long long count = 0;
-    size_t bytes_w = 0, bytes_pc = 0;
+    size_t bytes_w = 0, bytes_pc = 0, bytes_pm = 0;
     bool ready = false;
+    bool pm_ready = false;
     bool arena = false;   // carved from an Arena (released with it)
     bool queued = false;  // scheduled for generation in the current run_levels call
+    bool pm_queued = false;
 };
 
 // Bump allocator over device chunks taken from the caching allocator; everything carved
@@ -178,6 +181,7 @@ struct RunStats {
     unsigned long long codewords = 0;
     unsigned long long popc_issued = 0;    // POPC the pair kernels issue (H per pair, 0 in zero mode)
     unsigned long long zero_codewords = 0; // codewords swept by the zero-test mode
+    unsigned long long tc_codewords = 0;   // codewords swept by the tensor-core kernel
     int launches = 0;
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)

@@ -44,7 +44,27 @@ struct LevelDesc {
     int loop_tile;            // loop-side entries per job
     int rank_shift;           // lex rank >> rank_shift goes into the key
     int count_all;            // 1: every nonzero codeword is a logical (no detector)
+    // tensor-core sweep only (null / 0 elsewhere): the two lists as signed +-1 int8 rows
+    // of kPmRowBytes (bit set -> +1, clear -> -1, beyond the live bits -> 0), 16-byte
+    // chunk c of row e stored at c ^ ((e >> 1) & 3) (the 64-byte swizzle of the operand)
+    int ksteps;               // 32-column MMA steps per pair (probe columns = 32 * ksteps)
+    const int8_t* xpm;        // la rows
+    const int8_t* ypm;        // rb rows
+    int n_live;               // live +-1 columns among the first 32 * ksteps
     int pad_;
+};
+
+constexpr int kPmRowBytes = 64;    // +-1 row: 64 int8 columns (the first two probe words)
+constexpr int kPmPadRows = 256;    // zero rows after every +-1 list (whole-tile copies)
+
+// One +-1 expansion: rows [0, rows) of `out` from the packed probe words of a list
+// (rows beyond `count` are written as zeros).
+struct ExpandDesc {
+    const uint32_t* words;    // count x HP
+    int8_t* out;              // rows x kPmRowBytes
+    unsigned long long chunk_base;  // first global 16-byte chunk of this descriptor
+    unsigned long long count, rows;
+    int HP, n_enc;            // live columns = min(non-pivot bits, 64)
 };
 
 // One list to generate: entries [0, count) of the colex (or reflected colex) order of the

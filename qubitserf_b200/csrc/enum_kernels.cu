@@ -20,48 +20,13 @@
 #include <cstdint>
 
 #include "engine_types.hpp"
+#include "enum_device.cuh"
 
 namespace qsfb {
 namespace dev {
 
-constexpr int kLd = kBinomMaxK + 1;
-constexpr int kMaxWords = 32;   // n <= 1024 bits after pivot removal; detector <= 1024 rows
-constexpr int kMaxW = 64;
 constexpr int RX = 8;           // register-side entries per lane
 constexpr int kChunk = 32;      // loop entries between survivor checks
-
-__device__ __forceinline__ unsigned long long binom(const unsigned long long* __restrict__ B,
-                                                    int n, int k) {
-    if (k < 0 || n < 0 || k > n) return 0ull;
-    return __ldg(B + (size_t)n * kLd + k);
-}
-
-// Colex unrank: the r-th s-subset of [0, hi) in colex order, written largest first into
-// c[0..s-1] (c[0] > c[1] > ...).  r = sum_i C(c_i, s - i).
-__device__ __forceinline__ void colex_unrank(const unsigned long long* __restrict__ B,
-                                             unsigned long long r, int s, int hi, int* c) {
-    for (int i = s; i >= 1; --i) {
-        // largest x in [i-1, hi-1] with C(x, i) <= r
-        int lo = i - 1, top = hi - 1;
-        while (lo < top) {
-            const int mid = (lo + top + 1) >> 1;
-            if (binom(B, mid, i) <= r) lo = mid; else top = mid - 1;
-        }
-        c[s - i] = lo;
-        r -= binom(B, lo, i);
-        hi = lo;
-    }
-}
-
-// Rows of entry e of a list: colex (reflect=0) rows ascending after reversal, or reflected
-// colex (reflect=1) rows K-1-c.  Writes rows ascending into rows[0..s-1].
-__device__ __forceinline__ void list_rows(const unsigned long long* __restrict__ B,
-                                          unsigned long long e, int s, int K, int reflect,
-                                          int* rows) {
-    int c[kMaxW];
-    colex_unrank(B, e, s, K, c);
-    for (int i = 0; i < s; ++i) rows[i] = reflect ? (K - 1 - c[i]) : c[s - 1 - i];
-}
 
 // ---------------------------------------------------------------- list generation
 __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restrict__ descs,
@@ -98,89 +63,6 @@ __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restric
         }
         if (D.pc) D.pc[e] = (uint8_t)pc;
     }
-}
-
-// ---------------------------------------------------------------- survivors
-// Lexicographic rank of sorted positions (the reference's unrank order,
-// cpp/qsf/combinatorics.hpp:52-61): C(K,w) - 1 - sum_i C(K-1-s_i, w-i).
-__device__ unsigned long long lex_rank(const unsigned long long* __restrict__ B,
-                                       const int* s, int w, int K) {
-    unsigned long long acc = 0;
-    for (int i = 0; i < w; ++i) acc += binom(B, K - 1 - s[i], w - i);
-    return binom(B, K, w) - 1ull - acc;
-}
-
-// Full evaluation of register entry `ereg` against the loop entries [l0, l0+ln).  Each pair
-// is first re-screened on all stored probe words (a lower bound on its weight) and only
-// then rebuilt from its rows.  Returns the (possibly lowered) strict bound T.
-__device__ __noinline__ int survivor_scan(const LevelDesc& D, const unsigned long long* __restrict__ B,
-                                          int regX, unsigned long long xoff,
-                                          unsigned long long ereg, int pc_reg,
-                                          unsigned long long l0, int ln, int T) {
-    const int sreg = regX ? D.a : D.b;
-    const int sloop = regX ? D.b : D.a;
-    const uint32_t* regbase = regX ? D.la + xoff * (unsigned long long)D.HP : D.rb;
-    const uint32_t* lbase = regX ? D.rb : D.la + xoff * (unsigned long long)D.HP;
-    const uint8_t* lpc = regX ? D.pcb : (D.pca ? D.pca + xoff : nullptr);
-    uint32_t xr[4];
-    for (int h = 0; h < D.HP; ++h) xr[h] = __ldg(regbase + ereg * D.HP + h);
-
-    int rreg[kMaxW], rloop[kMaxW];
-    if (regX) list_rows(B, xoff + ereg, D.a, D.K, 0, rreg);
-    else list_rows(B, ereg, D.b, D.K, 1, rreg);
-    uint32_t fr[kMaxWords], sr[kMaxWords];
-    for (int h = 0; h < D.W32; ++h) fr[h] = 0u;
-    for (int h = 0; h < D.SW; ++h) sr[h] = 0u;
-    for (int i = 0; i < sreg; ++i) {
-        const uint32_t* r = D.red + (size_t)rreg[i] * D.W32;
-        for (int h = 0; h < D.W32; ++h) fr[h] ^= __ldg(r + h);
-        const uint32_t* s = D.syn + (size_t)rreg[i] * D.SW;
-        for (int h = 0; h < D.SW; ++h) sr[h] ^= __ldg(s + h);
-    }
-    for (int j = 0; j < ln; ++j) {
-        const unsigned long long el = l0 + (unsigned long long)j;
-        const int pcl = lpc ? (int)__ldg(lpc + el) : sloop;
-        int lb = pc_reg + pcl;
-        for (int h = 0; h < D.HP; ++h) lb += __popc(xr[h] ^ __ldg(lbase + el * D.HP + h));
-        if (lb >= T) continue;
-        if (regX) list_rows(B, el, D.b, D.K, 1, rloop);
-        else list_rows(B, xoff + el, D.a, D.K, 0, rloop);
-        int wt = pc_reg + pcl;
-        uint32_t fl[kMaxWords];
-        for (int h = 0; h < D.W32; ++h) fl[h] = 0u;
-        for (int i = 0; i < sloop; ++i) {
-            const uint32_t* r = D.red + (size_t)rloop[i] * D.W32;
-            for (int h = 0; h < D.W32; ++h) fl[h] ^= __ldg(r + h);
-        }
-        for (int h = 0; h < D.W32; ++h) wt += __popc(fr[h] ^ fl[h]);
-        if (wt >= T) continue;
-        bool logical = D.count_all != 0;
-        if (!logical) {
-            uint32_t acc = 0u;
-            for (int h = 0; h < D.SW; ++h) {
-                uint32_t s = sr[h];
-                for (int i = 0; i < sloop; ++i) s ^= __ldg(D.syn + (size_t)rloop[i] * D.SW + h);
-                acc |= s;
-            }
-            logical = acc != 0u;
-        }
-        if (!logical) continue;
-        // sorted positions: prefix rows (all <= p) then suffix rows (all > p)
-        int pos[kMaxW];
-        const int* pre = regX ? rreg : rloop;
-        const int* suf = regX ? rloop : rreg;
-        for (int i = 0; i < D.a; ++i) pos[i] = pre[i];
-        for (int i = 0; i < D.b; ++i) pos[D.a + i] = suf[i];
-        const unsigned long long rk = lex_rank(B, pos, D.w, D.K) >> D.rank_shift;
-        const unsigned long long key = ((unsigned long long)(wt + 1) << kKeyWtShift) |
-                                       ((unsigned long long)D.g << kKeyGShift) |
-                                       (rk & kKeyRankMask);
-        const unsigned long long old = atomicMin(D.key, key);
-        const unsigned long long cur = old < key ? old : key;
-        const int nb = (int)(cur >> kKeyWtShift);
-        if (nb < T) T = nb;
-    }
-    return T;
 }
 
 // ---------------------------------------------------------------- pair sweep

@@ -1,6 +1,7 @@
 #include "filter_plan.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 namespace qsfb {
@@ -69,6 +70,18 @@ double filter_pass_rate(int filt, int nred, int t) {
     const int nb = std::min(std::max(nred, 0), kBits);
     std::call_once(g_once[fi][nb], fill_table, fi, nb);
     return g_cdf[fi][nb][std::min(t, kMaxT)];
+}
+
+double hamming_pass_rate(int bits, int t) {
+    if (t < 0) return 0.0;
+    if (t >= bits) return 1.0;
+    const double lp = -bits * std::log(2.0);
+    double acc = 0.0, lc = 0.0;
+    for (int i = 0; i <= t; ++i) {
+        if (i > 0) lc += std::log((double)(bits - i + 1) / i);
+        acc += std::exp(lc + lp);
+    }
+    return std::min(acc, 1.0);
 }
 
 FilterChoice choose_filter(int HP, int nred, int t, bool zero_test) {

@@ -26,4 +26,8 @@ FilterChoice choose_filter(int HP, int nred, int t, bool zero_test);
 // P(filter value <= t) under the fair-coin model (exposed for the tests of the planner).
 double filter_pass_rate(int filt, int nred, int t);
 
+// P(Binomial(bits, 1/2) <= t): pass rate of an exact Hamming-distance filter over `bits`
+// random columns (the tensor-core sweep's).
+double hamming_pass_rate(int bits, int t);
+
 }  // namespace qsfb

@@ -1,0 +1,534 @@
+// Tensor-core pair sweep (sm_100a tcgen05) for full-rank information sets.
+//
+// For a full-rank set every pair (P, Q) of a level weighs w + popc(red(P) ^ red(Q)); the
+// CUDA-core sweep bounds the popcount from below with a few POPCs per pair.  Here the
+// bound is an exact Hamming distance over the first 64 non-pivot columns, taken as an
+// integer matrix product: with bits written as +-1 int8 values,
+//     <x, y> = n_live - 2 * hamming(x, y)
+// over the n_live live columns (dead columns are 0 on both sides), so a 128 x 128 block
+// of pairs is two `tcgen05.mma.kind::i8` steps (K = 32 each) into a 32-bit TMEM
+// accumulator.  A pair can beat the bound T only if
+//     hamming <= T - 1 - w   <=>   <x, y> >= n_live - 2 (T - 1 - w),
+// so the read-back takes a running maximum over each 64-column slice of the accumulator
+// and hands the rare slices that reach the threshold to the exact survivor evaluation
+// shared with the CUDA-core sweep (same key, same tie-breaking, same counts).
+//
+// Data movement is what bounds this kernel, so every suffix row fetched into shared
+// memory serves 256 prefix rows: a job holds a 256-row prefix tile (two M = 128 halves,
+// 16 KB) and streams 128-row suffix tiles (8 KB) through an 8-deep ring; each suffix tile
+// feeds two accumulators, one per half.  Rows are 64 bytes, pre-swizzled in global memory
+// (16-byte chunk c of row e at c ^ ((e >> 1) & 3)), so a plain bulk copy of 8-row-aligned
+// rows lands in the 64-byte-swizzled K-major operand layout.
+//
+// CTA = 10 warps: warp 0 issues the bulk copies, warp 1 owns the TMEM allocation (four
+// 128-column accumulators = all 512 columns: two halves x double buffer) and issues the
+// MMAs from one thread, warps 2-9 read back (two warps per TMEM lane quarter, one per
+// half; `tcgen05.ld` of 128 columns).  Every wait is bounded (about two seconds of
+// %globaltimer); a wait that runs out sets the launch's error word (1 copy warp, 2 MMA
+// warp, 3 read-back warps: the first role that gave up) and the CTA winds down without
+// touching the device further.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "engine_types.hpp"
+#include "enum_device.cuh"
+
+namespace qsfb {
+namespace dev {
+
+constexpr int kTcM = 128;                  // rows per MMA (UMMA M)
+constexpr int kTcHalves = 2;               // MMA row blocks per prefix tile
+constexpr int kTcRows = kTcM * kTcHalves;  // prefix rows per tile
+constexpr int kTcN = 128;                  // suffix rows per tile (UMMA N)
+constexpr int kTcK = 2;                    // K = 32 steps (64 columns)
+constexpr int kTcBStages = 8;              // suffix tiles in flight
+constexpr int kTcJB = 16;                  // suffix tiles per job
+constexpr int kTcSlice = 64;               // accumulator columns per rescan slice
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcThreads = 32 * (2 + kTcEpiWarps);
+constexpr uint32_t kTcHalfBytes = kTcM * kPmRowBytes;      // 8 KB
+constexpr uint32_t kTcABytes = kTcRows * kPmRowBytes;      // 16 KB
+constexpr uint32_t kTcBBytes = kTcN * kPmRowBytes;         // 8 KB
+constexpr uint32_t kTcOffA = 0;                            // two prefix tiles
+constexpr uint32_t kTcOffB = 2 * kTcABytes;                // kTcBStages suffix tiles
+constexpr uint32_t kTcOffBar = kTcOffB + kTcBStages * kTcBBytes;
+constexpr uint32_t kTcSmem = kTcOffBar + 512 + 1024;       // + barriers, TMEM slot, alignment
+constexpr uint32_t kTcTmemCols = 2 * kTcHalves * kTcN;     // 512: buffers x halves x N
+constexpr unsigned long long kTcWaitNs = 2000000000ull;
+static_assert(kTcTmemCols <= 512, "TMEM holds 512 columns");
+static_assert(kPmRowBytes == 64, "operand rows are 64 bytes (64 int8 columns)");
+
+// instruction descriptor: D s32 (bits 4-5 = 2), A and B signed int8 (bits 7-9, 10-12 = 1),
+// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kTcIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the phase of `bar` with the given parity; false after ~2 s (error path).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try(bar, parity)) return true;
+        if (global_ns() - t0 > kTcWaitNs) return false;
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+// 1-D bulk copy global -> shared, completion counted on `bar` (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+// K-major operand, 64-byte swizzle: rows of 64 B, 8-row groups 512 B apart (SBO),
+// LBO unused (1), descriptor version 1, layout type 4.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 128 consecutive 32-bit accumulator columns of this thread's TMEM lane; the wait for
+// the load sits in the same statement, so no use of v can be scheduled before it.
+__device__ __forceinline__ void tmem_ld128(uint32_t taddr, int32_t (&v)[128]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x128.b32 {"
+        "%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63,"
+        "%64,%65,%66,%67,%68,%69,%70,%71,%72,%73,%74,%75,%76,%77,%78,%79,"
+        "%80,%81,%82,%83,%84,%85,%86,%87,%88,%89,%90,%91,%92,%93,%94,%95,"
+        "%96,%97,%98,%99,%100,%101,%102,%103,%104,%105,%106,%107,%108,%109,%110,%111,"
+        "%112,%113,%114,%115,%116,%117,%118,%119,%120,%121,%122,%123,%124,%125,%126,%127}, [%128];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+          "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]),
+          "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]),
+          "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]),
+          "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]),
+          "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]),
+          "=r"(v[61]), "=r"(v[62]), "=r"(v[63]), "=r"(v[64]), "=r"(v[65]), "=r"(v[66]),
+          "=r"(v[67]), "=r"(v[68]), "=r"(v[69]), "=r"(v[70]), "=r"(v[71]), "=r"(v[72]),
+          "=r"(v[73]), "=r"(v[74]), "=r"(v[75]), "=r"(v[76]), "=r"(v[77]), "=r"(v[78]),
+          "=r"(v[79]), "=r"(v[80]), "=r"(v[81]), "=r"(v[82]), "=r"(v[83]), "=r"(v[84]),
+          "=r"(v[85]), "=r"(v[86]), "=r"(v[87]), "=r"(v[88]), "=r"(v[89]), "=r"(v[90]),
+          "=r"(v[91]), "=r"(v[92]), "=r"(v[93]), "=r"(v[94]), "=r"(v[95]), "=r"(v[96]),
+          "=r"(v[97]), "=r"(v[98]), "=r"(v[99]), "=r"(v[100]), "=r"(v[101]), "=r"(v[102]),
+          "=r"(v[103]), "=r"(v[104]), "=r"(v[105]), "=r"(v[106]), "=r"(v[107]), "=r"(v[108]),
+          "=r"(v[109]), "=r"(v[110]), "=r"(v[111]), "=r"(v[112]), "=r"(v[113]), "=r"(v[114]),
+          "=r"(v[115]), "=r"(v[116]), "=r"(v[117]), "=r"(v[118]), "=r"(v[119]), "=r"(v[120]),
+          "=r"(v[121]), "=r"(v[122]), "=r"(v[123]), "=r"(v[124]), "=r"(v[125]), "=r"(v[126]),
+          "=r"(v[127])
+        : "r"(taddr)
+        : "memory");
+}
+
+// Shared setup of both tensor-core kernels: barriers by thread 0, TMEM by warp 1.
+__device__ __forceinline__ uint32_t tc_setup(uint32_t bar0, int nbar, const uint32_t* counts,
+                                             uint32_t* tmem_slot) {
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < nbar; ++i) mbar_init(bar0 + 8u * i, counts[i]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tmem_slot)), "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+}
+
+__device__ __forceinline__ void tc_teardown(uint32_t tmem) {
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTcTmemCols));
+}
+
+// One job: prefix tile `ia` (256 rows from the 8-aligned start of the term's block) against
+// suffix tiles [b0, b1) of the term's prefix of the suffix list.
+struct TcJob {
+    const LevelDesc* D;
+    unsigned long long xoff, nx, ny, r0;
+    unsigned long long b0, b1;   // suffix tiles
+};
+
+__device__ __forceinline__ TcJob tc_decode(const LevelDesc* __restrict__ descs, int ndesc,
+                                           unsigned long long job,
+                                           const unsigned long long* __restrict__ B) {
+    int lo = 0, hi = ndesc - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].job_base <= job) lo = mid; else hi = mid - 1;
+    }
+    const LevelDesc& D = descs[lo];
+    const unsigned long long local = job - D.job_base;
+    int tl = 0, th = D.nterms - 1;
+    while (tl < th) {
+        const int mid = (tl + th + 1) >> 1;
+        if (__ldg(D.term_jobs + mid) <= local) tl = mid; else th = mid - 1;
+    }
+    const unsigned long long idx = local - __ldg(D.term_jobs + tl);
+    const int p = D.p_lo + tl;
+    TcJob J;
+    J.D = &D;
+    J.nx = binom(B, p, D.a - 1);
+    J.ny = binom(B, D.K - 1 - p, D.b);
+    J.xoff = binom(B, p, D.a);
+    const unsigned long long nbt = (J.ny + kTcN - 1) / kTcN;
+    const unsigned long long nbc = (nbt + kTcJB - 1) / kTcJB;
+    const unsigned long long ia = idx / nbc, jc = idx - ia * nbc;
+    J.r0 = (J.xoff & ~7ull) + ia * kTcRows;
+    J.b0 = jc * kTcJB;
+    J.b1 = J.b0 + kTcJB < nbt ? J.b0 + kTcJB : nbt;
+    return J;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+pairs_tc_kernel(const LevelDesc* __restrict__ descs, int ndesc, unsigned long long total_jobs,
+                const unsigned long long* __restrict__ B, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte alignment of the operand tiles (covers the 512-byte swizzle atom)
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const uint32_t s0 = smem_u32(smem);
+    const uint32_t bar = s0 + kTcOffBar;
+    // barrier slots (8 bytes each): a_full 0-1, a_empty 2-3, b_full 4-11, b_empty 12-19,
+    // acc_full 20-21, acc_empty 22-23
+    auto a_full = [&](uint32_t i) { return bar + 8u * i; };
+    auto a_empty = [&](uint32_t i) { return bar + 8u * (2 + i); };
+    auto b_full = [&](uint32_t i) { return bar + 8u * (4 + i); };
+    auto b_empty = [&](uint32_t i) { return bar + 8u * (4 + kTcBStages + i); };
+    auto acc_full = [&](uint32_t i) { return bar + 8u * (4 + 2 * kTcBStages + i); };
+    auto acc_empty = [&](uint32_t i) { return bar + 8u * (6 + 2 * kTcBStages + i); };
+    constexpr int kNBar = 8 + 2 * kTcBStages;
+    uint32_t counts[kNBar];
+    for (int i = 0; i < kNBar; ++i) counts[i] = 1;
+    counts[6 + 2 * kTcBStages] = counts[7 + 2 * kTcBStages] = 32 * kTcEpiWarps;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 256);
+    const uint32_t tmem = tc_setup(bar, kNBar, counts, tmem_slot);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        // ------------------------------------------------------------ tile copies
+        if (lane == 0) {
+            uint32_t it_a = 0, it_b = 0;
+            bool ok = true;
+            for (unsigned long long job = blockIdx.x; ok && job < total_jobs; job += gridDim.x) {
+                const TcJob J = tc_decode(descs, ndesc, job, B);
+                const uint32_t sa = it_a & 1u;
+                if (!(ok = mbar_wait(a_empty(sa), ((it_a >> 1) & 1u) ^ 1u))) break;
+                mbar_expect_tx(a_full(sa), kTcABytes);
+                bulk_g2s(s0 + kTcOffA + sa * kTcABytes, J.D->xpm + J.r0 * kPmRowBytes, kTcABytes,
+                         a_full(sa));
+                ++it_a;
+                for (unsigned long long bt = J.b0; bt < J.b1; ++bt) {
+                    const uint32_t sb = it_b % kTcBStages;
+                    if (!(ok = mbar_wait(b_empty(sb), ((it_b / kTcBStages) & 1u) ^ 1u))) break;
+                    mbar_expect_tx(b_full(sb), kTcBBytes);
+                    bulk_g2s(s0 + kTcOffB + sb * kTcBBytes, J.D->ypm + bt * kTcN * kPmRowBytes,
+                             kTcBBytes, b_full(sb));
+                    ++it_b;
+                }
+            }
+            if (!ok) atomicCAS(err, 0, 1);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issue
+        if (lane == 0) {
+            uint32_t it_a = 0, it_b = 0, it_c = 0;
+            bool ok = true;
+            for (unsigned long long job = blockIdx.x; ok && job < total_jobs; job += gridDim.x) {
+                const TcJob J = tc_decode(descs, ndesc, job, B);
+                const uint32_t sa = it_a & 1u;
+                if (!(ok = mbar_wait(a_full(sa), (it_a >> 1) & 1u))) break;
+                tc_fence_after();
+                const uint32_t a_addr = s0 + kTcOffA + sa * kTcABytes;
+                for (unsigned long long bt = J.b0; bt < J.b1; ++bt) {
+                    const uint32_t sb = it_b % kTcBStages, ac = it_c & 1u;
+                    if (!(ok = mbar_wait(b_full(sb), (it_b / kTcBStages) & 1u))) break;
+                    if (!(ok = mbar_wait(acc_empty(ac), ((it_c >> 1) & 1u) ^ 1u))) break;
+                    tc_fence_after();
+                    const uint32_t b_addr = s0 + kTcOffB + sb * kTcBBytes;
+#pragma unroll
+                    for (int h = 0; h < kTcHalves; ++h)
+#pragma unroll
+                        for (int k = 0; k < kTcK; ++k)   // K = 32 int8 columns = 32 bytes
+                            mma_i8(tmem + (ac * kTcHalves + h) * kTcN,
+                                   smem_desc(a_addr + h * kTcHalfBytes + 32u * k),
+                                   smem_desc(b_addr + 32u * k), k > 0 ? 1u : 0u);
+                    mma_commit(b_empty(sb));
+                    mma_commit(acc_full(ac));
+                    ++it_b;
+                    ++it_c;
+                }
+                if (!ok) break;
+                mma_commit(a_empty(sa));
+                ++it_a;
+            }
+            if (!ok) atomicCAS(err, 0, 2);
+        }
+    } else {
+        // ------------------------------------------------------------ read-back
+        const int quarter = warp & 3;            // TMEM lanes [32*quarter, 32*quarter+32)
+        const int half = (warp - 2) >> 2;        // accumulator / prefix half
+        const int row = half * kTcM + quarter * 32 + lane;   // prefix-tile row
+        uint32_t it_c = 0;
+        bool ok = true;
+        for (unsigned long long job = blockIdx.x; ok && job < total_jobs; job += gridDim.x) {
+            const TcJob J = tc_decode(descs, ndesc, job, B);
+            const LevelDesc& D = *J.D;
+            const unsigned long long r = J.r0 + row;
+            const bool valid = r >= J.xoff && r < J.xoff + J.nx;
+            for (unsigned long long bt = J.b0; bt < J.b1; ++bt) {
+                const uint32_t ac = it_c & 1u;
+                ok = mbar_wait(acc_full(ac), (it_c >> 1) & 1u);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+                tc_fence_after();
+                __syncwarp();   // the TMEM load below is warp-collective
+                int T = (int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
+                const int thr = D.n_live - 2 * (T - 1 - D.w);
+                int32_t v[128];
+                tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (ac * kTcHalves + half) * kTcN,
+                           v);
+                tc_fence_before();
+                mbar_arrive(acc_empty(ac));
+                int m0 = v[0], m1 = v[64];
+#pragma unroll
+                for (int i = 1; i + 1 < 64; i += 2) {
+                    m0 = __vimax3_s32(v[i], v[i + 1], m0);
+                    m1 = __vimax3_s32(v[64 + i], v[65 + i], m1);
+                }
+                m0 = max(m0, v[63]);
+                m1 = max(m1, v[127]);
+                const uint32_t flags = (m0 >= thr ? 1u : 0u) | (m1 >= thr ? 2u : 0u);
+                if (valid && flags) {
+                    for (int sl = 0; sl < kTcN / kTcSlice; ++sl) {
+                        if (!(flags >> sl & 1u)) continue;
+                        const unsigned long long c0 = bt * kTcN + (unsigned long long)sl * kTcSlice;
+                        if (c0 >= J.ny) break;
+                        const int ln = (int)(J.ny - c0 < (unsigned long long)kTcSlice ? J.ny - c0 : kTcSlice);
+                        T = survivor_scan(D, B, 1, J.xoff, r - J.xoff, D.a, c0, ln, T);
+                    }
+                }
+                ++it_c;
+            }
+            if (!ok) break;
+            if (warp == 2 && lane == 0) {
+                const unsigned long long lo = J.r0 > J.xoff ? J.r0 : J.xoff;
+                const unsigned long long hi =
+                    J.r0 + kTcRows < J.xoff + J.nx ? J.r0 + kTcRows : J.xoff + J.nx;
+                const unsigned long long c_lo = J.b0 * kTcN;
+                const unsigned long long c_hi = J.b1 * kTcN < J.ny ? J.b1 * kTcN : J.ny;
+                if (hi > lo && c_hi > c_lo) atomicAdd(D.count, (hi - lo) * (c_hi - c_lo));
+            }
+        }
+        if (!ok && lane == 0) atomicCAS(err, 0, 3);
+    }
+    tc_teardown(tmem);
+}
+
+// +-1 expansion of packed probe words, one thread per 16-byte output chunk (16 columns).
+__global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __restrict__ descs,
+                                                        int ndesc, unsigned long long total) {
+    constexpr int kChunks = kPmRowBytes / 16;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long gc = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         gc < total; gc += stride) {
+        int lo = 0, hi = ndesc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (descs[mid].chunk_base <= gc) lo = mid; else hi = mid - 1;
+        }
+        const ExpandDesc& E = descs[lo];
+        const unsigned long long c = gc - E.chunk_base;
+        const unsigned long long e = c / kChunks;
+        const int j = (int)(c % kChunks);      // columns [16j, 16j + 16)
+        uint32_t bits = 0, live = 0;
+        if (e < E.count && (j >> 1) < E.HP) {
+            bits = (__ldg(E.words + e * E.HP + (j >> 1)) >> (16 * (j & 1))) & 0xFFFFu;
+            const int nl = E.n_enc - 16 * j;   // live columns in this chunk
+            live = nl >= 16 ? 0xFFFFu : (nl > 0 ? (1u << nl) - 1u : 0u);
+        }
+        uint32_t q[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const uint32_t b = (bits >> (4 * n)) & 0xFu, l = (live >> (4 * n)) & 0xFu;
+            // one byte per column: 0/1 spread of the nibble
+            const uint32_t sb = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
+            const uint32_t sl = (l & 1u) | ((l & 2u) << 7) | ((l & 4u) << 14) | ((l & 8u) << 21);
+            // set -> 0x01, clear -> 0xFF, dead -> 0x00
+            q[n] = (0xFFFFFFFFu - 0xFEu * sb) & (sl * 0xFFu);
+        }
+        const int pos = j ^ (int)((e >> 1) & 3);   // 64-byte swizzle
+        uint4* dst = reinterpret_cast<uint4*>(E.out + e * kPmRowBytes + pos * 16);
+        *dst = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+}
+
+// Self-test of the operand layout: D = A (256 x 64) * B (128 x 64)^T through the same
+// copy / MMA / TMEM path (both halves), written out as 256 x 128 s32.  A and B are rows
+// in the pre-swizzled layout.
+__global__ void __launch_bounds__(kTcThreads, 1)
+tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, int ksteps,
+                   int32_t* __restrict__ out, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const uint32_t s0 = smem_u32(smem);
+    const uint32_t bar = s0 + kTcOffBar;   // 0: operands landed, 1: accumulators ready
+    const uint32_t counts[2] = {1, 1};
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 256);
+    const uint32_t tmem = tc_setup(bar, 2, counts, tmem_slot);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        mbar_expect_tx(bar, kTcABytes + kTcBBytes);
+        bulk_g2s(s0 + kTcOffA, A, kTcABytes, bar);
+        bulk_g2s(s0 + kTcOffB, Bm, kTcBBytes, bar);
+    }
+    if (warp == 1 && lane == 0) {
+        ok = mbar_wait(bar, 0);
+        if (ok) {
+            tc_fence_after();
+            for (int h = 0; h < kTcHalves; ++h)
+                for (int k = 0; k < ksteps; ++k)
+                    mma_i8(tmem + h * kTcN, smem_desc(s0 + kTcOffA + h * kTcHalfBytes + 32u * k),
+                           smem_desc(s0 + kTcOffB + 32u * k), k > 0 ? 1u : 0u);
+            mma_commit(bar + 8);
+        } else {
+            atomicCAS(err, 0, 2);
+        }
+    }
+    if (warp >= 2) {
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        ok = mbar_wait(bar + 8, 0);
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+            tc_fence_after();
+            __syncwarp();
+            int32_t v[128];
+            tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + half * kTcN, v);
+            int32_t* o = out + (size_t)(half * kTcM + quarter * 32 + lane) * kTcN;
+            for (int i = 0; i < kTcN; ++i) o[i] = v[i];
+        } else if (lane == 0) {
+            atomicCAS(err, 0, 3);
+        }
+    }
+    tc_teardown(tmem);
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------- host launchers
+int tc_tile_rows() { return dev::kTcRows; }
+int tc_tile_cols() { return dev::kTcN; }
+int tc_job_tiles() { return dev::kTcJB; }
+
+cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_chunks,
+                             int num_sms, cudaStream_t st) {
+    if (total_chunks == 0) return cudaSuccess;
+    unsigned long long blocks = (total_chunks + 255) / 256;
+    const unsigned long long cap = (unsigned long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    dev::expand_pm_kernel<<<(unsigned)blocks, 256, 0, st>>>(d, nd, total_chunks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
+                            const unsigned long long* B, int* err, int num_sms, cudaStream_t st) {
+    if (jobs == 0) return cudaSuccess;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(dev::pairs_tc_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)dev::kTcSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    unsigned long long blocks = (unsigned long long)num_sms;
+    if (jobs < blocks) blocks = jobs;
+    dev::pairs_tc_kernel<<<(unsigned)blocks, dev::kTcThreads, dev::kTcSmem, st>>>(d, nd, jobs, B,
+                                                                                 err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int32_t* out,
+                               int* err, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(dev::tc_selftest_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)dev::kTcSmem);
+    if (e != cudaSuccess) return e;
+    dev::tc_selftest_kernel<<<1, dev::kTcThreads, dev::kTcSmem, st>>>(A, Bm, ksteps, out, err);
+    return cudaGetLastError();
+}
+
+}  // namespace qsfb
