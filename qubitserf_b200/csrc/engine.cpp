@@ -18,7 +18,9 @@ cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
 cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_chunks,
                              int num_sms, cudaStream_t st);
 cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
-                            const unsigned long long* B, int* err, int num_sms, cudaStream_t st);
+                            const unsigned long long* B, void* job_recs, int* err, int num_sms,
+                            cudaStream_t st);
+size_t tc_job_record_bytes();
 int tc_tile_rows();
 int tc_tile_cols();
 int tc_job_tiles();
@@ -525,6 +527,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     }
 
     // 3) term tables and job counts
+    unsigned long long tc_jobs = 0;
     for (Plan& P : plans) {
         const int K = reqs[P.req].side->K;
         P.term_jobs.assign(P.nterms + 1, 0ull);
@@ -547,6 +550,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         }
         P.term_jobs[P.nterms] = acc;
         P.jobs = acc;
+        if (P.tc) tc_jobs += acc;
     }
 
     // launch groups: CUDA-core variants (filter, HP, mode), then one tensor-core group
@@ -576,8 +580,10 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     off = off + nplans * 8;
     const size_t off_err = off;
     off = align_up(off + 8, 64);
-    const size_t total_bytes = off;
-    int rc = s->ensure(total_bytes, total_bytes);
+    const size_t total_bytes = off;                 // host-written part
+    const size_t off_recs = off;                    // device-only: decoded tensor-core jobs
+    off = align_up(off + tc_jobs * tc_job_record_bytes(), 64);
+    int rc = s->ensure(off, total_bytes);
     if (rc != kOk) return rc;
     char* h = (char*)s->h_stage.h;
     char* d = (char*)s->d_stage.d;
@@ -704,8 +710,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         const Group& Gp = groups[gi];
         const LevelDesc* gd = (const LevelDesc*)(d + off_lvl) + Gp.first;
         const cudaError_t e =
-            Gp.tc ? launch_pairs_tc(gd, Gp.count, Gp.jobs, dev->d_binom, (int*)(d + off_err),
-                                    dev->num_sms, st)
+            Gp.tc ? launch_pairs_tc(gd, Gp.count, Gp.jobs, dev->d_binom, d + off_recs,
+                                    (int*)(d + off_err), dev->num_sms, st)
                   : launch_pairs(Gp.filt, Gp.HP, Gp.mode, gd, Gp.count, Gp.jobs,
                                  (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
                                  dev->num_sms, st);

@@ -214,48 +214,76 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem) {
                      "r"(kTcTmemCols));
 }
 
-// One job: prefix tile `ia` (256 rows from the 8-aligned start of the term's block) against
-// suffix tiles [b0, b1) of the term's prefix of the suffix list.
-struct TcJob {
-    const LevelDesc* D;
-    unsigned long long xoff, nx, ny, r0;
-    unsigned long long b0, b1;   // suffix tiles
+// One job: prefix tile rows [r0, r0 + 256) (from the 8-aligned start of the term's block)
+// against suffix tiles [b0, b1) of the term's prefix of the suffix list.  A small kernel
+// decodes every job of the launch into one record (binary searches over the descriptors
+// and terms, one thread per job); the sweep's roles then read their next record one job
+// ahead, so decoding costs them no dependent global loads.
+struct TcJobRec {
+    unsigned long long r0, xoff, nx, ny;
+    unsigned int d, b0, b1, pad;
 };
+static_assert(sizeof(TcJobRec) == 48, "job record layout");
 
-__device__ __forceinline__ TcJob tc_decode(const LevelDesc* __restrict__ descs, int ndesc,
-                                           unsigned long long job,
-                                           const unsigned long long* __restrict__ B) {
-    int lo = 0, hi = ndesc - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (descs[mid].job_base <= job) lo = mid; else hi = mid - 1;
+__global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restrict__ descs,
+                                                      int ndesc, unsigned long long total,
+                                                      const unsigned long long* __restrict__ B,
+                                                      TcJobRec* __restrict__ recs) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long job = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         job < total; job += stride) {
+        int lo = 0, hi = ndesc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (descs[mid].job_base <= job) lo = mid; else hi = mid - 1;
+        }
+        const LevelDesc& D = descs[lo];
+        const unsigned long long local = job - D.job_base;
+        int tl = 0, th = D.nterms - 1;
+        while (tl < th) {
+            const int mid = (tl + th + 1) >> 1;
+            if (__ldg(D.term_jobs + mid) <= local) tl = mid; else th = mid - 1;
+        }
+        const unsigned long long idx = local - __ldg(D.term_jobs + tl);
+        const int p = D.p_lo + tl;
+        TcJobRec R;
+        R.nx = binom(B, p, D.a - 1);
+        R.ny = binom(B, D.K - 1 - p, D.b);
+        R.xoff = binom(B, p, D.a);
+        const unsigned long long nbt = (R.ny + kTcN - 1) / kTcN;
+        const unsigned long long nbc = (nbt + kTcJB - 1) / kTcJB;
+        const unsigned long long ia = idx / nbc, jc = idx - ia * nbc;
+        R.r0 = (R.xoff & ~7ull) + ia * kTcRows;
+        R.b0 = (unsigned int)(jc * kTcJB);
+        R.b1 = (unsigned int)(jc * kTcJB + kTcJB < nbt ? jc * kTcJB + kTcJB : nbt);
+        R.d = (unsigned int)lo;
+        R.pad = 0;
+        recs[job] = R;
     }
-    const LevelDesc& D = descs[lo];
-    const unsigned long long local = job - D.job_base;
-    int tl = 0, th = D.nterms - 1;
-    while (tl < th) {
-        const int mid = (tl + th + 1) >> 1;
-        if (__ldg(D.term_jobs + mid) <= local) tl = mid; else th = mid - 1;
+}
+
+__device__ __forceinline__ TcJobRec tc_rec(const TcJobRec* __restrict__ recs,
+                                           unsigned long long job, unsigned long long total) {
+    TcJobRec R;
+    if (job < total) {
+        const uint4* q = reinterpret_cast<const uint4*>(recs + job);
+        const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        R.r0 = (unsigned long long)a.x | ((unsigned long long)a.y << 32);
+        R.xoff = (unsigned long long)a.z | ((unsigned long long)a.w << 32);
+        R.nx = (unsigned long long)b.x | ((unsigned long long)b.y << 32);
+        R.ny = (unsigned long long)b.z | ((unsigned long long)b.w << 32);
+        R.d = c.x; R.b0 = c.y; R.b1 = c.z; R.pad = 0;
+    } else {
+        R.r0 = R.xoff = R.nx = R.ny = 0;
+        R.d = R.b0 = R.b1 = R.pad = 0;
     }
-    const unsigned long long idx = local - __ldg(D.term_jobs + tl);
-    const int p = D.p_lo + tl;
-    TcJob J;
-    J.D = &D;
-    J.nx = binom(B, p, D.a - 1);
-    J.ny = binom(B, D.K - 1 - p, D.b);
-    J.xoff = binom(B, p, D.a);
-    const unsigned long long nbt = (J.ny + kTcN - 1) / kTcN;
-    const unsigned long long nbc = (nbt + kTcJB - 1) / kTcJB;
-    const unsigned long long ia = idx / nbc, jc = idx - ia * nbc;
-    J.r0 = (J.xoff & ~7ull) + ia * kTcRows;
-    J.b0 = jc * kTcJB;
-    J.b1 = J.b0 + kTcJB < nbt ? J.b0 + kTcJB : nbt;
-    return J;
+    return R;
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-pairs_tc_kernel(const LevelDesc* __restrict__ descs, int ndesc, unsigned long long total_jobs,
-                const unsigned long long* __restrict__ B, int* __restrict__ err) {
+pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict__ recs,
+                unsigned long long total_jobs, const unsigned long long* __restrict__ B,
+                int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte alignment of the operand tiles (covers the 512-byte swizzle atom)
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -277,27 +305,33 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, int ndesc, unsigned long lo
     const uint32_t tmem = tc_setup(bar, kNBar, counts, tmem_slot);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long j0 = blockIdx.x, js = gridDim.x;
     if (warp == 0) {
         // ------------------------------------------------------------ tile copies
         if (lane == 0) {
             uint32_t it_a = 0, it_b = 0;
             bool ok = true;
-            for (unsigned long long job = blockIdx.x; ok && job < total_jobs; job += gridDim.x) {
-                const TcJob J = tc_decode(descs, ndesc, job, B);
+            TcJobRec R = tc_rec(recs, j0, total_jobs);
+            for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
+                const TcJobRec N = tc_rec(recs, job + js, total_jobs);   // next, in flight
+                const LevelDesc& D = descs[R.d];
+                const int8_t* xpm = D.xpm;
+                const int8_t* ypm = D.ypm;
                 const uint32_t sa = it_a & 1u;
                 if (!(ok = mbar_wait(a_empty(sa), ((it_a >> 1) & 1u) ^ 1u))) break;
                 mbar_expect_tx(a_full(sa), kTcABytes);
-                bulk_g2s(s0 + kTcOffA + sa * kTcABytes, J.D->xpm + J.r0 * kPmRowBytes, kTcABytes,
+                bulk_g2s(s0 + kTcOffA + sa * kTcABytes, xpm + R.r0 * kPmRowBytes, kTcABytes,
                          a_full(sa));
                 ++it_a;
-                for (unsigned long long bt = J.b0; bt < J.b1; ++bt) {
+                for (unsigned long long bt = R.b0; bt < R.b1; ++bt) {
                     const uint32_t sb = it_b % kTcBStages;
                     if (!(ok = mbar_wait(b_empty(sb), ((it_b / kTcBStages) & 1u) ^ 1u))) break;
                     mbar_expect_tx(b_full(sb), kTcBBytes);
-                    bulk_g2s(s0 + kTcOffB + sb * kTcBBytes, J.D->ypm + bt * kTcN * kPmRowBytes,
+                    bulk_g2s(s0 + kTcOffB + sb * kTcBBytes, ypm + bt * kTcN * kPmRowBytes,
                              kTcBBytes, b_full(sb));
                     ++it_b;
                 }
+                R = N;
             }
             if (!ok) atomicCAS(err, 0, 1);
         }
@@ -306,13 +340,16 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, int ndesc, unsigned long lo
         if (lane == 0) {
             uint32_t it_a = 0, it_b = 0, it_c = 0;
             bool ok = true;
-            for (unsigned long long job = blockIdx.x; ok && job < total_jobs; job += gridDim.x) {
-                const TcJob J = tc_decode(descs, ndesc, job, B);
+            TcJobRec R = tc_rec(recs, j0, total_jobs);
+            for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
+                const TcJobRec N = tc_rec(recs, job + js, total_jobs);
+                const unsigned int tb0 = R.b0, tb1 = R.b1;
+                R = N;
                 const uint32_t sa = it_a & 1u;
                 if (!(ok = mbar_wait(a_full(sa), (it_a >> 1) & 1u))) break;
                 tc_fence_after();
                 const uint32_t a_addr = s0 + kTcOffA + sa * kTcABytes;
-                for (unsigned long long bt = J.b0; bt < J.b1; ++bt) {
+                for (unsigned int bt = tb0; bt < tb1; ++bt) {
                     const uint32_t sb = it_b % kTcBStages, ac = it_c & 1u;
                     if (!(ok = mbar_wait(b_full(sb), (it_b / kTcBStages) & 1u))) break;
                     if (!(ok = mbar_wait(acc_empty(ac), ((it_c >> 1) & 1u) ^ 1u))) break;
@@ -343,20 +380,25 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, int ndesc, unsigned long lo
         const int row = half * kTcM + quarter * 32 + lane;   // prefix-tile row
         uint32_t it_c = 0;
         bool ok = true;
-        for (unsigned long long job = blockIdx.x; ok && job < total_jobs; job += gridDim.x) {
-            const TcJob J = tc_decode(descs, ndesc, job, B);
-            const LevelDesc& D = *J.D;
-            const unsigned long long r = J.r0 + row;
-            const bool valid = r >= J.xoff && r < J.xoff + J.nx;
-            for (unsigned long long bt = J.b0; bt < J.b1; ++bt) {
+        TcJobRec R = tc_rec(recs, j0, total_jobs);
+        for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
+            const TcJobRec C = R;
+            R = tc_rec(recs, job + js, total_jobs);   // next, in flight
+            const LevelDesc& D = descs[C.d];
+            const unsigned long long r0 = C.r0, b0 = C.b0, b1 = C.b1;
+            const unsigned long long r = r0 + row;
+            const bool valid = r >= C.xoff && r < C.xoff + C.nx;
+            // the bound is read once per job (a stale, larger bound only adds rescans)
+            int T = (int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
+            const int n_live = D.n_live, w = D.w;
+            for (unsigned long long bt = b0; bt < b1; ++bt) {
                 const uint32_t ac = it_c & 1u;
                 ok = mbar_wait(acc_full(ac), (it_c >> 1) & 1u);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
                 tc_fence_after();
                 __syncwarp();   // the TMEM load below is warp-collective
-                int T = (int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
-                const int thr = D.n_live - 2 * (T - 1 - D.w);
+                const int thr = n_live - 2 * (T - 1 - w);
                 int32_t v[128];
                 tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (ac * kTcHalves + half) * kTcN,
                            v);
@@ -375,20 +417,20 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, int ndesc, unsigned long lo
                     for (int sl = 0; sl < kTcN / kTcSlice; ++sl) {
                         if (!(flags >> sl & 1u)) continue;
                         const unsigned long long c0 = bt * kTcN + (unsigned long long)sl * kTcSlice;
-                        if (c0 >= J.ny) break;
-                        const int ln = (int)(J.ny - c0 < (unsigned long long)kTcSlice ? J.ny - c0 : kTcSlice);
-                        T = survivor_scan(D, B, 1, J.xoff, r - J.xoff, D.a, c0, ln, T);
+                        if (c0 >= C.ny) break;
+                        const int ln = (int)(C.ny - c0 < (unsigned long long)kTcSlice ? C.ny - c0 : kTcSlice);
+                        T = survivor_scan(D, B, 1, C.xoff, r - C.xoff, D.a, c0, ln, T);
                     }
                 }
                 ++it_c;
             }
             if (!ok) break;
             if (warp == 2 && lane == 0) {
-                const unsigned long long lo = J.r0 > J.xoff ? J.r0 : J.xoff;
+                const unsigned long long lo = r0 > C.xoff ? r0 : C.xoff;
                 const unsigned long long hi =
-                    J.r0 + kTcRows < J.xoff + J.nx ? J.r0 + kTcRows : J.xoff + J.nx;
-                const unsigned long long c_lo = J.b0 * kTcN;
-                const unsigned long long c_hi = J.b1 * kTcN < J.ny ? J.b1 * kTcN : J.ny;
+                    r0 + kTcRows < C.xoff + C.nx ? r0 + kTcRows : C.xoff + C.nx;
+                const unsigned long long c_lo = b0 * kTcN;
+                const unsigned long long c_hi = b1 * kTcN < C.ny ? b1 * kTcN : C.ny;
                 if (hi > lo && c_hi > c_lo) atomicAdd(D.count, (hi - lo) * (c_hi - c_lo));
             }
         }
@@ -503,9 +545,19 @@ cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long tot
     return cudaGetLastError();
 }
 
+size_t tc_job_record_bytes() { return sizeof(dev::TcJobRec); }
+
 cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
-                            const unsigned long long* B, int* err, int num_sms, cudaStream_t st) {
+                            const unsigned long long* B, void* job_recs, int* err, int num_sms,
+                            cudaStream_t st) {
     if (jobs == 0) return cudaSuccess;
+    dev::TcJobRec* recs = (dev::TcJobRec*)job_recs;
+    {
+        unsigned long long blocks = (jobs + 255) / 256;
+        const unsigned long long cap = (unsigned long long)num_sms * 8;
+        if (blocks > cap) blocks = cap;
+        dev::tc_jobs_kernel<<<(unsigned)blocks, 256, 0, st>>>(d, nd, jobs, B, recs);
+    }
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(dev::pairs_tc_kernel,
@@ -516,8 +568,8 @@ cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
     }
     unsigned long long blocks = (unsigned long long)num_sms;
     if (jobs < blocks) blocks = jobs;
-    dev::pairs_tc_kernel<<<(unsigned)blocks, dev::kTcThreads, dev::kTcSmem, st>>>(d, nd, jobs, B,
-                                                                                 err);
+    dev::pairs_tc_kernel<<<(unsigned)blocks, dev::kTcThreads, dev::kTcSmem, st>>>(d, recs, jobs,
+                                                                                 B, err);
     return cudaGetLastError();
 }
 
