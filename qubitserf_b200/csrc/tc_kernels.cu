@@ -412,14 +412,41 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 }
                 m0 = max(m0, v[63]);
                 m1 = max(m1, v[127]);
-                const uint32_t flags = (m0 >= thr ? 1u : 0u) | (m1 >= thr ? 2u : 0u);
-                if (valid && flags) {
+                const uint32_t flags = valid ? ((m0 >= thr ? 1u : 0u) | (m1 >= thr ? 2u : 0u)) : 0u;
+                // Flagged slices are rescanned by the whole warp: the 32 lanes screen the
+                // slice's 64 pairs on every stored probe word at once (an exact lower bound
+                // on the weight), and only pairs still under the bound are rebuilt.
+                uint32_t need = __ballot_sync(0xffffffffu, flags != 0u);
+                while (need) {
+                    const int src = __ffs(need) - 1;
+                    need &= need - 1u;
+                    const unsigned long long rr = __shfl_sync(0xffffffffu, r, src);
+                    const uint32_t fl = __shfl_sync(0xffffffffu, flags, src);
+                    const int HP = D.HP;
+                    uint32_t xr[4] = {0u, 0u, 0u, 0u};
+                    for (int h = 0; h < HP; ++h) xr[h] = __ldg(D.la + rr * HP + h);
                     for (int sl = 0; sl < kTcN / kTcSlice; ++sl) {
-                        if (!(flags >> sl & 1u)) continue;
-                        const unsigned long long c0 = bt * kTcN + (unsigned long long)sl * kTcSlice;
-                        if (c0 >= C.ny) break;
-                        const int ln = (int)(C.ny - c0 < (unsigned long long)kTcSlice ? C.ny - c0 : kTcSlice);
-                        T = survivor_scan(D, B, 1, C.xoff, r - C.xoff, D.a, c0, ln, T);
+                        if (!(fl >> sl & 1u)) continue;
+                        for (int part = 0; part < kTcSlice / 32; ++part) {
+                            const unsigned long long c =
+                                bt * kTcN + (unsigned long long)(sl * kTcSlice + part * 32 + lane);
+                            bool cand = false;
+                            if (c < C.ny) {
+                                int lb = D.a + D.b;
+                                for (int h = 0; h < HP; ++h)
+                                    lb += __popc(xr[h] ^ __ldg(D.rb + c * HP + h));
+                                cand = lb < T;
+                            }
+                            uint32_t cm = __ballot_sync(0xffffffffu, cand);
+                            while (cm) {
+                                const int s2 = __ffs(cm) - 1;
+                                cm &= cm - 1u;
+                                const unsigned long long cc = __shfl_sync(0xffffffffu, c, s2);
+                                int Tn = T;
+                                if (lane == 0) Tn = survivor_scan(D, B, 1, C.xoff, rr - C.xoff, D.a, cc, 1, T);
+                                T = __shfl_sync(0xffffffffu, Tn, 0);
+                            }
+                        }
                     }
                 }
                 ++it_c;
