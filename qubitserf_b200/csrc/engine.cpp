@@ -15,7 +15,7 @@ cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long lo
 cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
-cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_chunks,
+cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_rows,
                              int num_sms, cudaStream_t st);
 cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
                             const unsigned long long* B, void* job_recs, int* err, int num_sms,
@@ -415,7 +415,9 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             P.p_lo = a - 1;
             P.nterms = K - b - a + 1;
             int ks = 0, nl = 0;
-            if (tensor_enabled() && P.full && P.HP >= 2 && b > 0)
+            // (+-1 lists hold 64 bytes per entry: keep them, and their 32-bit row indices, modest)
+            if (tensor_enabled() && P.full && P.HP >= 2 && b > 0 &&
+                dev->binom(K, a) < (1ull << 28) && dev->binom(K, b) < (1ull << 28))
                 ks = tc_depth(nred, T - 1 - w, P.popcs, &nl);
             if (pairs > (1ull << 26) && std::getenv("QSFB_DEBUG") &&
                 std::getenv("QSFB_DEBUG")[0] == '2')
@@ -616,12 +618,12 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         ExpandDesc& D = he[i];
         D.words = L.words;
         D.out = L.pm;
-        D.chunk_base = exp_total;
+        D.row_base = exp_total;
         D.count = L.count;
         D.rows = L.count + kPmPadRows;
         D.HP = E.HP;
         D.n_enc = E.n_enc;
-        exp_total += D.rows * (kPmRowBytes / 16);
+        exp_total += D.rows;
     }
 
     unsigned long long* hkeys = (unsigned long long*)(h + off_keys);

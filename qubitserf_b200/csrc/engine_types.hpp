@@ -62,7 +62,7 @@ constexpr int kPmPadRows = 256;    // zero rows after every +-1 list (whole-tile
 struct ExpandDesc {
     const uint32_t* words;    // count x HP
     int8_t* out;              // rows x kPmRowBytes
-    unsigned long long chunk_base;  // first global 16-byte chunk of this descriptor
+    unsigned long long row_base;  // first global row of this descriptor
     unsigned long long count, rows;
     int HP, n_enc;            // live columns = min(non-pivot bits, 64)
 };

@@ -23,7 +23,8 @@
 // CTA = 10 warps: warp 0 issues the bulk copies, warp 1 owns the TMEM allocation (four
 // 128-column accumulators = all 512 columns: two halves x double buffer) and issues the
 // MMAs from one thread, warps 2-9 read back (two warps per TMEM lane quarter, one per
-// half; `tcgen05.ld` of 128 columns).  Every wait is bounded (about two seconds of
+// half; one `tcgen05.ld` of 128 columns per tile each).  Reading the accumulators back is
+// what bounds the sweep: 4 bytes of TMEM per pair against 64 MACs of MMA work.  Every wait is bounded (about two seconds of
 // %globaltimer); a wait that runs out sets the launch's error word (1 copy warp, 2 MMA
 // warp, 3 read-back warps: the first role that gave up) and the CTA winds down without
 // touching the device further.
@@ -44,7 +45,7 @@ constexpr int kTcK = 2;                    // K = 32 steps (64 columns)
 constexpr int kTcBStages = 8;              // suffix tiles in flight
 constexpr int kTcJB = 16;                  // suffix tiles per job
 constexpr int kTcSlice = 64;               // accumulator columns per rescan slice
-constexpr int kTcEpiWarps = 8;
+constexpr int kTcEpiWarps = 8;             // 2 halves x 4 lane quarters
 constexpr int kTcThreads = 32 * (2 + kTcEpiWarps);
 constexpr uint32_t kTcHalfBytes = kTcM * kPmRowBytes;      // 8 KB
 constexpr uint32_t kTcABytes = kTcRows * kPmRowBytes;      // 16 KB
@@ -146,8 +147,33 @@ __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// 128 consecutive 32-bit accumulator columns of this thread's TMEM lane; the wait for
-// the load sits in the same statement, so no use of v can be scheduled before it.
+// 64 consecutive 32-bit accumulator columns of this thread's TMEM lane; the wait for the
+// load sits in the same statement, so no use of v can be scheduled before it.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, int32_t (&v)[64]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {"
+        "%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+          "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]),
+          "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]),
+          "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]),
+          "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]),
+          "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]),
+          "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+        : "r"(taddr)
+        : "memory");
+}
+
+// 128 consecutive 32-bit accumulator columns of this thread's TMEM lane (load and wait in
+// one statement, as above).
 __device__ __forceinline__ void tmem_ld128(uint32_t taddr, int32_t (&v)[128]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x128.b32 {"
@@ -216,14 +242,22 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem) {
 
 // One job: prefix tile rows [r0, r0 + 256) (from the 8-aligned start of the term's block)
 // against suffix tiles [b0, b1) of the term's prefix of the suffix list.  A small kernel
-// decodes every job of the launch into one record (binary searches over the descriptors
-// and terms, one thread per job); the sweep's roles then read their next record one job
-// ahead, so decoding costs them no dependent global loads.
+// decodes every job of the launch into one 64-byte record (binary searches over the
+// descriptors and terms, one thread per job) that carries everything the steady state
+// needs: the two operand lists, the witness key, the bound as it stood at decode time and
+// the threshold constants.  The sweep's roles read their next record one job ahead, so a
+// job costs them no dependent global loads.  Row and entry indices fit 32 bits: a +-1 list
+// of 2^32 rows would need 256 GB.
 struct TcJobRec {
-    unsigned long long r0, xoff, nx, ny;
-    unsigned int d, b0, b1, pad;
+    const int8_t* xpm;
+    const int8_t* ypm;
+    unsigned long long* key;
+    unsigned int r0, xoff, nx, ny;
+    unsigned int d, b0, b1;
+    unsigned int tnw;     // bound field (bits 0-11) | n_live << 12 | w << 20
+    unsigned long long pad;
 };
-static_assert(sizeof(TcJobRec) == 48, "job record layout");
+static_assert(sizeof(TcJobRec) == 64, "job record layout");
 
 __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restrict__ descs,
                                                       int ndesc, unsigned long long total,
@@ -246,17 +280,25 @@ __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restric
         }
         const unsigned long long idx = local - __ldg(D.term_jobs + tl);
         const int p = D.p_lo + tl;
-        TcJobRec R;
-        R.nx = binom(B, p, D.a - 1);
-        R.ny = binom(B, D.K - 1 - p, D.b);
-        R.xoff = binom(B, p, D.a);
-        const unsigned long long nbt = (R.ny + kTcN - 1) / kTcN;
+        const unsigned long long nx = binom(B, p, D.a - 1);
+        const unsigned long long ny = binom(B, D.K - 1 - p, D.b);
+        const unsigned long long xoff = binom(B, p, D.a);
+        const unsigned long long nbt = (ny + kTcN - 1) / kTcN;
         const unsigned long long nbc = (nbt + kTcJB - 1) / kTcJB;
         const unsigned long long ia = idx / nbc, jc = idx - ia * nbc;
-        R.r0 = (R.xoff & ~7ull) + ia * kTcRows;
+        TcJobRec R;
+        R.xpm = D.xpm;
+        R.ypm = D.ypm;
+        R.key = D.key;
+        R.r0 = (unsigned int)((xoff & ~7ull) + ia * kTcRows);
+        R.xoff = (unsigned int)xoff;
+        R.nx = (unsigned int)nx;
+        R.ny = (unsigned int)ny;
+        R.d = (unsigned int)lo;
         R.b0 = (unsigned int)(jc * kTcJB);
         R.b1 = (unsigned int)(jc * kTcJB + kTcJB < nbt ? jc * kTcJB + kTcJB : nbt);
-        R.d = (unsigned int)lo;
+        const unsigned int T0 = (unsigned int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
+        R.tnw = (T0 & 0xFFFu) | ((unsigned int)D.n_live << 12) | ((unsigned int)D.w << 20);
         R.pad = 0;
         recs[job] = R;
     }
@@ -267,15 +309,18 @@ __device__ __forceinline__ TcJobRec tc_rec(const TcJobRec* __restrict__ recs,
     TcJobRec R;
     if (job < total) {
         const uint4* q = reinterpret_cast<const uint4*>(recs + job);
-        const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-        R.r0 = (unsigned long long)a.x | ((unsigned long long)a.y << 32);
-        R.xoff = (unsigned long long)a.z | ((unsigned long long)a.w << 32);
-        R.nx = (unsigned long long)b.x | ((unsigned long long)b.y << 32);
-        R.ny = (unsigned long long)b.z | ((unsigned long long)b.w << 32);
-        R.d = c.x; R.b0 = c.y; R.b1 = c.z; R.pad = 0;
+        const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+        R.xpm = (const int8_t*)((unsigned long long)a.x | ((unsigned long long)a.y << 32));
+        R.ypm = (const int8_t*)((unsigned long long)a.z | ((unsigned long long)a.w << 32));
+        R.key = (unsigned long long*)((unsigned long long)b.x | ((unsigned long long)b.y << 32));
+        R.r0 = b.z; R.xoff = b.w;
+        R.nx = c.x; R.ny = c.y; R.d = c.z; R.b0 = c.w;
+        R.b1 = d.x; R.tnw = d.y; R.pad = 0;
     } else {
-        R.r0 = R.xoff = R.nx = R.ny = 0;
-        R.d = R.b0 = R.b1 = R.pad = 0;
+        R.xpm = R.ypm = nullptr;
+        R.key = nullptr;
+        R.r0 = R.xoff = R.nx = R.ny = R.d = R.b0 = R.b1 = R.tnw = 0;
+        R.pad = 0;
     }
     return R;
 }
@@ -314,9 +359,8 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             TcJobRec R = tc_rec(recs, j0, total_jobs);
             for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
                 const TcJobRec N = tc_rec(recs, job + js, total_jobs);   // next, in flight
-                const LevelDesc& D = descs[R.d];
-                const int8_t* xpm = D.xpm;
-                const int8_t* ypm = D.ypm;
+                const int8_t* xpm = R.xpm;
+                const int8_t* ypm = R.ypm;
                 const uint32_t sa = it_a & 1u;
                 if (!(ok = mbar_wait(a_empty(sa), ((it_a >> 1) & 1u) ^ 1u))) break;
                 mbar_expect_tx(a_full(sa), kTcABytes);
@@ -375,22 +419,29 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
         }
     } else {
         // ------------------------------------------------------------ read-back
+        const int e = warp - 2;
         const int quarter = warp & 3;            // TMEM lanes [32*quarter, 32*quarter+32)
-        const int half = (warp - 2) >> 2;        // accumulator / prefix half
+        const int half = e >> 2;                 // accumulator / prefix half
         const int row = half * kTcM + quarter * 32 + lane;   // prefix-tile row
         uint32_t it_c = 0;
         bool ok = true;
         TcJobRec R = tc_rec(recs, j0, total_jobs);
+        const unsigned long long* kptr = nullptr;   // key of the previous job
+        int tkey = 0;                                // its value, loaded during that job
         for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
             const TcJobRec C = R;
             R = tc_rec(recs, job + js, total_jobs);   // next, in flight
-            const LevelDesc& D = descs[C.d];
+            const LevelDesc& D = descs[C.d];         // read only on the rare rescan path
             const unsigned long long r0 = C.r0, b0 = C.b0, b1 = C.b1;
             const unsigned long long r = r0 + row;
             const bool valid = r >= C.xoff && r < C.xoff + C.nx;
-            // the bound is read once per job (a stale, larger bound only adds rescans)
-            int T = (int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
-            const int n_live = D.n_live, w = D.w;
+            // Bound: the level's bound at decode time, tightened by the key value read
+            // during the previous job of the same level (a larger bound is always safe:
+            // it only flags more slices).  This job's read is consumed by the next one.
+            int T = (int)(C.tnw & 0xFFFu);
+            if (C.key == kptr) T = min(T, tkey);
+            const unsigned long long kv = *((volatile unsigned long long*)C.key);
+            const int n_live = (int)((C.tnw >> 12) & 0xFFu), w = (int)(C.tnw >> 20);
             for (unsigned long long bt = b0; bt < b1; ++bt) {
                 const uint32_t ac = it_c & 1u;
                 ok = mbar_wait(acc_full(ac), (it_c >> 1) & 1u);
@@ -404,15 +455,22 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                            v);
                 tc_fence_before();
                 mbar_arrive(acc_empty(ac));
-                int m0 = v[0], m1 = v[64];
+                // per 64-column slice, four independent 3-input max chains
+                uint32_t fbits = 0;
 #pragma unroll
-                for (int i = 1; i + 1 < 64; i += 2) {
-                    m0 = __vimax3_s32(v[i], v[i + 1], m0);
-                    m1 = __vimax3_s32(v[64 + i], v[65 + i], m1);
+                for (int sl = 0; sl < 2; ++sl) {
+                    int m[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int o = 64 * sl + 16 * c;
+                        m[c] = v[o];
+#pragma unroll
+                        for (int i = o + 1; i + 1 < o + 16; i += 2) m[c] = __vimax3_s32(v[i], v[i + 1], m[c]);
+                        m[c] = max(m[c], v[o + 15]);
+                    }
+                    if (max(max(m[0], m[1]), max(m[2], m[3])) >= thr) fbits |= 1u << sl;
                 }
-                m0 = max(m0, v[63]);
-                m1 = max(m1, v[127]);
-                const uint32_t flags = valid ? ((m0 >= thr ? 1u : 0u) | (m1 >= thr ? 2u : 0u)) : 0u;
+                const uint32_t flags = valid ? fbits : 0u;
                 // Flagged slices are rescanned by the whole warp: the 32 lanes screen the
                 // slice's 64 pairs on every stored probe word at once (an exact lower bound
                 // on the weight), and only pairs still under the bound are rebuilt.
@@ -452,6 +510,8 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 ++it_c;
             }
             if (!ok) break;
+            kptr = C.key;
+            tkey = min(T, (int)(kv >> kKeyWtShift));
             if (warp == 2 && lane == 0) {
                 const unsigned long long lo = r0 > C.xoff ? r0 : C.xoff;
                 const unsigned long long hi =
@@ -466,41 +526,49 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     tc_teardown(tmem);
 }
 
-// +-1 expansion of packed probe words, one thread per 16-byte output chunk (16 columns).
+// +-1 expansion of packed probe words, one thread per row: the first two probe words (64
+// columns) become 64 int8 values, written as four swizzled 16-byte chunks.
+__device__ __forceinline__ uint4 pm_chunk(uint32_t bits, uint32_t live) {
+    uint32_t q[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const uint32_t b = (bits >> (4 * n)) & 0xFu, l = (live >> (4 * n)) & 0xFu;
+        // one byte per column: 0/1 spread of the nibble
+        const uint32_t sb = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
+        const uint32_t sl = (l & 1u) | ((l & 2u) << 7) | ((l & 4u) << 14) | ((l & 8u) << 21);
+        // set -> 0x01, clear -> 0xFF, dead -> 0x00
+        q[n] = (0xFFFFFFFFu - 0xFEu * sb) & (sl * 0xFFu);
+    }
+    return make_uint4(q[0], q[1], q[2], q[3]);
+}
+
 __global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __restrict__ descs,
                                                         int ndesc, unsigned long long total) {
-    constexpr int kChunks = kPmRowBytes / 16;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long gc = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-         gc < total; gc += stride) {
+    for (unsigned long long ge = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         ge < total; ge += stride) {
         int lo = 0, hi = ndesc - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (descs[mid].chunk_base <= gc) lo = mid; else hi = mid - 1;
+            if (descs[mid].row_base <= ge) lo = mid; else hi = mid - 1;
         }
         const ExpandDesc& E = descs[lo];
-        const unsigned long long c = gc - E.chunk_base;
-        const unsigned long long e = c / kChunks;
-        const int j = (int)(c % kChunks);      // columns [16j, 16j + 16)
-        uint32_t bits = 0, live = 0;
-        if (e < E.count && (j >> 1) < E.HP) {
-            bits = (__ldg(E.words + e * E.HP + (j >> 1)) >> (16 * (j & 1))) & 0xFFFFu;
-            const int nl = E.n_enc - 16 * j;   // live columns in this chunk
-            live = nl >= 16 ? 0xFFFFu : (nl > 0 ? (1u << nl) - 1u : 0u);
+        const unsigned long long e = ge - E.row_base;
+        uint32_t w0 = 0u, w1 = 0u;
+        if (e < E.count) {
+            w0 = __ldg(E.words + e * E.HP);
+            if (E.HP > 1) w1 = __ldg(E.words + e * E.HP + 1);
         }
-        uint32_t q[4];
+        const int nl = e < E.count ? E.n_enc : 0;   // live columns of this row
+        uint4* row = reinterpret_cast<uint4*>(E.out + e * kPmRowBytes);
+        const int sw = (int)((e >> 1) & 3);           // 64-byte swizzle
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-            const uint32_t b = (bits >> (4 * n)) & 0xFu, l = (live >> (4 * n)) & 0xFu;
-            // one byte per column: 0/1 spread of the nibble
-            const uint32_t sb = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
-            const uint32_t sl = (l & 1u) | ((l & 2u) << 7) | ((l & 4u) << 14) | ((l & 8u) << 21);
-            // set -> 0x01, clear -> 0xFF, dead -> 0x00
-            q[n] = (0xFFFFFFFFu - 0xFEu * sb) & (sl * 0xFFu);
+        for (int j = 0; j < 4; ++j) {                 // columns [16j, 16j + 16)
+            const uint32_t bits = ((j < 2 ? w0 : w1) >> (16 * (j & 1))) & 0xFFFFu;
+            const int l = nl - 16 * j;
+            const uint32_t live = l >= 16 ? 0xFFFFu : (l > 0 ? (1u << l) - 1u : 0u);
+            row[j ^ sw] = pm_chunk(bits, live);
         }
-        const int pos = j ^ (int)((e >> 1) & 3);   // 64-byte swizzle
-        uint4* dst = reinterpret_cast<uint4*>(E.out + e * kPmRowBytes + pos * 16);
-        *dst = make_uint4(q[0], q[1], q[2], q[3]);
     }
 }
 
@@ -537,17 +605,19 @@ tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, 
             atomicCAS(err, 0, 2);
         }
     }
-    if (warp >= 2) {
+    if (warp >= 2 && warp < 10) {   // one warp per (half, lane quarter)
         const int quarter = warp & 3, half = (warp - 2) >> 2;
         ok = mbar_wait(bar + 8, 0);
         ok = __all_sync(0xffffffffu, ok);
         if (ok) {
             tc_fence_after();
             __syncwarp();
-            int32_t v[128];
-            tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + half * kTcN, v);
             int32_t* o = out + (size_t)(half * kTcM + quarter * 32 + lane) * kTcN;
-            for (int i = 0; i < kTcN; ++i) o[i] = v[i];
+            for (int cs = 0; cs < kTcN / kTcSlice; ++cs) {
+                int32_t v[64];
+                tmem_ld64(tmem + ((uint32_t)(quarter * 32) << 16) + half * kTcN + cs * kTcSlice, v);
+                for (int i = 0; i < 64; ++i) o[cs * kTcSlice + i] = v[i];
+            }
         } else if (lane == 0) {
             atomicCAS(err, 0, 3);
         }
@@ -562,13 +632,13 @@ int tc_tile_rows() { return dev::kTcRows; }
 int tc_tile_cols() { return dev::kTcN; }
 int tc_job_tiles() { return dev::kTcJB; }
 
-cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_chunks,
+cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_rows,
                              int num_sms, cudaStream_t st) {
-    if (total_chunks == 0) return cudaSuccess;
-    unsigned long long blocks = (total_chunks + 255) / 256;
+    if (total_rows == 0) return cudaSuccess;
+    unsigned long long blocks = (total_rows + 255) / 256;
     const unsigned long long cap = (unsigned long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
-    dev::expand_pm_kernel<<<(unsigned)blocks, 256, 0, st>>>(d, nd, total_chunks);
+    dev::expand_pm_kernel<<<(unsigned)blocks, 256, 0, st>>>(d, nd, total_rows);
     return cudaGetLastError();
 }
 
