@@ -1,5 +1,6 @@
 """Benchmark: certificates/s (exact BZ distances) on the 1024-code uneven batch, and the
-integer-pipe roofline of the pair-sweep kernel.
+roofline of the dominant pair-sweep kernel (the tcgen05 int8 sweep of full-rank sets; the
+CUDA-core POPC sweep's integer-pipe roofline is reported beside it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--mode batch|plain] [--codes 1024]
@@ -28,6 +29,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "certs/s batched vs plain on 1 B200 (exact d); Gcodewords/s vs int-pipe peak"
+TC_OPS_PER_PAIR = 2 * 64  # int8 multiply-adds of the tensor-core filter: 64 columns per pair
 POPC_PER_CLK_SM = 16     # 32-bit POPC results per clock per SM (CUDA arithmetic throughput table)
 
 
@@ -239,6 +241,7 @@ def main():
     barrier(pg)
     spans, pair_ms, cw, launches, rounds = [], 0.0, 0, 0, 0
     popc_issued, zero_cw = 0, 0
+    tc_ms, tc_cw = 0.0, 0
     popc_alg = 0.0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -249,6 +252,8 @@ def main():
             cw += st.codewords
             popc_issued += st.popc_issued
             zero_cw += st.zero_codewords
+            tc_ms += st.tc_ms
+            tc_cw += st.tc_codewords
             launches += st.kernel_launches
             rounds = st.rounds
     batch.free(handle)
@@ -270,7 +275,8 @@ def main():
                               "pair_ms": st.pair_ms, "gen_ms": st.gen_ms,
                               "host_plan_ms": st.host_plan_seconds * 1e3,
                               "host_apply_ms": st.host_apply_seconds * 1e3,
-                              "tc_share": st.tc_codewords / max(st.codewords, 1)}), flush=True)
+                              "tc_share": st.tc_codewords / max(st.codewords, 1),
+                              "tc_codewords": st.tc_codewords, "tc_ms": st.tc_ms}), flush=True)
         return
 
     # --- end to end: the one-shot public call from host matrices, K times
@@ -297,6 +303,16 @@ def main():
     peak_popc = nsm * POPC_PER_CLK_SM * f_mhz * 1e6
     pair_s = pair_ms / 1000.0
     achieved_cw = cw / max(pair_s, 1e-12)
+    # tensor-core sweep: int8 ops over its own CUDA-event time; peak = int8 dense, twice the
+    # measured bf16 rate (the kernel is timed alone in short launches: burst figure)
+    tc_s = max_over_ranks(pg, tc_ms / 1000.0)
+    tc_ops = tc_cw * TC_OPS_PER_PAIR / max(tc_s, 1e-12)
+    bf16 = pk.get("bf16_tflops")
+    tc_peak = (2.0 * bf16 * 1e12) if bf16 else 2.0 * 1.59e15
+    tc_traffic = tc_traffic_per_launch(tc_cw / max(args.steps, 1))
+    # CUDA-core sweep: the rest of the codewords over the rest of the pair-kernel time
+    cc_s = max(pair_s - tc_ms / 1000.0, 1e-12)
+    cc_cw_rate = (cw - tc_cw) / cc_s
     if rank != 0:
         return
     cpu = None if args.no_cpu_baseline else cpu_baseline_sample(codes)
@@ -304,23 +320,37 @@ def main():
         "metric": METRIC, "value": value, "unit": "certs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": span_s / args.steps * 1000.0,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i8",
         "data": "synthetic", "config": config,
         "plain_certs_per_s": plain, "batched_vs_plain": value / plain,
         "gcodewords_per_s": achieved_cw / 1e9,
         "codewords_per_step": cw / args.steps, "rounds_per_step": rounds,
         "roofline": {
+            "bound": "tensor", "kernel": "pairs_tc_kernel",
+            "achieved": tc_ops / 1e12, "peak": tc_peak / 1e12, "unit": "TOP/s (int8)",
+            "frac": tc_ops / tc_peak, "traffic": tc_traffic,
+            "peak_source": ("2 x measured bf16 dense (MEASURED_PEAKS.json bf16_tflops, burst)"
+                            if bf16 else "2 x fallback bf16 1.59 PFLOP/s"),
+            "numerator": "tensor-core codewords x 128 int8 ops (64 columns) / kernel time",
+            "binding": {"resource": "TMEM read-back of the s32 accumulators (4 B per pair)",
+                        "tmem_read_gbs": tc_cw * 4 / max(tc_s, 1e-12) / 1e9,
+                        "bytes_per_clk_per_sm": tc_cw * 4 / max(tc_s, 1e-12) /
+                                                (nsm * f_mhz * 1e6)},
+            "codeword_share": tc_cw / max(cw, 1),
+            "kernel_ms_per_step": tc_ms / max(args.steps, 1)},
+        "roofline_cuda_core": {
             "bound": "int-pipe (POPC on the XU pipe)", "kernel": "pairs_kernel",
-            "achieved": achieved_cw * popc_per_cw / 1e9, "peak": popc_peak / 1e9,
-            "unit": "Gpopc32/s", "frac": achieved_cw * popc_per_cw / popc_peak,
+            "achieved": cc_cw_rate * popc_per_cw / 1e9, "peak": popc_peak / 1e9,
+            "unit": "Gpopc32/s", "frac": cc_cw_rate * popc_per_cw / popc_peak,
             "traffic": traffic_per_launch(),
             "numerator": "codewords/s of the pair kernel x 2W POPC32 of the full evaluation "
                          "(W = ceil(n/64)); the kernel issues fewer (pivot columns removed, "
                          "probe words, zero test)",
             "peak_source": "measured: qsfb_microbench POPC chains over all SMs",
-            "kernel_popc_per_codeword": popc_issued / max(cw, 1),
-            "kernel_frac": popc_issued / max(pair_s, 1e-12) / popc_peak,
-            "zero_test_share": zero_cw / max(cw, 1),
+            "codewords_per_step": (cw - tc_cw) / max(args.steps, 1),
+            "kernel_popc_per_codeword": popc_issued / max(cw - tc_cw, 1),
+            "kernel_frac": popc_issued / max(cc_s, 1e-12) / popc_peak,
+            "zero_test_share": zero_cw / max(cw - tc_cw, 1),
             "lop3_peak_gops": lop3_peak / 1e9,
             "sm_mhz": f_mhz},
         "cpu_baseline": cpu,
@@ -334,6 +364,20 @@ def main():
                                         np.arange(1, len(dists) + 1))),
     }
     print(json.dumps(line), flush=True)
+
+
+def tc_traffic_per_launch(tc_cw_per_step):
+    """DRAM bytes per tensor-core launch: the committed per-codeword traffic of an ncu capture
+    on a smaller batch, scaled by the codewords of an average launch of this run."""
+    p = ROOT / "profiles" / "pairs_tc_kernel_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    per_cw = d.get("dram_bytes_per_codeword")
+    launches = d.get("launches_per_step_full_batch")
+    if per_cw is None or not launches:
+        return None
+    return per_cw * tc_cw_per_step / launches
 
 
 def traffic_per_launch():

@@ -74,7 +74,8 @@ class QsfbBatchStats(ctypes.Structure):
                 ("rounds", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong),
                 ("gen_ms", ctypes.c_double), ("host_plan_seconds", ctypes.c_double),
-                ("host_apply_seconds", ctypes.c_double), ("tc_codewords", ctypes.c_ulonglong)]
+                ("host_apply_seconds", ctypes.c_double), ("tc_codewords", ctypes.c_ulonglong),
+                ("tc_ms", ctypes.c_double)]
 
 
 class QsfbTiming(ctypes.Structure):

@@ -607,6 +607,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             stats->host_apply_s += rs.host_apply_s;
             stats->ms_gen += rs.ms_gen;
             stats->ms_pairs += rs.ms_pairs;
+            stats->ms_tc += rs.ms_tc;
             stats->jobs += rs.jobs;
             stats->codewords += rs.codewords;
             stats->popc_issued += rs.popc_issued;

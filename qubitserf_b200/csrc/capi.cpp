@@ -595,6 +595,7 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
         stats->device_ms = rs.ms_gen + rs.ms_pairs;
         stats->device_span_ms = span;
         stats->pair_ms = rs.ms_pairs;
+        stats->tc_ms = rs.ms_tc;
         stats->codewords = rs.codewords;
         stats->popc_issued = rs.popc_issued;
         stats->zero_codewords = rs.zero_codewords;

@@ -155,7 +155,8 @@ Session* Device::acquire() {
     Session* s = new Session();
     s->dev = this;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+        cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess ||
+        cudaEventCreate(&s->ev_tc0) != cudaSuccess || cudaEventCreate(&s->ev_tc1) != cudaSuccess) {
         cudaGetLastError();
         delete s;
         return nullptr;
@@ -554,6 +555,25 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         P.jobs = acc;
         if (P.tc) tc_jobs += acc;
     }
+    if (tc_jobs && std::getenv("QSFB_DEBUG") && std::getenv("QSFB_DEBUG")[0] == '3') {
+        unsigned long long tiles = 0, pairs = 0, atiles = 0;
+        for (const Plan& P : plans) {
+            if (!P.tc) continue;
+            const int K = reqs[P.req].side->K;
+            for (int t = 0; t < P.nterms; ++t) {
+                const int p = P.p_lo + t;
+                const unsigned long long nx = dev->binom(p, P.a - 1), ny = dev->binom(K - 1 - p, P.b);
+                const unsigned long long xoff = dev->binom(p, P.a);
+                const unsigned long long na = ((xoff & 7ull) + nx + tcM - 1) / tcM;
+                tiles += na * ((ny + tcN - 1) / tcN);
+                atiles += na * ((((ny + tcN - 1) / tcN) + tcJB - 1) / tcJB);
+                pairs += nx * ny;
+            }
+        }
+        std::fprintf(stderr, "qsfb tc launch: jobs=%llu tiles=%llu pairs=%llu tile_util=%.3f tiles_per_job=%.2f\n",
+                     tc_jobs, tiles, pairs, (double)pairs / ((double)tiles * tcM * tcN),
+                     (double)tiles / (double)tc_jobs);
+    }
 
     // launch groups: CUDA-core variants (filter, HP, mode), then one tensor-core group
     std::vector<int> order(plans.size());
@@ -708,9 +728,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     cudaEventCreate(&evm);
     cudaEventRecord(evm, st);
     unsigned long long all_jobs = 0;
+    bool tc_timed = false;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         const Group& Gp = groups[gi];
         const LevelDesc* gd = (const LevelDesc*)(d + off_lvl) + Gp.first;
+        if (Gp.tc) cudaEventRecord(s->ev_tc0, st);
         const cudaError_t e =
             Gp.tc ? launch_pairs_tc(gd, Gp.count, Gp.jobs, dev->d_binom, d + off_recs,
                                     (int*)(d + off_err), dev->num_sms, st)
@@ -723,6 +745,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             cudaGetLastError();
             cudaEventDestroy(evm);
             return kErrDevice;
+        }
+        if (Gp.tc) {
+            cudaEventRecord(s->ev_tc1, st);
+            tc_timed = true;
+            launches += 1;   // the job-decode kernel
         }
         ++launches;
         all_jobs += Gp.jobs;
@@ -789,6 +816,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         cudaEventElapsedTime(&b, evm, s->ev1);
         stats->ms_gen += a;
         stats->ms_pairs += b;
+        if (tc_timed) {
+            float c = 0.f;
+            cudaEventElapsedTime(&c, s->ev_tc0, s->ev_tc1);
+            stats->ms_tc += c;
+        }
         stats->jobs += all_jobs;
         stats->codewords += cw;
         stats->popc_issued += popc;

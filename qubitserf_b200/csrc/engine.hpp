@@ -83,6 +83,7 @@ struct Session {
     Device* dev = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_tc0 = nullptr, ev_tc1 = nullptr;   // around the tensor-core sweep
     DevScratch d_stage;    // descriptors + term tables + keys/counts
     HostScratch h_stage;   // pinned mirror of d_stage
     DevScratch d_ctr;      // job counters (one per kernel variant)
@@ -177,6 +178,7 @@ struct LevelOut {
 struct RunStats {
     double ms_gen = 0.0;     // device time of list generation
     double ms_pairs = 0.0;   // device time of the pair sweep
+    double ms_tc = 0.0;      // device time of the tensor-core sweep launches alone
     unsigned long long jobs = 0;
     unsigned long long codewords = 0;
     unsigned long long popc_issued = 0;    // POPC the pair kernels issue (H per pair, 0 in zero mode)

@@ -20,10 +20,10 @@
 // (16-byte chunk c of row e at c ^ ((e >> 1) & 3)), so a plain bulk copy of 8-row-aligned
 // rows lands in the 64-byte-swizzled K-major operand layout.
 //
-// CTA = 10 warps: warp 0 issues the bulk copies, warp 1 owns the TMEM allocation (four
-// 128-column accumulators = all 512 columns: two halves x double buffer) and issues the
-// MMAs from one thread, warps 2-9 read back (two warps per TMEM lane quarter, one per
-// half; one `tcgen05.ld` of 128 columns per tile each).  Reading the accumulators back is
+// CTA = 12 warps: warps 0 and 10 issue the bulk copies, warp 1 owns the TMEM allocation
+// (four 128-column accumulators = all 512 columns: two halves x double buffer), warps 1
+// and 11 issue the MMAs (one thread each, by suffix-tile parity), warps 2-9 read back (two
+// warps per TMEM lane quarter, one per half; one `tcgen05.ld` of 128 columns per tile).  Reading the accumulators back is
 // what bounds the sweep: 4 bytes of TMEM per pair against 64 MACs of MMA work.  Every wait is bounded (about two seconds of
 // %globaltimer); a wait that runs out sets the launch's error word (1 copy warp, 2 MMA
 // warp, 3 read-back warps: the first role that gave up) and the CTA winds down without
@@ -46,7 +46,7 @@ constexpr int kTcBStages = 8;              // suffix tiles in flight
 constexpr int kTcJB = 16;                  // suffix tiles per job
 constexpr int kTcSlice = 64;               // accumulator columns per rescan slice
 constexpr int kTcEpiWarps = 8;             // 2 halves x 4 lane quarters
-constexpr int kTcThreads = 32 * (2 + kTcEpiWarps);
+constexpr int kTcThreads = 32 * (4 + kTcEpiWarps);   // + two copy and two MMA warps
 constexpr uint32_t kTcHalfBytes = kTcM * kPmRowBytes;      // 8 KB
 constexpr uint32_t kTcABytes = kTcRows * kPmRowBytes;      // 16 KB
 constexpr uint32_t kTcBBytes = kTcN * kPmRowBytes;         // 8 KB
@@ -78,11 +78,13 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
 }
 
+// Non-suspending probe of a barrier phase: the pollers here are single threads on the
+// critical path, so they spin instead of sleeping through the phase change.
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(bar), "r"(parity)
@@ -90,12 +92,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Wait for the phase of `bar` with the given parity; false after ~2 s (error path).
+// Wait for the phase of `bar` with the given parity; false after ~2 s (error path).  The
+// timer is only consulted after a few thousand probes: normal waits are far shorter, and
+// a %globaltimer read on every wait would sit on the critical path.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    if (mbar_try(bar, parity)) return true;
+    for (int i = 0; i < 4096; ++i)
+        if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (;;) {
-        for (int i = 0; i < 64; ++i)
+        for (int i = 0; i < 1024; ++i)
             if (mbar_try(bar, parity)) return true;
         if (global_ns() - t0 > kTcWaitNs) return false;
     }
@@ -345,13 +350,22 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     constexpr int kNBar = 8 + 2 * kTcBStages;
     uint32_t counts[kNBar];
     for (int i = 0; i < kNBar; ++i) counts[i] = 1;
-    counts[6 + 2 * kTcBStages] = counts[7 + 2 * kTcBStages] = 32 * kTcEpiWarps;
+    counts[2] = counts[3] = 2;   // a prefix slot is released by both MMA threads
+    counts[6 + 2 * kTcBStages] = counts[7 + 2 * kTcBStages] = kTcEpiWarps;   // one per warp
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 256);
     const uint32_t tmem = tc_setup(bar, kNBar, counts, tmem_slot);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long j0 = blockIdx.x, js = gridDim.x;
-    if (warp == 0) {
+    // Copies and MMA issue are split by suffix-tile parity over two threads each (warps 0
+    // and 10 copy, warps 1 and 11 issue): every role is a chain of dependent barrier
+    // operations, and two chains per role keep the tensor pipe fed.  The thread of parity p
+    // owns the suffix stages of parity p and accumulator buffer p; the prefix tile is loaded
+    // by the parity-0 copier and released when both MMA threads have committed.
+    const bool is_copy = warp == 0 || warp == 10;
+    const bool is_mma = warp == 1 || warp == 11;
+    const uint32_t par = warp >= 10 ? 1u : 0u;
+    if (is_copy) {
         // ------------------------------------------------------------ tile copies
         if (lane == 0) {
             uint32_t it_a = 0, it_b = 0;
@@ -359,30 +373,31 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             TcJobRec R = tc_rec(recs, j0, total_jobs);
             for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
                 const TcJobRec N = tc_rec(recs, job + js, total_jobs);   // next, in flight
-                const int8_t* xpm = R.xpm;
                 const int8_t* ypm = R.ypm;
                 const uint32_t sa = it_a & 1u;
-                if (!(ok = mbar_wait(a_empty(sa), ((it_a >> 1) & 1u) ^ 1u))) break;
-                mbar_expect_tx(a_full(sa), kTcABytes);
-                bulk_g2s(s0 + kTcOffA + sa * kTcABytes, xpm + R.r0 * kPmRowBytes, kTcABytes,
-                         a_full(sa));
+                if (par == 0) {
+                    if (!(ok = mbar_wait(a_empty(sa), ((it_a >> 1) & 1u) ^ 1u))) break;
+                    mbar_expect_tx(a_full(sa), kTcABytes);
+                    bulk_g2s(s0 + kTcOffA + sa * kTcABytes, R.xpm + R.r0 * kPmRowBytes, kTcABytes,
+                             a_full(sa));
+                }
                 ++it_a;
-                for (unsigned long long bt = R.b0; bt < R.b1; ++bt) {
+                for (unsigned long long bt = R.b0; bt < R.b1; ++bt, ++it_b) {
+                    if ((it_b & 1u) != par) continue;
                     const uint32_t sb = it_b % kTcBStages;
                     if (!(ok = mbar_wait(b_empty(sb), ((it_b / kTcBStages) & 1u) ^ 1u))) break;
                     mbar_expect_tx(b_full(sb), kTcBBytes);
                     bulk_g2s(s0 + kTcOffB + sb * kTcBBytes, ypm + bt * kTcN * kPmRowBytes,
                              kTcBBytes, b_full(sb));
-                    ++it_b;
                 }
                 R = N;
             }
             if (!ok) atomicCAS(err, 0, 1);
         }
-    } else if (warp == 1) {
+    } else if (is_mma) {
         // ------------------------------------------------------------ MMA issue
         if (lane == 0) {
-            uint32_t it_a = 0, it_b = 0, it_c = 0;
+            uint32_t it_a = 0, it_b = 0;
             bool ok = true;
             TcJobRec R = tc_rec(recs, j0, total_jobs);
             for (unsigned long long job = j0; ok && job < total_jobs; job += js) {
@@ -390,13 +405,16 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 const unsigned int tb0 = R.b0, tb1 = R.b1;
                 R = N;
                 const uint32_t sa = it_a & 1u;
+                // both threads wait for the prefix tile before releasing it (keeps the
+                // two arrivals of every release phase from different jobs apart)
                 if (!(ok = mbar_wait(a_full(sa), (it_a >> 1) & 1u))) break;
                 tc_fence_after();
                 const uint32_t a_addr = s0 + kTcOffA + sa * kTcABytes;
-                for (unsigned int bt = tb0; bt < tb1; ++bt) {
-                    const uint32_t sb = it_b % kTcBStages, ac = it_c & 1u;
+                for (unsigned int bt = tb0; bt < tb1; ++bt, ++it_b) {
+                    if ((it_b & 1u) != par) continue;
+                    const uint32_t sb = it_b % kTcBStages, ac = par;   // buffer = tile parity
                     if (!(ok = mbar_wait(b_full(sb), (it_b / kTcBStages) & 1u))) break;
-                    if (!(ok = mbar_wait(acc_empty(ac), ((it_c >> 1) & 1u) ^ 1u))) break;
+                    if (!(ok = mbar_wait(acc_empty(ac), ((it_b >> 1) & 1u) ^ 1u))) break;
                     tc_fence_after();
                     const uint32_t b_addr = s0 + kTcOffB + sb * kTcBBytes;
 #pragma unroll
@@ -408,8 +426,6 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                                    smem_desc(b_addr + 32u * k), k > 0 ? 1u : 0u);
                     mma_commit(b_empty(sb));
                     mma_commit(acc_full(ac));
-                    ++it_b;
-                    ++it_c;
                 }
                 if (!ok) break;
                 mma_commit(a_empty(sa));
@@ -444,8 +460,9 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             const int n_live = (int)((C.tnw >> 12) & 0xFFu), w = (int)(C.tnw >> 20);
             for (unsigned long long bt = b0; bt < b1; ++bt) {
                 const uint32_t ac = it_c & 1u;
-                ok = mbar_wait(acc_full(ac), (it_c >> 1) & 1u);
-                ok = __all_sync(0xffffffffu, ok);
+                // one lane polls the barrier, the warp follows (256 pollers would contend)
+                if (lane == 0) ok = mbar_wait(acc_full(ac), (it_c >> 1) & 1u);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
                 if (!ok) break;
                 tc_fence_after();
                 __syncwarp();   // the TMEM load below is warp-collective
@@ -454,7 +471,8 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (ac * kTcHalves + half) * kTcN,
                            v);
                 tc_fence_before();
-                mbar_arrive(acc_empty(ac));
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty(ac));   // one arrival per warp
                 // per 64-column slice, four independent 3-input max chains
                 uint32_t fbits = 0;
 #pragma unroll
