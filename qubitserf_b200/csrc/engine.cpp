@@ -328,6 +328,16 @@ unsigned long long key_init(int bound) {
     return ((unsigned long long)f << kKeyWtShift) | ((1ull << kKeyWtShift) - 1);
 }
 
+// QSFB_DEBUG=<level>: diagnostics on stderr (1 failures, 2 plans of heavy levels, 3
+// tensor-core launch statistics); read once.
+int debug_level() {
+    static const int lvl = [] {
+        const char* e = std::getenv("QSFB_DEBUG");
+        return e ? std::atoi(e) : 0;
+    }();
+    return lvl;
+}
+
 // Tensor-core sweep switch: QSFB_TENSOR=0 keeps every level on the CUDA-core kernels.
 bool tensor_enabled() {
     static const bool on = [] {
@@ -420,8 +430,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             if (tensor_enabled() && P.full && P.HP >= 2 && b > 0 &&
                 dev->binom(K, a) < (1ull << 28) && dev->binom(K, b) < (1ull << 28))
                 ks = tc_depth(nred, T - 1 - w, P.popcs, &nl);
-            if (pairs > (1ull << 26) && std::getenv("QSFB_DEBUG") &&
-                std::getenv("QSFB_DEBUG")[0] == '2')
+            if (debug_level() == 2 && pairs > (1ull << 26))
                 std::fprintf(stderr, "qsfb plan: K=%d w=%d a=%d b=%d nred=%d rank=%d HP=%d T=%d "
                              "mode=%d filt=%d ks=%d\n", K, w, a, b, nred, rank, P.HP, T, P.mode,
                              P.filt, ks);
@@ -476,16 +485,23 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     const int loop_tile = (int)((lt + 31) / 32 * 32);
 
     // 2) lists to build: packed probe words for every plan, +-1 rows for tensor plans
-    struct GenReq { SideDev* S; int g, size, reflect, HP; };
+    // A list generated in this call writes its +-1 rows in the same pass when a tensor plan
+    // needs them; a list generated earlier gets them from the expansion kernel.
+    struct GenReq { SideDev* S; int g, size, reflect, HP; bool pm; int n_enc; };
     struct ExpReq { SideDev* S; int g, size, reflect, HP, n_enc; };
     std::vector<GenReq> gens;
     std::vector<ExpReq> exps;
+    std::vector<std::pair<int8_t*, size_t>> pad_zero;   // new +-1 buffers: zero their tail rows
     // the `queued` marks only live for this call, whatever path it leaves by
     struct ClearQueued {
         std::vector<GenReq>& g;
         std::vector<ExpReq>& e;
         ~ClearQueued() {
-            for (const GenReq& G : g) G.S->lists[std::make_tuple(G.g, G.size, G.reflect)].queued = false;
+            for (const GenReq& G : g) {
+                ListBuf& L = G.S->lists[std::make_tuple(G.g, G.size, G.reflect)];
+                L.queued = L.pm_queued = false;
+                L.gen_idx = -1;
+            }
             for (const ExpReq& E : e)
                 E.S->lists[std::make_tuple(E.g, E.size, E.reflect)].pm_queued = false;
         }
@@ -499,7 +515,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             if (!(L.ready || L.queued)) {
                 if (L.words) {   // allocated by an earlier execution: regenerate in place
                     L.queued = true;
-                    gens.push_back({S, P.g, size, side, P.HP});
+                    L.gen_idx = (int)gens.size();
+                    gens.push_back({S, P.g, size, side, P.HP, false, 0});
                 } else {
                     L.queued = true;
                     L.count = dev->binom(S->K, size);
@@ -513,7 +530,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                         if (!L.pc) { L.queued = false; return kErrMemory; }
                     }
                     S->list_bytes += L.bytes_w + L.bytes_pc;
-                    gens.push_back({S, P.g, size, side, P.HP});
+                    L.gen_idx = (int)gens.size();
+                    gens.push_back({S, P.g, size, side, P.HP, false, 0});
                 }
             }
             if (!P.tc || L.pm_ready || L.pm_queued) continue;
@@ -522,10 +540,18 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 L.pm = (int8_t*)(L.arena ? S->arena->alloc(L.bytes_pm) : dev->alloc(L.bytes_pm));
                 if (!L.pm) return kErrMemory;
                 S->list_bytes += L.bytes_pm;
+                pad_zero.push_back({L.pm + (size_t)L.count * kPmRowBytes,
+                                    (size_t)kPmPadRows * kPmRowBytes});
             }
             L.pm_queued = true;
             const int nred = (int)S->nonpivot[P.g].size();
-            exps.push_back({S, P.g, size, side, P.HP, std::min(nred, kPmRowBytes)});
+            const int n_enc = std::min(nred, kPmRowBytes);
+            if (L.queued && L.gen_idx >= 0) {   // generated in this call: fused
+                gens[L.gen_idx].pm = true;
+                gens[L.gen_idx].n_enc = n_enc;
+            } else {
+                exps.push_back({S, P.g, size, side, P.HP, n_enc});
+            }
         }
     }
 
@@ -555,7 +581,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         P.jobs = acc;
         if (P.tc) tc_jobs += acc;
     }
-    if (tc_jobs && std::getenv("QSFB_DEBUG") && std::getenv("QSFB_DEBUG")[0] == '3') {
+    if (tc_jobs && debug_level() == 3) {
         unsigned long long tiles = 0, pairs = 0, atiles = 0;
         for (const Plan& P : plans) {
             if (!P.tc) continue;
@@ -620,6 +646,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.red = G.S->d_red + (size_t)G.g * G.S->K * G.S->W32;
         D.out = L.words;
         D.pc = L.pc;
+        D.pm = G.pm ? L.pm : nullptr;
+        D.n_enc = G.n_enc;
         D.entry_base = gen_total;
         D.count = L.count;
         D.K = G.S->K;
@@ -710,6 +738,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         cudaGetLastError();
         return kErrDevice;
     }
+    for (const auto& z : pad_zero)
+        if (cudaMemsetAsync(z.first, 0, z.second, st) != cudaSuccess) {
+            cudaGetLastError();
+            return kErrDevice;
+        }
     cudaEventRecord(s->ev0, st);
     int launches = 0;
     if (!gens.empty()) {
@@ -740,7 +773,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                                  (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
                                  dev->num_sms, st);
         if (e != cudaSuccess) {
-            if (std::getenv("QSFB_DEBUG"))
+            if (debug_level() >= 1)
                 std::fprintf(stderr, "qsfb: pair launch failed: %s\n", cudaGetErrorString(e));
             cudaGetLastError();
             cudaEventDestroy(evm);
@@ -759,14 +792,14 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                                      cudaMemcpyDeviceToHost, st);
     if (se == cudaSuccess) se = cudaStreamSynchronize(st);
     if (se != cudaSuccess) {
-        if (std::getenv("QSFB_DEBUG"))
+        if (debug_level() >= 1)
             std::fprintf(stderr, "qsfb: level run failed: %s\n", cudaGetErrorString(se));
         cudaGetLastError();
         cudaEventDestroy(evm);
         return kErrDevice;
     }
     if (*(const int*)(h + off_err) != 0) {   // a tensor-core wait ran out
-        if (std::getenv("QSFB_DEBUG"))
+        if (debug_level() >= 1)
             std::fprintf(stderr, "qsfb: tensor-core sweep wait ran out (role %d)\n",
                          *(const int*)(h + off_err));
         cudaEventDestroy(evm);
@@ -776,6 +809,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         ListBuf& L = G.S->lists[std::make_tuple(G.g, G.size, G.reflect)];
         L.ready = true;
         L.queued = false;
+        L.gen_idx = -1;
+        if (G.pm) {
+            L.pm_ready = true;
+            L.pm_queued = false;
+        }
     }
     for (const ExpReq& E : exps) {
         ListBuf& L = E.S->lists[std::make_tuple(E.g, E.size, E.reflect)];

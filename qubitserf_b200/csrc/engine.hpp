@@ -109,6 +109,7 @@ struct ListBuf {
     bool arena = false;   // carved from an Arena (released with it)
     bool queued = false;  // scheduled for generation in the current run_levels call
     bool pm_queued = false;
+    int gen_idx = -1;     // position in the current call's generation list (while queued)
 };
 
 // Bump allocator over device chunks taken from the caching allocator; everything carved

@@ -73,9 +73,12 @@ struct GenDesc {
     const uint32_t* red;      // K x W32
     uint32_t* out;            // count x HP
     uint8_t* pc;              // count (null when full rank)
+    int8_t* pm;               // +-1 rows (count + kPmPadRows), or null when not needed
     unsigned long long entry_base;  // first global entry index of this descriptor
     unsigned long long count;
     int K, size, W32, HP, rank, reflect;
+    int n_enc;                // live +-1 columns (pm only)
+    int pad_;
 };
 
 }  // namespace qsfb

@@ -130,5 +130,36 @@ static __device__ __noinline__ int survivor_scan(const LevelDesc& D, const unsig
     return T;
 }
 
+// 16 probe bits -> 16 int8 columns of a +-1 row: set -> +1, clear -> -1, dead (beyond the
+// live columns, `live` bit clear) -> 0.
+__device__ __forceinline__ uint4 pm_chunk(uint32_t bits, uint32_t live) {
+    uint32_t q[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const uint32_t b = (bits >> (4 * n)) & 0xFu, l = (live >> (4 * n)) & 0xFu;
+        // one byte per column: 0/1 spread of the nibble
+        const uint32_t sb = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
+        const uint32_t sl = (l & 1u) | ((l & 2u) << 7) | ((l & 4u) << 14) | ((l & 8u) << 21);
+        // set -> 0x01, clear -> 0xFF, dead -> 0x00
+        q[n] = (0xFFFFFFFFu - 0xFEu * sb) & (sl * 0xFFu);
+    }
+    return make_uint4(q[0], q[1], q[2], q[3]);
+}
+
+// One +-1 row (kPmRowBytes = 64 columns from the first two probe words), written as four
+// 16-byte chunks at their 64-byte-swizzle positions (chunk c of row e at c ^ ((e >> 1) & 3)).
+__device__ __forceinline__ void write_pm_row(int8_t* out, unsigned long long e, uint32_t w0,
+                                             uint32_t w1, int n_live) {
+    uint4* row = reinterpret_cast<uint4*>(out + e * kPmRowBytes);
+    const int sw = (int)((e >> 1) & 3);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {              // columns [16j, 16j + 16)
+        const uint32_t bits = ((j < 2 ? w0 : w1) >> (16 * (j & 1))) & 0xFFFFu;
+        const int l = n_live - 16 * j;
+        const uint32_t live = l >= 16 ? 0xFFFFu : (l > 0 ? (1u << l) - 1u : 0u);
+        row[j ^ sw] = pm_chunk(bits, live);
+    }
+}
+
 }  // namespace dev
 }  // namespace qsfb

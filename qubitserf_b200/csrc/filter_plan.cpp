@@ -72,16 +72,31 @@ double filter_pass_rate(int filt, int nred, int t) {
     return g_cdf[fi][nb][std::min(t, kMaxT)];
 }
 
+namespace {
+// cdf of Binomial(bits, 1/2) for bits <= 128, filled once (static storage, no heap)
+double g_ham[kBits + 1][kBits + 1];
+std::once_flag g_ham_once;
+void fill_ham() {
+    for (int bits = 0; bits <= kBits; ++bits) {
+        const double lp = -bits * std::log(2.0);
+        double acc = 0.0, lc = 0.0;
+        for (int t = 0; t <= kBits; ++t) {
+            if (t <= bits) {
+                if (t > 0) lc += std::log((double)(bits - t + 1) / t);
+                acc += std::exp(lc + lp);
+            }
+            g_ham[bits][t] = std::min(acc, 1.0);
+        }
+    }
+}
+}  // namespace
+
 double hamming_pass_rate(int bits, int t) {
     if (t < 0) return 0.0;
     if (t >= bits) return 1.0;
-    const double lp = -bits * std::log(2.0);
-    double acc = 0.0, lc = 0.0;
-    for (int i = 0; i <= t; ++i) {
-        if (i > 0) lc += std::log((double)(bits - i + 1) / i);
-        acc += std::exp(lc + lp);
-    }
-    return std::min(acc, 1.0);
+    if (bits > kBits) bits = kBits;   // callers ask for at most four probe words
+    std::call_once(g_ham_once, fill_ham);
+    return g_ham[bits][t];
 }
 
 FilterChoice choose_filter(int HP, int nred, int t, bool zero_test) {

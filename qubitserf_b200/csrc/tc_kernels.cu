@@ -546,20 +546,6 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
 
 // +-1 expansion of packed probe words, one thread per row: the first two probe words (64
 // columns) become 64 int8 values, written as four swizzled 16-byte chunks.
-__device__ __forceinline__ uint4 pm_chunk(uint32_t bits, uint32_t live) {
-    uint32_t q[4];
-#pragma unroll
-    for (int n = 0; n < 4; ++n) {
-        const uint32_t b = (bits >> (4 * n)) & 0xFu, l = (live >> (4 * n)) & 0xFu;
-        // one byte per column: 0/1 spread of the nibble
-        const uint32_t sb = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
-        const uint32_t sl = (l & 1u) | ((l & 2u) << 7) | ((l & 4u) << 14) | ((l & 8u) << 21);
-        // set -> 0x01, clear -> 0xFF, dead -> 0x00
-        q[n] = (0xFFFFFFFFu - 0xFEu * sb) & (sl * 0xFFu);
-    }
-    return make_uint4(q[0], q[1], q[2], q[3]);
-}
-
 __global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __restrict__ descs,
                                                         int ndesc, unsigned long long total) {
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
@@ -577,16 +563,7 @@ __global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __rest
             w0 = __ldg(E.words + e * E.HP);
             if (E.HP > 1) w1 = __ldg(E.words + e * E.HP + 1);
         }
-        const int nl = e < E.count ? E.n_enc : 0;   // live columns of this row
-        uint4* row = reinterpret_cast<uint4*>(E.out + e * kPmRowBytes);
-        const int sw = (int)((e >> 1) & 3);           // 64-byte swizzle
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {                 // columns [16j, 16j + 16)
-            const uint32_t bits = ((j < 2 ? w0 : w1) >> (16 * (j & 1))) & 0xFFFFu;
-            const int l = nl - 16 * j;
-            const uint32_t live = l >= 16 ? 0xFFFFu : (l > 0 ? (1u << l) - 1u : 0u);
-            row[j ^ sw] = pm_chunk(bits, live);
-        }
+        write_pm_row(E.out, e, w0, w1, e < E.count ? E.n_enc : 0);   // padding rows: zeros
     }
 }
 
