@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <unordered_map>
 
 namespace qsfb {
 
@@ -371,7 +372,7 @@ struct Plan {
     unsigned long long pairs;        // C(K, w) of the level (witness rank width)
     unsigned long long range_pairs;  // pairs of this plan's terms
     int p_lo, nterms;
-    std::vector<unsigned long long> term_jobs;
+    int table = -1;                  // term job table (prefix sums, nterms + 1 entries)
     unsigned long long jobs;
 };
 
@@ -391,11 +392,6 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     //    the terms whose rectangles fill the MMA tiles and CUDA-core plans for the rest
     std::vector<Plan> plans;
     unsigned long long cc_pairs = 0;
-    auto range_pairs = [&](int K, int a, int b, int p0, int n) {
-        unsigned long long acc = 0;
-        for (int p = p0; p < p0 + n; ++p) acc += dev->binom(p, a - 1) * dev->binom(K - 1 - p, b);
-        return acc;
-    };
     for (size_t r = 0; r < reqs.size(); ++r) {
         const LevelReq& q = reqs[r];
         SideDev* S = q.side;
@@ -406,6 +402,31 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         int a, b;
         if (pairs <= (1ull << 14)) { a = w; b = 0; }
         else { a = (w + 1) / 2; b = w - a; }
+        // tensor-core term range of this level (the same for every set): terms whose
+        // rectangles keep at least half of every tile busy; nx grows and ny shrinks with p
+        int p1 = -1, p2 = -1;
+        unsigned long long tc_pairs = 0, lo_pairs = 0, hi_pairs = 0;
+        bool range_done = false;
+        auto tc_range = [&]() {
+            range_done = true;
+            const int plo = a - 1, pend = K - b;   // terms p in [plo, pend)
+            int lo = plo, hi = pend;               // first p with nx >= tcM / 2
+            while (lo < hi) {
+                const int mid = (lo + hi) / 2;
+                if (dev->binom(mid, a - 1) >= (unsigned long long)(tcM / 2)) hi = mid; else lo = mid + 1;
+            }
+            int l2 = plo - 1, h2 = pend - 1;       // last p with ny >= tcN / 2
+            while (l2 < h2) {
+                const int mid = (l2 + h2 + 1) / 2;
+                if (dev->binom(K - 1 - mid, b) >= (unsigned long long)(tcN / 2)) l2 = mid; else h2 = mid - 1;
+            }
+            if (lo > l2) return;
+            p1 = lo;
+            p2 = l2;
+            for (int p = plo; p < p1; ++p) lo_pairs += dev->binom(p, a - 1) * dev->binom(K - 1 - p, b);
+            for (int p = p2 + 1; p < pend; ++p) hi_pairs += dev->binom(p, a - 1) * dev->binom(K - 1 - p, b);
+            tc_pairs = pairs - lo_pairs - hi_pairs;
+        };
         for (int g = 0; g < q.active; ++g) {
             Plan P;
             P.req = (int)r; P.g = g; P.a = a; P.b = b;
@@ -434,18 +455,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 std::fprintf(stderr, "qsfb plan: K=%d w=%d a=%d b=%d nred=%d rank=%d HP=%d T=%d "
                              "mode=%d filt=%d ks=%d\n", K, w, a, b, nred, rank, P.HP, T, P.mode,
                              P.filt, ks);
-            int p1 = -1, p2 = -1;
-            if (ks > 0) {
-                // terms whose rectangles keep at least half of every tile busy
-                for (int p = P.p_lo; p < P.p_lo + P.nterms; ++p) {
-                    if (dev->binom(p, a - 1) >= (unsigned long long)(tcM / 2) &&
-                        dev->binom(K - 1 - p, b) >= (unsigned long long)(tcN / 2)) {
-                        if (p1 < 0) p1 = p;
-                        p2 = p;
-                    }
-                }
-            }
-            if (p1 < 0) {
+            if (ks > 0 && !range_done) tc_range();
+            if (ks == 0 || p1 < 0) {
                 P.range_pairs = pairs;
                 cc_pairs += pairs;
                 plans.push_back(std::move(P));
@@ -458,20 +469,20 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             TP.n_live = nl;
             TP.p_lo = p1;
             TP.nterms = p2 - p1 + 1;
-            TP.range_pairs = range_pairs(K, a, b, p1, TP.nterms);
+            TP.range_pairs = tc_pairs;
             if (p1 > P.p_lo) {
                 Plan L = P;
                 L.nterms = p1 - P.p_lo;
-                L.range_pairs = range_pairs(K, a, b, L.p_lo, L.nterms);
-                cc_pairs += L.range_pairs;
+                L.range_pairs = lo_pairs;
+                cc_pairs += lo_pairs;
                 plans.push_back(std::move(L));
             }
             if (p2 + 1 < p_end) {
                 Plan R = P;
                 R.p_lo = p2 + 1;
                 R.nterms = p_end - R.p_lo;
-                R.range_pairs = range_pairs(K, a, b, R.p_lo, R.nterms);
-                cc_pairs += R.range_pairs;
+                R.range_pairs = hi_pairs;
+                cc_pairs += hi_pairs;
                 plans.push_back(std::move(R));
             }
             plans.push_back(std::move(TP));
@@ -484,6 +495,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     lt = std::max<unsigned long long>(32, std::min<unsigned long long>(1024, lt));
     const int loop_tile = (int)((lt + 31) / 32 * 32);
 
+    const auto tp1 = std::chrono::steady_clock::now();
     // 2) lists to build: packed probe words for every plan, +-1 rows for tensor plans
     // A list generated in this call writes its +-1 rows in the same pass when a tensor plan
     // needs them; a list generated earlier gets them from the expansion kernel.
@@ -555,31 +567,46 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         }
     }
 
-    // 3) term tables and job counts
+    const auto tp2 = std::chrono::steady_clock::now();
+    // 3) term tables and job counts, shared by every plan with the same level shape (K, a,
+    //    b), sweep and term range: sets of a level and levels of equal shape across codes
+    //    differ only in their lists
     unsigned long long tc_jobs = 0;
+    std::vector<std::vector<unsigned long long>> tables;
+    std::unordered_map<unsigned long long, int> table_of;   // packed (K, a, b, tc, p_lo, nterms)
     for (Plan& P : plans) {
-        const int K = reqs[P.req].side->K;
-        P.term_jobs.assign(P.nterms + 1, 0ull);
-        unsigned long long acc = 0;
-        for (int t = 0; t < P.nterms; ++t) {
-            const int p = P.p_lo + t;
-            const unsigned long long nx = dev->binom(p, P.a - 1);
-            const unsigned long long ny = dev->binom(K - 1 - p, P.b);
-            P.term_jobs[t] = acc;
-            if (P.tc) {
-                // prefix tiles from the 8-aligned start of the block x suffix-tile chunks
-                const unsigned long long xoff = dev->binom(p, P.a);
-                const unsigned long long na = ((xoff & 7ull) + nx + tcM - 1) / tcM;
-                const unsigned long long nbt = (ny + tcN - 1) / tcN;
-                acc += na * ((nbt + tcJB - 1) / tcJB);
-            } else {
-                const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
-                acc += ((rn + kRegTile - 1) / kRegTile) * ((ln + loop_tile - 1) / loop_tile);
+        const unsigned long long tkey =
+            ((unsigned long long)reqs[P.req].side->K << 42) | ((unsigned long long)P.a << 35) |
+            ((unsigned long long)P.b << 28) | ((unsigned long long)(P.tc ? 1 : 0) << 27) |
+            ((unsigned long long)P.p_lo << 14) | (unsigned long long)P.nterms;
+        auto it = table_of.find(tkey);
+        if (it == table_of.end()) {
+            const int K = reqs[P.req].side->K;
+            std::vector<unsigned long long> tj(P.nterms + 1, 0ull);
+            unsigned long long acc = 0;
+            for (int t = 0; t < P.nterms; ++t) {
+                const int p = P.p_lo + t;
+                const unsigned long long nx = dev->binom(p, P.a - 1);
+                const unsigned long long ny = dev->binom(K - 1 - p, P.b);
+                tj[t] = acc;
+                if (P.tc) {
+                    // prefix tiles from the 8-aligned start of the block x suffix-tile chunks
+                    const unsigned long long xoff = dev->binom(p, P.a);
+                    const unsigned long long na = ((xoff & 7ull) + nx + tcM - 1) / tcM;
+                    const unsigned long long nbt = (ny + tcN - 1) / tcN;
+                    acc += na * ((nbt + tcJB - 1) / tcJB);
+                } else {
+                    const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
+                    acc += ((rn + kRegTile - 1) / kRegTile) * ((ln + loop_tile - 1) / loop_tile);
+                }
             }
+            tj[P.nterms] = acc;
+            it = table_of.emplace(tkey, (int)tables.size()).first;
+            tables.push_back(std::move(tj));
         }
-        P.term_jobs[P.nterms] = acc;
-        P.jobs = acc;
-        if (P.tc) tc_jobs += acc;
+        P.table = it->second;
+        P.jobs = tables[P.table].back();
+        if (P.tc) tc_jobs += P.jobs;
     }
     if (tc_jobs && debug_level() == 3) {
         unsigned long long tiles = 0, pairs = 0, atiles = 0;
@@ -609,6 +636,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                std::make_tuple(plans[y].tc, plans[y].filt, plans[y].HP, plans[y].mode);
     });
 
+    const auto tp3 = std::chrono::steady_clock::now();
     // 4) staging layout
     const size_t nplans = plans.size();
     size_t off = 0;
@@ -620,7 +648,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     off = align_up(off + nplans * sizeof(LevelDesc), 64);
     const size_t off_terms = off;
     size_t terms_total = 0;
-    for (const Plan& P : plans) terms_total += P.term_jobs.size();
+    for (const auto& tj : tables) terms_total += tj.size();
     off = align_up(off + terms_total * 8, 64);
     const size_t off_keys = off;
     off = align_up(off + reqs.size() * 8, 64);
@@ -680,7 +708,15 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
 
     LevelDesc* hl = (LevelDesc*)(h + off_lvl);
     unsigned long long* hterms = (unsigned long long*)(h + off_terms);
-    size_t term_cursor = 0;
+    std::vector<size_t> table_off(tables.size());
+    {
+        size_t cur = 0;
+        for (size_t i = 0; i < tables.size(); ++i) {
+            std::memcpy(hterms + cur, tables[i].data(), tables[i].size() * 8);
+            table_off[i] = cur;
+            cur += tables[i].size();
+        }
+    }
     struct Group { bool tc; int filt, HP, mode, first, count; unsigned long long jobs; };
     std::vector<Group> groups;
     for (size_t oi = 0; oi < order.size(); ++oi) {
@@ -700,9 +736,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.pca = La.pc;
         D.rb = Rb.words;
         D.pcb = Rb.pc;
-        std::memcpy(hterms + term_cursor, P.term_jobs.data(), P.term_jobs.size() * 8);
-        D.term_jobs = (const uint64_t*)(d + off_terms + term_cursor * 8);
-        term_cursor += P.term_jobs.size();
+        D.term_jobs = (const uint64_t*)(d + off_terms + table_off[P.table] * 8);
         D.key = (unsigned long long*)(d + off_keys + (size_t)P.req * 8);
         D.count = (unsigned long long*)(d + off_counts + (size_t)order[oi] * 8);
         D.job_base = Gp.jobs;
@@ -729,6 +763,15 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     if (groups.size() > 64) return kErrUnsupported;
 
     // 5) launch
+    if (debug_level() == 4) {
+        const auto tp4 = std::chrono::steady_clock::now();
+        auto us = [](std::chrono::steady_clock::time_point x, std::chrono::steady_clock::time_point y) {
+            return std::chrono::duration<double, std::micro>(y - x).count();
+        };
+        std::fprintf(stderr, "qsfb plan: reqs=%zu plans=%zu gens=%zu exps=%zu tables=%zu | plan %.0f us, lists %.0f us, "
+                     "terms %.0f us, staging %.0f us\n", reqs.size(), plans.size(), gens.size(),
+                     exps.size(), tables.size(), us(tp0, tp1), us(tp1, tp2), us(tp2, tp3), us(tp3, tp4));
+    }
     if (stats)
         stats->host_plan_s +=
             std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
