@@ -186,6 +186,7 @@ typedef struct {
     double host_plan_seconds;    /* host planning of the rounds (before their launches) */
     double host_apply_seconds;   /* host schedule updates after the rounds */
     unsigned long long tc_codewords;    /* codewords swept by the tensor-core kernel */
+    double tc_ms;                /* tensor-core sweep launches alone (CUDA events) */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free. */
@@ -259,7 +260,9 @@ int qsfb_microbench(int which, double* ops_per_s);
  * D = A * B^T over the first 32 * ksteps columns, with A 256 x 64 and B 128 x 64 int8
  * (row-major; the sweep stores +1 / -1 / 0) and D 256 x 128 int32 (row-major), computed
  * by the sweep's own copy, tcgen05 MMA and TMEM read-back path.  ksteps in 1..2.
- * Returns 0, 1 (null), 2 (ksteps), 4 (device) or 6 (memory). */
+ * ksteps = -1 runs the timeout drill: the operands are never copied, the kernel's bounded
+ * waits run out after 50 ms and the call returns 4 with the device still usable.
+ * Returns 0, 1 (null), 2 (ksteps), 4 (device or a wait that ran out) or 6 (memory). */
 int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D);
 
 /* Overwrite a 256 MiB device buffer (more than the 126 MB L2) and wait; benchmarks call it

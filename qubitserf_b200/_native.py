@@ -472,7 +472,8 @@ def microbench(which):
 
 def tc_selftest(ksteps, A, B):
     """D = A[:, :32k] @ B[:, :32k].T (int32, 256 x 128) through the tensor-core sweep's own
-    copy / MMA / TMEM path; A is 256 x 64 and B 128 x 64 int8."""
+    copy / MMA / TMEM path; A is 256 x 64 and B 128 x 64 int8.  ksteps = -1 is the
+    timeout drill (raises RuntimeError with rc 4)."""
     A = np.ascontiguousarray(A, dtype=np.int8)
     B = np.ascontiguousarray(B, dtype=np.int8)
     if A.shape != (256, 64) or B.shape != (128, 64):

@@ -642,7 +642,7 @@ int qsfb_microbench(int which, double* ops_per_s) {
 
 int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D) {
     if (!A || !B || !D) return kErrNull;
-    if (ksteps < 1 || ksteps > kPmRowBytes / 32) return kErrShape;
+    if (ksteps == 0 || ksteps < -1 || ksteps > kPmRowBytes / 32) return kErrShape;
     int rc = kOk;
     Device* dev = device_or(&rc);
     if (!dev) return rc;

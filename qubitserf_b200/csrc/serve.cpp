@@ -74,6 +74,10 @@ size_t list_footprint(Device* dev, const BzSide& S) {
                 seen.push_back(sz);
                 const unsigned long long c = dev->binom(S.K, sz.first);
                 bytes += (size_t)c * HP * 4 + (full ? 0 : (size_t)c) + 512;
+                // +-1 rows of the tensor-core sweep (full-rank sets with two or more
+                // probe words; counted whether or not the planner ends up using them)
+                if (full && HP >= 2 && sz.first > 0)
+                    bytes += (size_t)(c + kPmPadRows) * kPmRowBytes;
             }
         }
     }

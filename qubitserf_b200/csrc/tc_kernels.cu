@@ -92,17 +92,19 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Wait for the phase of `bar` with the given parity; false after ~2 s (error path).  The
-// timer is only consulted after a few thousand probes: normal waits are far shorter, and
-// a %globaltimer read on every wait would sit on the critical path.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Wait for the phase of `bar` with the given parity; false after `limit_ns` (error path,
+// ~2 s by default).  The timer is only consulted after a few thousand probes: normal
+// waits are far shorter, and a %globaltimer read on every wait would sit on the critical
+// path.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          unsigned long long limit_ns = kTcWaitNs) {
     for (int i = 0; i < 4096; ++i)
         if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (;;) {
         for (int i = 0; i < 1024; ++i)
             if (mbar_try(bar, parity)) return true;
-        if (global_ns() - t0 > kTcWaitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -569,7 +571,9 @@ __global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __rest
 
 // Self-test of the operand layout: D = A (256 x 64) * B (128 x 64)^T through the same
 // copy / MMA / TMEM path (both halves), written out as 256 x 128 s32.  A and B are rows
-// in the pre-swizzled layout.
+// in the pre-swizzled layout.  ksteps < 0 is the timeout drill: no copy is issued, so the
+// operand and accumulator waits run out after 50 ms and the error word is set, as a
+// broken pipeline would; the launch still ends normally and frees its TMEM.
 __global__ void __launch_bounds__(kTcThreads, 1)
 tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, int ksteps,
                    int32_t* __restrict__ out, int* __restrict__ err) {
@@ -582,13 +586,15 @@ tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, 
     const uint32_t tmem = tc_setup(bar, 2, counts, tmem_slot);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     bool ok = true;
-    if (warp == 0 && lane == 0) {
+    const bool drill = ksteps < 0;
+    const unsigned long long limit = drill ? 50000000ull : kTcWaitNs;
+    if (warp == 0 && lane == 0 && !drill) {
         mbar_expect_tx(bar, kTcABytes + kTcBBytes);
         bulk_g2s(s0 + kTcOffA, A, kTcABytes, bar);
         bulk_g2s(s0 + kTcOffB, Bm, kTcBBytes, bar);
     }
     if (warp == 1 && lane == 0) {
-        ok = mbar_wait(bar, 0);
+        ok = mbar_wait(bar, 0, limit);
         if (ok) {
             tc_fence_after();
             for (int h = 0; h < kTcHalves; ++h)
@@ -602,7 +608,7 @@ tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, 
     }
     if (warp >= 2 && warp < 10) {   // one warp per (half, lane quarter)
         const int quarter = warp & 3, half = (warp - 2) >> 2;
-        ok = mbar_wait(bar + 8, 0);
+        ok = mbar_wait(bar + 8, 0, limit);
         ok = __all_sync(0xffffffffu, ok);
         if (ok) {
             tc_fence_after();

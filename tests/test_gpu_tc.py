@@ -69,3 +69,14 @@ def test_tensor_sweep_equals_cuda_core_sweep():
     assert on["ans"] == off["ans"]
     # every level still evaluates every codeword exactly once
     assert on["codewords"] == off["codewords"]
+
+
+def test_bounded_wait_reports_and_device_survives(native):
+    # the drill copies nothing, so the kernel's operand and accumulator waits run out; the
+    # call reports rc 4 and the next launch on the same context is exact again
+    A = np.ones((256, 64), dtype=np.int8)
+    B = np.ones((128, 64), dtype=np.int8)
+    with pytest.raises(RuntimeError, match="rc=4"):
+        native.tc_selftest(-1, A, B)
+    D = native.tc_selftest(2, A, B)
+    assert np.array_equal(D, np.full((256, 128), 64, dtype=np.int32))
