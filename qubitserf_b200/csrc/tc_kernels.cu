@@ -341,19 +341,20 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t s0 = smem_u32(smem);
     const uint32_t bar = s0 + kTcOffBar;
-    // barrier slots (8 bytes each): a_full 0-1, a_empty 2-3, b_full 4-11, b_empty 12-19,
-    // acc_full 20-21, acc_empty 22-23
+    // barrier slots (8 bytes each): a_full 0-1, a_empty 2-3, b_full 4-11, tile_done 12-19,
+    // acc_empty 20-21.  One MMA commit per suffix tile signals both that its stage may be
+    // refilled and that its accumulator is ready: the copier and the read-back warps wait
+    // on the same tile_done barrier (tile i: stage i % kTcBStages, accumulator i & 1).
     auto a_full = [&](uint32_t i) { return bar + 8u * i; };
     auto a_empty = [&](uint32_t i) { return bar + 8u * (2 + i); };
     auto b_full = [&](uint32_t i) { return bar + 8u * (4 + i); };
-    auto b_empty = [&](uint32_t i) { return bar + 8u * (4 + kTcBStages + i); };
-    auto acc_full = [&](uint32_t i) { return bar + 8u * (4 + 2 * kTcBStages + i); };
-    auto acc_empty = [&](uint32_t i) { return bar + 8u * (6 + 2 * kTcBStages + i); };
-    constexpr int kNBar = 8 + 2 * kTcBStages;
+    auto tile_done = [&](uint32_t i) { return bar + 8u * (4 + kTcBStages + i); };
+    auto acc_empty = [&](uint32_t i) { return bar + 8u * (4 + 2 * kTcBStages + i); };
+    constexpr int kNBar = 6 + 2 * kTcBStages;
     uint32_t counts[kNBar];
     for (int i = 0; i < kNBar; ++i) counts[i] = 1;
     counts[2] = counts[3] = 2;   // a prefix slot is released by both MMA threads
-    counts[6 + 2 * kTcBStages] = counts[7 + 2 * kTcBStages] = kTcEpiWarps;   // one per warp
+    counts[4 + 2 * kTcBStages] = counts[5 + 2 * kTcBStages] = kTcEpiWarps;   // one per warp
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 256);
     const uint32_t tmem = tc_setup(bar, kNBar, counts, tmem_slot);
 
@@ -387,7 +388,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 for (unsigned long long bt = R.b0; bt < R.b1; ++bt, ++it_b) {
                     if ((it_b & 1u) != par) continue;
                     const uint32_t sb = it_b % kTcBStages;
-                    if (!(ok = mbar_wait(b_empty(sb), ((it_b / kTcBStages) & 1u) ^ 1u))) break;
+                    if (!(ok = mbar_wait(tile_done(sb), ((it_b / kTcBStages) & 1u) ^ 1u))) break;
                     mbar_expect_tx(b_full(sb), kTcBBytes);
                     bulk_g2s(s0 + kTcOffB + sb * kTcBBytes, ypm + bt * kTcN * kPmRowBytes,
                              kTcBBytes, b_full(sb));
@@ -426,8 +427,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                             mma_i8(tmem + (ac * kTcHalves + h) * kTcN,
                                    smem_desc(a_addr + h * kTcHalfBytes + 32u * k),
                                    smem_desc(b_addr + 32u * k), k > 0 ? 1u : 0u);
-                    mma_commit(b_empty(sb));
-                    mma_commit(acc_full(ac));
+                    mma_commit(tile_done(sb));
                 }
                 if (!ok) break;
                 mma_commit(a_empty(sa));
@@ -463,7 +463,8 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             for (unsigned long long bt = b0; bt < b1; ++bt) {
                 const uint32_t ac = it_c & 1u;
                 // one lane polls the barrier, the warp follows (256 pollers would contend)
-                if (lane == 0) ok = mbar_wait(acc_full(ac), (it_c >> 1) & 1u);
+                if (lane == 0)
+                    ok = mbar_wait(tile_done(it_c % kTcBStages), (it_c / kTcBStages) & 1u);
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 if (!ok) break;
                 tc_fence_after();
