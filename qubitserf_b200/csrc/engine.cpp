@@ -499,8 +499,18 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     // 2) lists to build: packed probe words for every plan, +-1 rows for tensor plans
     // A list generated in this call writes its +-1 rows in the same pass when a tensor plan
     // needs them; a list generated earlier gets them from the expansion kernel.
-    struct GenReq { SideDev* S; int g, size, reflect, HP; bool pm; int n_enc; };
-    struct ExpReq { SideDev* S; int g, size, reflect, HP, n_enc; };
+    struct GenReq {
+        SideDev* S;
+        int g, size, reflect, HP;
+        bool pm;
+        int n_enc;
+        unsigned long long pm_lo, pm_hi;
+    };
+    struct ExpReq {
+        SideDev* S;
+        int g, size, reflect, HP, n_enc;
+        unsigned long long lo, hi;
+    };
     std::vector<GenReq> gens;
     std::vector<ExpReq> exps;
     std::vector<std::pair<int8_t*, size_t>> pad_zero;   // new +-1 buffers: zero their tail rows
@@ -514,8 +524,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 L.queued = L.pm_queued = false;
                 L.gen_idx = -1;
             }
-            for (const ExpReq& E : e)
-                E.S->lists[std::make_tuple(E.g, E.size, E.reflect)].pm_queued = false;
+            for (const ExpReq& E : e) {
+                ListBuf& L = E.S->lists[std::make_tuple(E.g, E.size, E.reflect)];
+                L.pm_queued = false;
+                L.exp_idx = -1;
+            }
         }
     } clear_queued{gens, exps};
     for (const Plan& P : plans) {
@@ -528,7 +541,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 if (L.words) {   // allocated by an earlier execution: regenerate in place
                     L.queued = true;
                     L.gen_idx = (int)gens.size();
-                    gens.push_back({S, P.g, size, side, P.HP, false, 0});
+                    gens.push_back({S, P.g, size, side, P.HP, false, 0, 0, 0});
                 } else {
                     L.queued = true;
                     L.count = dev->binom(S->K, size);
@@ -543,10 +556,22 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                     }
                     S->list_bytes += L.bytes_w + L.bytes_pc;
                     L.gen_idx = (int)gens.size();
-                    gens.push_back({S, P.g, size, side, P.HP, false, 0});
+                    gens.push_back({S, P.g, size, side, P.HP, false, 0, 0, 0});
                 }
             }
-            if (!P.tc || L.pm_ready || L.pm_queued) continue;
+            if (!P.tc) continue;
+            // +-1 rows this tensor plan reads: the prefix blocks of its terms, and the
+            // suffix prefix of its first term plus one tile (columns past a term's end
+            // must hold real entries or zeros, not stale memory)
+            unsigned long long n_lo, n_hi;
+            if (side == 0) {
+                n_lo = dev->binom(P.p_lo, P.a);
+                n_hi = dev->binom(P.p_lo + P.nterms, P.a);
+            } else {
+                n_lo = 0;
+                n_hi = std::min(L.count, dev->binom(S->K - 1 - P.p_lo, P.b) + (unsigned long long)tcN);
+            }
+            if (L.pm_ready && n_lo >= L.pm_lo && n_hi <= L.pm_hi) continue;   // already written
             if (!L.pm) {
                 L.bytes_pm = (size_t)(L.count + kPmPadRows) * kPmRowBytes;
                 L.pm = (int8_t*)(L.arena ? S->arena->alloc(L.bytes_pm) : dev->alloc(L.bytes_pm));
@@ -555,14 +580,34 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 pad_zero.push_back({L.pm + (size_t)L.count * kPmRowBytes,
                                     (size_t)kPmPadRows * kPmRowBytes});
             }
-            L.pm_queued = true;
             const int nred = (int)S->nonpivot[P.g].size();
             const int n_enc = std::min(nred, kPmRowBytes);
-            if (L.queued && L.gen_idx >= 0) {   // generated in this call: fused
-                gens[L.gen_idx].pm = true;
-                gens[L.gen_idx].n_enc = n_enc;
-            } else {
-                exps.push_back({S, P.g, size, side, P.HP, n_enc});
+            if (L.queued && L.gen_idx >= 0) {   // generated in this call: fused, hull of needs
+                GenReq& G = gens[L.gen_idx];
+                if (!G.pm) {
+                    G.pm = true;
+                    G.n_enc = n_enc;
+                    G.pm_lo = n_lo;
+                    G.pm_hi = n_hi;
+                } else {
+                    G.pm_lo = std::min(G.pm_lo, n_lo);
+                    G.pm_hi = std::max(G.pm_hi, n_hi);
+                }
+                L.pm_queued = true;
+            } else {   // built earlier: expand the hull of what is written and what is needed
+                if (L.pm_ready) {
+                    n_lo = std::min(n_lo, L.pm_lo);
+                    n_hi = std::max(n_hi, L.pm_hi);
+                }
+                if (L.pm_queued && L.exp_idx >= 0) {
+                    ExpReq& E = exps[L.exp_idx];
+                    E.lo = std::min(E.lo, n_lo);
+                    E.hi = std::max(E.hi, n_hi);
+                } else {
+                    L.exp_idx = (int)exps.size();
+                    exps.push_back({S, P.g, size, side, P.HP, n_enc, n_lo, n_hi});
+                    L.pm_queued = true;
+                }
             }
         }
     }
@@ -676,6 +721,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.pc = L.pc;
         D.pm = G.pm ? L.pm : nullptr;
         D.n_enc = G.n_enc;
+        D.pm_lo = G.pm_lo;
+        D.pm_hi = G.pm_hi;
         D.entry_base = gen_total;
         D.count = L.count;
         D.K = G.S->K;
@@ -696,7 +743,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.out = L.pm;
         D.row_base = exp_total;
         D.count = L.count;
-        D.rows = L.count + kPmPadRows;
+        D.row_lo = E.lo;
+        D.rows = E.hi - E.lo;
         D.HP = E.HP;
         D.n_enc = E.n_enc;
         exp_total += D.rows;
@@ -856,12 +904,17 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         if (G.pm) {
             L.pm_ready = true;
             L.pm_queued = false;
+            L.pm_lo = G.pm_lo;
+            L.pm_hi = G.pm_hi;
         }
     }
     for (const ExpReq& E : exps) {
         ListBuf& L = E.S->lists[std::make_tuple(E.g, E.size, E.reflect)];
         L.pm_ready = true;
         L.pm_queued = false;
+        L.exp_idx = -1;
+        L.pm_lo = E.lo;
+        L.pm_hi = E.hi;
     }
 
     // 6) decode

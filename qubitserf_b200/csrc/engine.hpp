@@ -109,7 +109,9 @@ struct ListBuf {
     bool arena = false;   // carved from an Arena (released with it)
     bool queued = false;  // scheduled for generation in the current run_levels call
     bool pm_queued = false;
+    unsigned long long pm_lo = 0, pm_hi = 0;   // rows of `pm` written (when pm_ready)
     int gen_idx = -1;     // position in the current call's generation list (while queued)
+    int exp_idx = -1;     // position in the current call's expansion list (while pm_queued)
 };
 
 // Bump allocator over device chunks taken from the caching allocator; everything carved

@@ -57,13 +57,13 @@ struct LevelDesc {
 constexpr int kPmRowBytes = 64;    // +-1 row: 64 int8 columns (the first two probe words)
 constexpr int kPmPadRows = 256;    // zero rows after every +-1 list (whole-tile copies)
 
-// One +-1 expansion: rows [0, rows) of `out` from the packed probe words of a list
-// (rows beyond `count` are written as zeros).
+// One +-1 expansion: rows [row_lo, row_lo + rows) of `out` from the packed probe words of
+// a list (rows at or beyond `count` are written as zeros).
 struct ExpandDesc {
     const uint32_t* words;    // count x HP
-    int8_t* out;              // rows x kPmRowBytes
+    int8_t* out;              // (count + kPmPadRows) x kPmRowBytes
     unsigned long long row_base;  // first global row of this descriptor
-    unsigned long long count, rows;
+    unsigned long long count, row_lo, rows;
     int HP, n_enc;            // live columns = min(non-pivot bits, 64)
 };
 
@@ -76,6 +76,7 @@ struct GenDesc {
     int8_t* pm;               // +-1 rows (count + kPmPadRows), or null when not needed
     unsigned long long entry_base;  // first global entry index of this descriptor
     unsigned long long count;
+    unsigned long long pm_lo, pm_hi;  // entries whose +-1 rows are written (pm only)
     int K, size, W32, HP, rank, reflect;
     int n_enc;                // live +-1 columns (pm only)
     int pad_;

@@ -62,7 +62,8 @@ __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restric
             o[0] = acc[0];
         }
         if (D.pc) D.pc[e] = (uint8_t)pc;
-        if (D.pm) write_pm_row(D.pm, e, acc[0], acc[1], D.n_enc);   // +-1 form, same pass
+        if (D.pm && e >= D.pm_lo && e < D.pm_hi)   // +-1 form of the rows a tensor plan reads
+            write_pm_row(D.pm, e, acc[0], acc[1], D.n_enc);
     }
 }
 

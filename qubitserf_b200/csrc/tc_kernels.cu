@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __rest
             if (descs[mid].row_base <= ge) lo = mid; else hi = mid - 1;
         }
         const ExpandDesc& E = descs[lo];
-        const unsigned long long e = ge - E.row_base;
+        const unsigned long long e = E.row_lo + (ge - E.row_base);
         uint32_t w0 = 0u, w1 = 0u;
         if (e < E.count) {
             w0 = __ldg(E.words + e * E.HP);
