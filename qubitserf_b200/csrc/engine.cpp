@@ -723,7 +723,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.n_enc = G.n_enc;
         D.pm_lo = G.pm_lo;
         D.pm_hi = G.pm_hi;
-        D.entry_base = gen_total;
+        D.entry_base = gen_total;   // in runs of kGenRun entries
         D.count = L.count;
         D.K = G.S->K;
         D.size = G.size;
@@ -731,7 +731,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.HP = G.HP;
         D.rank = G.S->ranks[G.g];
         D.reflect = G.reflect;
-        gen_total += L.count;
+        gen_total += (L.count + kGenRun - 1) / kGenRun;
     }
     ExpandDesc* he = (ExpandDesc*)(h + off_exp);
     unsigned long long exp_total = 0;

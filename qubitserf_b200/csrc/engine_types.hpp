@@ -54,6 +54,7 @@ struct LevelDesc {
     int pad_;
 };
 
+constexpr int kGenRun = 8;         // consecutive list entries generated by one thread
 constexpr int kPmRowBytes = 64;    // +-1 row: 64 int8 columns (the first two probe words)
 constexpr int kPmPadRows = 256;    // zero rows after every +-1 list (whole-tile copies)
 
@@ -74,7 +75,7 @@ struct GenDesc {
     uint32_t* out;            // count x HP
     uint8_t* pc;              // count (null when full rank)
     int8_t* pm;               // +-1 rows (count + kPmPadRows), or null when not needed
-    unsigned long long entry_base;  // first global entry index of this descriptor
+    unsigned long long entry_base;  // first global run (kGenRun entries) of this descriptor
     unsigned long long count;
     unsigned long long pm_lo, pm_hi;  // entries whose +-1 rows are written (pm only)
     int K, size, W32, HP, rank, reflect;

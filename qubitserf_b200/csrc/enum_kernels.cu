@@ -29,41 +29,71 @@ constexpr int RX = 8;           // register-side entries per lane
 constexpr int kChunk = 32;      // loop entries between survivor checks
 
 // ---------------------------------------------------------------- list generation
+// One thread per run of kGenRun consecutive entries of a list: the first entry is unranked
+// (binary searches over the binomial table), the next ones follow by the colex successor
+// (raise the lowest element that can move, reset the ones below it), so the XOR of the
+// rows changes by the few rows that leave and enter -- usually one of each.
+__device__ __forceinline__ void xor_row(const GenDesc& D, int row, uint32_t (&acc)[4]) {
+    const uint32_t* r = D.red + (size_t)row * D.W32;
+#pragma unroll
+    for (int h = 0; h < 4; ++h)
+        if (h < D.HP && h < D.W32) acc[h] ^= __ldg(r + h);
+}
+
 __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restrict__ descs,
                                                         int ndesc, unsigned long long total,
                                                         const unsigned long long* __restrict__ B) {
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long ge = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-         ge < total; ge += stride) {
+    for (unsigned long long gr = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         gr < total; gr += stride) {
         int lo = 0, hi = ndesc - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (descs[mid].entry_base <= ge) lo = mid; else hi = mid - 1;
+            if (descs[mid].entry_base <= gr) lo = mid; else hi = mid - 1;
         }
         const GenDesc& D = descs[lo];
-        const unsigned long long e = ge - D.entry_base;
-        int rows[kMaxW];
-        list_rows(B, e, D.size, D.K, D.reflect, rows);
+        const unsigned long long e0 = (gr - D.entry_base) * kGenRun;
+        const int n = (int)(D.count - e0 < (unsigned long long)kGenRun ? D.count - e0 : kGenRun);
+        const int s = D.size;
+        // colex combination, ascending: c[0] < c[1] < ... < c[s-1]
+        int c[kMaxW], top[kMaxW];
+        colex_unrank(B, e0, s, D.K, top);          // largest first
+        for (int i = 0; i < s; ++i) c[i] = top[s - 1 - i];
+        auto row_of = [&](int v) { return D.reflect ? D.K - 1 - v : v; };
         uint32_t acc[4] = {0u, 0u, 0u, 0u};
         int pc = 0;
-        for (int i = 0; i < D.size; ++i) {
-            const uint32_t* r = D.red + (size_t)rows[i] * D.W32;
-#pragma unroll
-            for (int h = 0; h < 4; ++h)
-                if (h < D.HP && h < D.W32) acc[h] ^= __ldg(r + h);
-            pc += rows[i] < D.rank;
+        for (int i = 0; i < s; ++i) {
+            const int r = row_of(c[i]);
+            xor_row(D, r, acc);
+            pc += r < D.rank;
         }
-        uint32_t* o = D.out + e * (unsigned long long)D.HP;
-        if (D.HP == 4) {
-            *reinterpret_cast<uint4*>(o) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
-        } else if (D.HP == 2) {
-            *reinterpret_cast<uint2*>(o) = make_uint2(acc[0], acc[1]);
-        } else {
-            o[0] = acc[0];
+        for (int j = 0; j < n; ++j) {
+            const unsigned long long e = e0 + j;
+            uint32_t* o = D.out + e * (unsigned long long)D.HP;
+            if (D.HP == 4) {
+                *reinterpret_cast<uint4*>(o) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+            } else if (D.HP == 2) {
+                *reinterpret_cast<uint2*>(o) = make_uint2(acc[0], acc[1]);
+            } else {
+                o[0] = acc[0];
+            }
+            if (D.pc) D.pc[e] = (uint8_t)pc;
+            if (D.pm && e >= D.pm_lo && e < D.pm_hi)   // +-1 form of the rows a tensor plan reads
+                write_pm_row(D.pm, e, acc[0], acc[1], D.n_enc);
+            if (j + 1 == n) break;
+            // colex successor: lowest t with c[t] + 1 < c[t+1] (c[s] = K)
+            int t = 0;
+            while (t < s - 1 && c[t] + 1 == c[t + 1]) ++t;
+            for (int i = 0; i <= t; ++i) {
+                const int r_old = row_of(c[i]);
+                xor_row(D, r_old, acc);
+                pc -= r_old < D.rank;
+                c[i] = i < t ? i : c[i] + 1;
+                const int r_new = row_of(c[i]);
+                xor_row(D, r_new, acc);
+                pc += r_new < D.rank;
+            }
         }
-        if (D.pc) D.pc[e] = (uint8_t)pc;
-        if (D.pm && e >= D.pm_lo && e < D.pm_hi)   // +-1 form of the rows a tensor plan reads
-            write_pm_row(D.pm, e, acc[0], acc[1], D.n_enc);
     }
 }
 
@@ -299,7 +329,7 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
 // ---------------------------------------------------------------- host launchers
 cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
                              const unsigned long long* d_binom, int num_sms, cudaStream_t st) {
-    if (total == 0) return cudaSuccess;
+    if (total == 0) return cudaSuccess;   // total: runs of kGenRun entries
     unsigned long long blocks = (total + 255) / 256;
     const unsigned long long cap = (unsigned long long)num_sms * 16;
     if (blocks > cap) blocks = cap;

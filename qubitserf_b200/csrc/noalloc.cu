@@ -230,7 +230,7 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
             G.red = red;
             G.out = side == 0 ? la : rb;
             G.pc = side == 0 ? pca : pcb;
-            G.entry_base = gen_total;
+            G.entry_base = gen_total;   // in runs of kGenRun entries
             G.count = side == 0 ? na : nb;
             G.K = K;
             G.size = side == 0 ? a : b;
@@ -238,7 +238,7 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
             G.HP = HP;
             G.rank = 0;          // raw rows: no pivot structure
             G.reflect = side;
-            gen_total += G.count;
+            gen_total += (G.count + kGenRun - 1) / kGenRun;
         }
         unsigned long long acc = 0;
         for (int t = 0; t < nterms; ++t) {
