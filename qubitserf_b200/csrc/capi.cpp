@@ -613,15 +613,74 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
 
 void qsfb_batch_free(QsfbBatchHandle* H) { delete H; }
 
+// One-shot batch.  A large batch is cut into chunks and pipelined: while the rounds of
+// chunk k run on the device (this thread), a helper thread prepares chunk k + 1 (host
+// reduction on all cores, seed eliminations and upload on its own stream).  The first
+// chunk is small so the device starts early.  Codes are independent, so the answers are
+// those of one batch; at most two chunks hold device memory at a time.
 int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
                QsfbBatchStats* stats) {
     const double t0 = now_seconds();
-    QsfbBatchHandle* H = nullptr;
-    int rc = qsfb_batch_prepare(queries, nq, host_threads, &H);
-    if (rc != kOk) return rc;
-    rc = qsfb_batch_execute(H, out, stats);
-    qsfb_batch_free(H);
-    if (stats) stats->seconds = now_seconds() - t0;
+    constexpr int kPipeMin = 256;   // below this the batch runs in one piece
+    std::vector<int> cut{0};
+    if (nq >= kPipeMin) {
+        const int first = std::max(32, nq / 8);
+        cut.push_back(first);
+        const int rest = nq - first, parts = 3;
+        for (int i = 1; i <= parts; ++i) cut.push_back(first + (int)((long long)rest * i / parts));
+    } else {
+        cut.push_back(nq);
+    }
+    const int nchunks = (int)cut.size() - 1;
+    std::vector<QsfbBatchHandle*> H(nchunks, nullptr);
+    std::vector<int> prc(nchunks, kOk);
+    auto prepare = [&](int c) {
+        prc[c] = qsfb_batch_prepare(queries + cut[c], cut[c + 1] - cut[c], host_threads, &H[c]);
+    };
+    QsfbBatchStats total;
+    std::memset(&total, 0, sizeof(total));
+    int rc = kOk;
+    prepare(0);
+    for (int c = 0; c < nchunks; ++c) {
+        std::thread next;
+        if (c + 1 < nchunks) next = std::thread(prepare, c + 1);
+        if (rc == kOk) rc = prc[c];
+        if (rc == kOk) {
+            QsfbBatchStats st;
+            std::memset(&st, 0, sizeof(st));
+            rc = qsfb_batch_execute(H[c], out ? out + cut[c] : nullptr, &st);
+            total.prepare_seconds += st.prepare_seconds;
+            total.host_setup_seconds += st.host_setup_seconds;
+            total.device_seed_seconds += st.device_seed_seconds;
+            total.device_ms += st.device_ms;
+            total.device_span_ms += st.device_span_ms;
+            total.pair_ms += st.pair_ms;
+            total.tc_ms += st.tc_ms;
+            total.codewords += st.codewords;
+            total.popc_issued += st.popc_issued;
+            total.zero_codewords += st.zero_codewords;
+            total.tc_codewords += st.tc_codewords;
+            total.rounds += st.rounds;
+            total.kernel_launches += st.kernel_launches;
+            total.certificates += st.certificates;
+            total.device_bytes = std::max(total.device_bytes, st.device_bytes);
+            total.gen_ms += st.gen_ms;
+            total.host_plan_seconds += st.host_plan_seconds;
+            total.host_apply_seconds += st.host_apply_seconds;
+        }
+        qsfb_batch_free(H[c]);
+        H[c] = nullptr;
+        if (next.joinable()) next.join();
+    }
+    for (QsfbBatchHandle* h : H) qsfb_batch_free(h);
+    if (rc == kOk) {
+        for (int c = 0; c < nchunks; ++c)
+            if (prc[c] != kOk) { rc = prc[c]; break; }
+    }
+    if (stats) {
+        *stats = total;
+        stats->seconds = now_seconds() - t0;
+    }
     return rc;
 }
 

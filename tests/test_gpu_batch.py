@@ -101,3 +101,21 @@ def test_full_1024_batch_matches_reference(native):
             bad.append((i, "levels", a.levels, r[1]))
     assert not bad, bad[:10]
     assert st.certificates == 1024
+
+
+def test_one_shot_pipeline_equals_single_batch(native):
+    """qsfb_batch cuts batches of 256+ queries into pipelined chunks; the answers equal one
+    prepared batch executed as a whole."""
+    from qubitserf_b200 import workloads as W
+    items = native.batch_items(W.batch_1024(300))
+    ans, st = native.Batch(items).run()                 # pipelined (4 chunks)
+    b = native.Batch(items)
+    h = b.prepare()
+    ref, st2 = b.execute(h)                             # one batch
+    b.free(h)
+    assert st.certificates == st2.certificates == len(items)
+    for a, r in zip(ans, ref):
+        assert (a.distance, a.lower_bound, a.proven, a.levels, a.z_weight, a.x_weight) == \
+            (r.distance, r.lower_bound, r.proven, r.levels, r.z_weight, r.x_weight)
+        assert a.witness_ok == 1
+    assert st.codewords == st2.codewords
