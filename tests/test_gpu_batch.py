@@ -108,7 +108,7 @@ def test_one_shot_pipeline_equals_single_batch(native):
     prepared batch executed as a whole."""
     from qubitserf_b200 import workloads as W
     items = native.batch_items(W.batch_1024(300))
-    ans, st = native.Batch(items).run()                 # pipelined (4 chunks)
+    ans, st = native.Batch(items).run()                 # pipelined (3 chunks)
     b = native.Batch(items)
     h = b.prepare()
     ref, st2 = b.execute(h)                             # one batch
