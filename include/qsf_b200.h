@@ -264,10 +264,12 @@ int qsfb_microbench(int which, double* ops_per_s);
  * D = A * B^T over the first 32 * ksteps columns, with A 256 x 64 and B 128 x 64 int8
  * (row-major; the sweep stores +1 / -1 / 0) and D 256 x 128 int32 (row-major), computed
  * by the sweep's own copy, tcgen05 MMA and TMEM read-back path.  ksteps in 1..2.
- * ksteps = -1 runs the timeout drill: the operands are never copied, the kernel's bounded
- * waits run out after 50 ms and the call returns 4 with the device still usable.
+ * packed = 1 reads the accumulators back as the sweep does (16-bit halves, two columns per
+ * register; exact for |D| < 32768), 0 as 32-bit columns.  ksteps = -1 runs the timeout
+ * drill: the operands are never copied, the kernel's bounded waits run out after 50 ms and
+ * the call returns 4 with the device still usable.
  * Returns 0, 1 (null), 2 (ksteps), 4 (device or a wait that ran out) or 6 (memory). */
-int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D);
+int qsfb_tc_selftest(int ksteps, int packed, const int8_t* A, const int8_t* B, int32_t* D);
 
 /* Overwrite a 256 MiB device buffer (more than the 126 MB L2) and wait; benchmarks call it
  * between timed steps.  Returns 0, or 4 without a device. */

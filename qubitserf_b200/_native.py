@@ -136,7 +136,7 @@ SIGNATURES = [
     ("qsfb_server_stop", _i, [ctypes.c_void_p]),
     ("qsfb_microbench", _i, [_i, ctypes.POINTER(ctypes.c_double)]),
     ("qsfb_flush_l2", _i, []),
-    ("qsfb_tc_selftest", _i, [_i, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("qsfb_tc_selftest", _i, [_i, _i, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
 ]
@@ -470,15 +470,16 @@ def microbench(which):
     return v.value
 
 
-def tc_selftest(ksteps, A, B):
+def tc_selftest(ksteps, A, B, packed=False):
     """D = A[:, :32k] @ B[:, :32k].T (int32, 256 x 128) through the tensor-core sweep's own
-    copy / MMA / TMEM path; A is 256 x 64 and B 128 x 64 int8.  ksteps = -1 is the
-    timeout drill (raises RuntimeError with rc 4)."""
+    copy / MMA / TMEM path; A is 256 x 64 and B 128 x 64 int8.  packed: read back as the
+    sweep does (16-bit halves).  ksteps = -1 is the timeout drill (raises RuntimeError with
+    rc 4)."""
     A = np.ascontiguousarray(A, dtype=np.int8)
     B = np.ascontiguousarray(B, dtype=np.int8)
     if A.shape != (256, 64) or B.shape != (128, 64):
         raise ValueError("tc_selftest: A must be 256 x 64 and B 128 x 64 int8")
     D = np.zeros((256, 128), dtype=np.int32)
-    _check(lib().qsfb_tc_selftest(int(ksteps), A.ctypes.data, B.ctypes.data, D.ctypes.data),
-           "qsfb_tc_selftest")
+    _check(lib().qsfb_tc_selftest(int(ksteps), int(bool(packed)), A.ctypes.data, B.ctypes.data,
+                                  D.ctypes.data), "qsfb_tc_selftest")
     return D

@@ -20,8 +20,8 @@
 using namespace qsfb;
 
 namespace qsfb {
-cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int32_t* out,
-                               int* err, cudaStream_t st);
+cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int packed,
+                               int32_t* out, int* err, cudaStream_t st);
 int tc_tile_rows();
 int tc_tile_cols();
 cudaError_t microbench_peak(int which, int num_sms, uint32_t* d_out, cudaStream_t st,
@@ -708,7 +708,7 @@ int qsfb_microbench(int which, double* ops_per_s) {
     return e == cudaSuccess ? kOk : kErrDevice;
 }
 
-int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D) {
+int qsfb_tc_selftest(int ksteps, int packed, const int8_t* A, const int8_t* B, int32_t* D) {
     if (!A || !B || !D) return kErrNull;
     if (ksteps == 0 || ksteps < -1 || ksteps > kPmRowBytes / 32) return kErrShape;
     int rc = kOk;
@@ -741,7 +741,7 @@ int qsfb_tc_selftest(int ksteps, const int8_t* A, const int8_t* B, int32_t* D) {
     bool ok = cudaMemcpyAsync(buf, h.data(), bytes_a + bytes_b, cudaMemcpyHostToDevice, st) ==
                   cudaSuccess &&
               cudaMemsetAsync(dErr, 0, sizeof(int), st) == cudaSuccess &&
-              launch_tc_selftest(dA, dB, ksteps, dD, dErr, st) == cudaSuccess &&
+              launch_tc_selftest(dA, dB, ksteps, packed, dD, dErr, st) == cudaSuccess &&
               cudaMemcpyAsync(D, dD, bytes_d, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
               cudaMemcpyAsync(&herr, dErr, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
               cudaStreamSynchronize(st) == cudaSuccess;

@@ -219,6 +219,32 @@ __device__ __forceinline__ void tmem_ld128(uint32_t taddr, int32_t (&v)[128]) {
         : "memory");
 }
 
+// 128 consecutive accumulator columns of this thread's TMEM lane, read as 16-bit values:
+// register i holds the low halves of columns 2i and 2i + 1 (the accumulators here are
+// integers in [-64, 64], exact in 16 bits).  Load and wait in one statement.
+__device__ __forceinline__ void tmem_ld128_p16(uint32_t taddr, uint32_t (&v)[64]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.pack::16b.b32 {"
+        "%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+          "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]),
+          "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]),
+          "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]),
+          "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]),
+          "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]),
+          "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+        : "r"(taddr)
+        : "memory");
+}
+
 // Shared setup of both tensor-core kernels: barriers by thread 0, TMEM by warp 1.
 __device__ __forceinline__ uint32_t tc_setup(uint32_t bar0, int nbar, const uint32_t* counts,
                                              uint32_t* tmem_slot) {
@@ -470,26 +496,29 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 tc_fence_after();
                 __syncwarp();   // the TMEM load below is warp-collective
                 const int thr = n_live - 2 * (T - 1 - w);
-                int32_t v[128];
-                tmem_ld128(tmem + ((uint32_t)(quarter * 32) << 16) + (ac * kTcHalves + half) * kTcN,
-                           v);
+                // the accumulators are in [-64, 64]: read them as packed 16-bit halves
+                uint32_t v[64];
+                tmem_ld128_p16(tmem + ((uint32_t)(quarter * 32) << 16) + (ac * kTcHalves + half) * kTcN,
+                               v);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(acc_empty(ac));   // one arrival per warp
-                // per 64-column slice, four independent 3-input max chains
+                // per 64-column slice (32 registers), four chains of 16-bit x2 3-input maxima
                 uint32_t fbits = 0;
 #pragma unroll
                 for (int sl = 0; sl < 2; ++sl) {
-                    int m[4];
+                    uint32_t m[4];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        const int o = 64 * sl + 16 * c;
+                        const int o = 32 * sl + 8 * c;
                         m[c] = v[o];
 #pragma unroll
-                        for (int i = o + 1; i + 1 < o + 16; i += 2) m[c] = __vimax3_s32(v[i], v[i + 1], m[c]);
-                        m[c] = max(m[c], v[o + 15]);
+                        for (int i = o + 1; i + 1 < o + 8; i += 2) m[c] = __vimax3_s16x2(v[i], v[i + 1], m[c]);
+                        m[c] = __vmaxs2(m[c], v[o + 7]);
                     }
-                    if (max(max(m[0], m[1]), max(m[2], m[3])) >= thr) fbits |= 1u << sl;
+                    const uint32_t mm = __vmaxs2(__vmaxs2(m[0], m[1]), __vmaxs2(m[2], m[3]));
+                    const int mx = max((int)(int16_t)(mm & 0xFFFFu), (int)(int16_t)(mm >> 16));
+                    if (mx >= thr) fbits |= 1u << sl;
                 }
                 const uint32_t flags = valid ? fbits : 0u;
                 // Flagged slices are rescanned by the whole warp: the 32 lanes screen the
@@ -577,7 +606,7 @@ __global__ void __launch_bounds__(256) expand_pm_kernel(const ExpandDesc* __rest
 // broken pipeline would; the launch still ends normally and frees its TMEM.
 __global__ void __launch_bounds__(kTcThreads, 1)
 tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, int ksteps,
-                   int32_t* __restrict__ out, int* __restrict__ err) {
+                   int packed, int32_t* __restrict__ out, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t s0 = smem_u32(smem);
@@ -615,10 +644,19 @@ tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, 
             tc_fence_after();
             __syncwarp();
             int32_t* o = out + (size_t)(half * kTcM + quarter * 32 + lane) * kTcN;
-            for (int cs = 0; cs < kTcN / kTcSlice; ++cs) {
-                int32_t v[64];
-                tmem_ld64(tmem + ((uint32_t)(quarter * 32) << 16) + half * kTcN + cs * kTcSlice, v);
-                for (int i = 0; i < 64; ++i) o[cs * kTcSlice + i] = v[i];
+            if (packed) {   // the sweep's read-back: 16-bit halves, sign-extended here
+                uint32_t v[64];
+                tmem_ld128_p16(tmem + ((uint32_t)(quarter * 32) << 16) + half * kTcN, v);
+                for (int i = 0; i < 64; ++i) {
+                    o[2 * i] = (int32_t)(int16_t)(v[i] & 0xFFFFu);
+                    o[2 * i + 1] = (int32_t)(int16_t)(v[i] >> 16);
+                }
+            } else {
+                for (int cs = 0; cs < kTcN / kTcSlice; ++cs) {
+                    int32_t v[64];
+                    tmem_ld64(tmem + ((uint32_t)(quarter * 32) << 16) + half * kTcN + cs * kTcSlice, v);
+                    for (int i = 0; i < 64; ++i) o[cs * kTcSlice + i] = v[i];
+                }
             }
         } else if (lane == 0) {
             atomicCAS(err, 0, 3);
@@ -672,13 +710,14 @@ cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
     return cudaGetLastError();
 }
 
-cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int32_t* out,
-                               int* err, cudaStream_t st) {
+cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int packed,
+                               int32_t* out, int* err, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(dev::tc_selftest_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)dev::kTcSmem);
     if (e != cudaSuccess) return e;
-    dev::tc_selftest_kernel<<<1, dev::kTcThreads, dev::kTcSmem, st>>>(A, Bm, ksteps, out, err);
+    dev::tc_selftest_kernel<<<1, dev::kTcThreads, dev::kTcSmem, st>>>(A, Bm, ksteps, packed, out,
+                                                                     err);
     return cudaGetLastError();
 }
 

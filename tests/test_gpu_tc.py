@@ -16,13 +16,14 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+@pytest.mark.parametrize("packed", [False, True])
 @pytest.mark.parametrize("ksteps", [1, 2])
-def test_selftest_matches_integer_product(native, ksteps):
+def test_selftest_matches_integer_product(native, ksteps, packed):
     rng = np.random.default_rng(10 + ksteps)
     vals = np.array([-1, 0, 1], dtype=np.int8)
     A = rng.choice(vals, size=(256, 64), p=[0.45, 0.1, 0.45]).astype(np.int8)
     B = rng.choice(vals, size=(128, 64), p=[0.45, 0.1, 0.45]).astype(np.int8)
-    D = native.tc_selftest(ksteps, A, B)
+    D = native.tc_selftest(ksteps, A, B, packed=packed)
     k = 32 * ksteps
     ref = A[:, :k].astype(np.int32) @ B[:, :k].astype(np.int32).T
     assert np.array_equal(D, ref)
