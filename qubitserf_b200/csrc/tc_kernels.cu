@@ -20,10 +20,11 @@
 // (16-byte chunk c of row e at c ^ ((e >> 1) & 3)), so a plain bulk copy of 8-row-aligned
 // rows lands in the 64-byte-swizzled K-major operand layout.
 //
-// CTA = 12 warps: warps 0 and 10 issue the bulk copies, warp 1 owns the TMEM allocation
+// CTA = 20 warps: warps 0 and 18 issue the bulk copies, warp 1 owns the TMEM allocation
 // (four 128-column accumulators = all 512 columns: two halves x double buffer), warps 1
-// and 11 issue the MMAs (one thread each, by suffix-tile parity), warps 2-9 read back (two
-// warps per TMEM lane quarter, one per half; one `tcgen05.ld` of 128 columns per tile).  Reading the accumulators back is
+// and 19 issue the MMAs (one thread each, by suffix-tile parity), warps 2-17 read back in
+// two groups of eight, one per accumulator buffer (even / odd suffix tiles), each with one
+// warp per TMEM lane quarter and half and one packed `tcgen05.ld` of 128 columns per tile.  Reading the accumulators back is
 // what bounds the sweep: 4 bytes of TMEM per pair against 64 MACs of MMA work.  Every wait is bounded (about two seconds of
 // %globaltimer); a wait that runs out sets the launch's error word (1 copy warp, 2 MMA
 // warp, 3 read-back warps: the first role that gave up) and the CTA winds down without
@@ -45,7 +46,8 @@ constexpr int kTcK = 2;                    // K = 32 steps (64 columns)
 constexpr int kTcBStages = 8;              // suffix tiles in flight
 constexpr int kTcJB = 16;                  // suffix tiles per job
 constexpr int kTcSlice = 64;               // accumulator columns per rescan slice
-constexpr int kTcEpiWarps = 8;             // 2 halves x 4 lane quarters
+constexpr int kTcEpiGroups = 2;            // read-back groups: one per accumulator buffer
+constexpr int kTcEpiWarps = 8 * kTcEpiGroups;   // x 2 halves x 4 lane quarters
 constexpr int kTcThreads = 32 * (4 + kTcEpiWarps);   // + two copy and two MMA warps
 constexpr uint32_t kTcHalfBytes = kTcM * kPmRowBytes;      // 8 KB
 constexpr uint32_t kTcABytes = kTcRows * kPmRowBytes;      // 16 KB
@@ -380,7 +382,8 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     uint32_t counts[kNBar];
     for (int i = 0; i < kNBar; ++i) counts[i] = 1;
     counts[2] = counts[3] = 2;   // a prefix slot is released by both MMA threads
-    counts[4 + 2 * kTcBStages] = counts[5 + 2 * kTcBStages] = kTcEpiWarps;   // one per warp
+    // one arrival per read-back warp of the buffer's group
+    counts[4 + 2 * kTcBStages] = counts[5 + 2 * kTcBStages] = kTcEpiWarps / kTcEpiGroups;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 256);
     const uint32_t tmem = tc_setup(bar, kNBar, counts, tmem_slot);
 
@@ -391,9 +394,10 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     // operations, and two chains per role keep the tensor pipe fed.  The thread of parity p
     // owns the suffix stages of parity p and accumulator buffer p; the prefix tile is loaded
     // by the parity-0 copier and released when both MMA threads have committed.
-    const bool is_copy = warp == 0 || warp == 10;
-    const bool is_mma = warp == 1 || warp == 11;
-    const uint32_t par = warp >= 10 ? 1u : 0u;
+    constexpr int kWarpCopy1 = 2 + kTcEpiWarps, kWarpMma1 = 3 + kTcEpiWarps;
+    const bool is_copy = warp == 0 || warp == kWarpCopy1;
+    const bool is_mma = warp == 1 || warp == kWarpMma1;
+    const uint32_t par = warp >= kWarpCopy1 ? 1u : 0u;
     if (is_copy) {
         // ------------------------------------------------------------ tile copies
         if (lane == 0) {
@@ -465,7 +469,8 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
         // ------------------------------------------------------------ read-back
         const int e = warp - 2;
         const int quarter = warp & 3;            // TMEM lanes [32*quarter, 32*quarter+32)
-        const int half = e >> 2;                 // accumulator / prefix half
+        const int half = (e >> 2) & 1;           // accumulator / prefix half
+        const uint32_t group = (uint32_t)(e >> 3);   // reads the tiles of this parity
         const int row = half * kTcM + quarter * 32 + lane;   // prefix-tile row
         uint32_t it_c = 0;
         bool ok = true;
@@ -486,8 +491,9 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             if (C.key == kptr) T = min(T, tkey);
             const unsigned long long kv = *((volatile unsigned long long*)C.key);
             const int n_live = (int)((C.tnw >> 12) & 0xFFu), w = (int)(C.tnw >> 20);
-            for (unsigned long long bt = b0; bt < b1; ++bt) {
+            for (unsigned long long bt = b0; bt < b1; ++bt, ++it_c) {
                 const uint32_t ac = it_c & 1u;
+                if (ac != group) continue;               // the other group's tile
                 // one lane polls the barrier, the warp follows (256 pollers would contend)
                 if (lane == 0)
                     ok = mbar_wait(tile_done(it_c % kTcBStages), (it_c / kTcBStages) & 1u);
@@ -557,7 +563,6 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                         }
                     }
                 }
-                ++it_c;
             }
             if (!ok) break;
             kptr = C.key;
