@@ -332,10 +332,12 @@ def main():
             "peak_source": ("2 x measured bf16 dense (MEASURED_PEAKS.json bf16_tflops, burst)"
                             if bf16 else "2 x fallback bf16 1.59 PFLOP/s"),
             "numerator": "tensor-core codewords x 128 int8 ops (64 columns) / kernel time",
-            "binding": {"resource": "TMEM read-back of the s32 accumulators (4 B per pair)",
-                        "tmem_read_gbs": tc_cw * 4 / max(tc_s, 1e-12) / 1e9,
-                        "bytes_per_clk_per_sm": tc_cw * 4 / max(tc_s, 1e-12) /
-                                                (nsm * f_mhz * 1e6)},
+            "binding": {"resource": "per-tile hand-off chain between the copy, MMA-issue and "
+                                    "TMEM read-back roles (ncu: tensor pipe, TMEM, L2 and DRAM "
+                                    "all below saturation)",
+                        "tmem_columns_read_gbs": tc_cw * 4 / max(tc_s, 1e-12) / 1e9,
+                        "tmem_bytes_per_clk_per_sm": tc_cw * 4 / max(tc_s, 1e-12) /
+                                                     (nsm * f_mhz * 1e6)},
             "codeword_share": tc_cw / max(cw, 1),
             "kernel_ms_per_step": tc_ms / max(args.steps, 1)},
         "roofline_cuda_core": {
