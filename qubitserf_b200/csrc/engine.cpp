@@ -157,11 +157,19 @@ Session* Device::acquire() {
     s->dev = this;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess ||
-        cudaEventCreate(&s->ev_tc0) != cudaSuccess || cudaEventCreate(&s->ev_tc1) != cudaSuccess) {
+        cudaEventCreate(&s->ev_tc0) != cudaSuccess || cudaEventCreate(&s->ev_tc1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         delete s;
         return nullptr;
     }
+    for (int k = 0; k < Session::kAux; ++k)
+        if (cudaStreamCreateWithFlags(&s->aux[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->ev_join[k], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            delete s;
+            return nullptr;
+        }
     return s;
 }
 
@@ -851,32 +859,49 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     cudaEvent_t evm;
     cudaEventCreate(&evm);
     cudaEventRecord(evm, st);
+    // fork: the pair launches (independent levels; they share only the atomic witness keys)
+    // go round-robin over the auxiliary streams, the tensor-core sweep first
+    cudaEventRecord(s->ev_fork, st);
+    for (int k = 0; k < Session::kAux; ++k) cudaStreamWaitEvent(s->aux[k], s->ev_fork, 0);
     unsigned long long all_jobs = 0;
     bool tc_timed = false;
-    for (size_t gi = 0; gi < groups.size(); ++gi) {
+    int next_aux = 0;
+    for (size_t gi0 = 0; gi0 < groups.size(); ++gi0) {
+        // tensor-core group (sorted last) launched first
+        const size_t gi = (groups.back().tc ? (gi0 == 0 ? groups.size() - 1 : gi0 - 1) : gi0);
         const Group& Gp = groups[gi];
         const LevelDesc* gd = (const LevelDesc*)(d + off_lvl) + Gp.first;
-        if (Gp.tc) cudaEventRecord(s->ev_tc0, st);
+        cudaStream_t gs = s->aux[next_aux];
+        next_aux = (next_aux + 1) % Session::kAux;
+        if (Gp.tc) cudaEventRecord(s->ev_tc0, gs);
         const cudaError_t e =
             Gp.tc ? launch_pairs_tc(gd, Gp.count, Gp.jobs, dev->d_binom, d + off_recs,
-                                    (int*)(d + off_err), dev->num_sms, st)
+                                    (int*)(d + off_err), dev->num_sms, gs)
                   : launch_pairs(Gp.filt, Gp.HP, Gp.mode, gd, Gp.count, Gp.jobs,
                                  (unsigned long long*)s->d_ctr.d + gi, dev->d_binom,
-                                 dev->num_sms, st);
+                                 dev->num_sms, gs);
         if (e != cudaSuccess) {
             if (debug_level() >= 1)
                 std::fprintf(stderr, "qsfb: pair launch failed: %s\n", cudaGetErrorString(e));
+            cudaGetLastError();
+            // nothing launched so far may still run when the staging is reused
+            for (int k = 0; k < Session::kAux; ++k) cudaStreamSynchronize(s->aux[k]);
             cudaGetLastError();
             cudaEventDestroy(evm);
             return kErrDevice;
         }
         if (Gp.tc) {
-            cudaEventRecord(s->ev_tc1, st);
+            cudaEventRecord(s->ev_tc1, gs);
             tc_timed = true;
             launches += 1;   // the job-decode kernel
         }
         ++launches;
         all_jobs += Gp.jobs;
+    }
+    // join
+    for (int k = 0; k < Session::kAux; ++k) {
+        cudaEventRecord(s->ev_join[k], s->aux[k]);
+        cudaStreamWaitEvent(st, s->ev_join[k], 0);
     }
     cudaEventRecord(s->ev1, st);
     cudaError_t se = cudaMemcpyAsync(h + off_keys, d + off_keys, off_err + 8 - off_keys,

@@ -84,6 +84,12 @@ struct Session {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_tc0 = nullptr, ev_tc1 = nullptr;   // around the tensor-core sweep
+    // pair launches of a round are spread over these streams (forked after the list
+    // generation, joined before the results are read back): their tails overlap
+    static constexpr int kAux = 3;
+    cudaStream_t aux[kAux] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kAux] = {nullptr, nullptr, nullptr};
     DevScratch d_stage;    // descriptors + term tables + keys/counts
     HostScratch h_stage;   // pinned mirror of d_stage
     DevScratch d_ctr;      // job counters (one per kernel variant)
