@@ -381,6 +381,7 @@ struct Plan {
     unsigned long long range_pairs;  // pairs of this plan's terms
     int p_lo, nterms;
     int table = -1;                  // term job table (prefix sums, nterms + 1 entries)
+    ListBuf* list[2] = {nullptr, nullptr};   // prefix (a) and suffix (b) lists of its set
     unsigned long long jobs;
 };
 
@@ -539,12 +540,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             }
         }
     } clear_queued{gens, exps};
-    for (const Plan& P : plans) {
+    for (Plan& P : plans) {
         SideDev* S = reqs[P.req].side;
         for (int side = 0; side < 2; ++side) {
             const int size = side == 0 ? P.a : P.b;   // b = 0: one empty entry
             auto key = std::make_tuple(P.g, size, side);
-            ListBuf& L = S->lists[key];
+            ListBuf& L = S->lists[key];   // map nodes are stable: kept in the plan
+            P.list[side] = &L;
             if (!(L.ready || L.queued)) {
                 if (L.words) {   // allocated by an earlier execution: regenerate in place
                     L.queued = true;
@@ -784,8 +786,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         Group& Gp = groups.back();
         SideDev* S = reqs[P.req].side;
         LevelDesc& D = hl[oi];
-        const ListBuf& La = S->lists[std::make_tuple(P.g, P.a, 0)];
-        const ListBuf& Rb = S->lists[std::make_tuple(P.g, P.b, 1)];
+        const ListBuf& La = *P.list[0];
+        const ListBuf& Rb = *P.list[1];
         D.red = S->d_red + (size_t)P.g * S->K * S->W32;
         D.syn = S->d_syn + (size_t)P.g * S->K * std::max(S->SW, 1);
         D.la = La.words;
