@@ -5,6 +5,10 @@
 #include "bz.hpp"
 
 #include <algorithm>
+#include <tuple>
+#include <mutex>
+#include <memory>
+#include <map>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -101,7 +105,34 @@ int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, b
     return best;
 }
 
+namespace {
+// The column orders depend only on (n, trials, seed) and the process's thread count, so
+// every code of the same length shares them: computed once per key.
+std::vector<int> seed_orders_uncached(int n, int trials, unsigned seed, int only);
+std::mutex g_orders_mu;
+std::map<std::tuple<int, int, unsigned>, std::shared_ptr<const std::vector<int>>> g_orders;
+}  // namespace
+
 std::vector<int> seed_orders(int n, int trials, unsigned seed, int only) {
+    const auto key = std::make_tuple(n, trials, seed);
+    std::shared_ptr<const std::vector<int>> all;
+    {
+        std::lock_guard<std::mutex> lk(g_orders_mu);
+        auto it = g_orders.find(key);
+        if (it != g_orders.end()) all = it->second;
+    }
+    if (!all) {
+        auto v = std::make_shared<const std::vector<int>>(seed_orders_uncached(n, trials, seed, -1));
+        std::lock_guard<std::mutex> lk(g_orders_mu);
+        all = g_orders.emplace(key, v).first->second;
+    }
+    if (only < 0) return *all;
+    if (only >= trials || (size_t)(only + 1) * n > all->size()) return {};
+    return std::vector<int>(all->begin() + (size_t)only * n, all->begin() + (size_t)(only + 1) * n);
+}
+
+namespace {
+std::vector<int> seed_orders_uncached(int n, int trials, unsigned seed, int only) {
     int nth = (int)std::thread::hardware_concurrency();
     if (nth < 1) nth = 1;
     if (nth > trials) nth = trials;
@@ -122,6 +153,7 @@ std::vector<int> seed_orders(int n, int trials, unsigned seed, int only) {
     }
     return out;
 }
+}  // namespace
 
 void BzSide::apply_device_seed(unsigned key) {
     seed_pending = false;
