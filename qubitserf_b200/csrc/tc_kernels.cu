@@ -13,22 +13,26 @@
 // and hands the rare slices that reach the threshold to the exact survivor evaluation
 // shared with the CUDA-core sweep (same key, same tie-breaking, same counts).
 //
-// Data movement is what bounds this kernel, so every suffix row fetched into shared
-// memory serves 256 prefix rows: a job holds a 256-row prefix tile (two M = 128 halves,
-// 16 KB) and streams 128-row suffix tiles (8 KB) through an 8-deep ring; each suffix tile
-// feeds two accumulators, one per half.  Rows are 64 bytes, pre-swizzled in global memory
-// (16-byte chunk c of row e at c ^ ((e >> 1) & 3)), so a plain bulk copy of 8-row-aligned
-// rows lands in the 64-byte-swizzled K-major operand layout.
+// Every suffix row fetched into shared memory serves 256 prefix rows, which keeps the
+// operand traffic far below L2 and DRAM bandwidth: a job holds a 256-row prefix tile (two
+// M = 128 halves, 16 KB) and streams 128-row suffix tiles (8 KB) through an 8-deep ring;
+// each suffix tile feeds two accumulators, one per half.  Rows are 64 bytes, pre-swizzled
+// in global memory (16-byte chunk c of row e at c ^ ((e >> 1) & 3)), so a plain bulk copy
+// of 8-row-aligned rows lands in the 64-byte-swizzled K-major operand layout.
 //
 // CTA = 20 warps: warps 0 and 18 issue the bulk copies, warp 1 owns the TMEM allocation
 // (four 128-column accumulators = all 512 columns: two halves x double buffer), warps 1
 // and 19 issue the MMAs (one thread each, by suffix-tile parity), warps 2-17 read back in
 // two groups of eight, one per accumulator buffer (even / odd suffix tiles), each with one
-// warp per TMEM lane quarter and half and one packed `tcgen05.ld` of 128 columns per tile.  Reading the accumulators back is
-// what bounds the sweep: 4 bytes of TMEM per pair against 64 MACs of MMA work.  Every wait is bounded (about two seconds of
-// %globaltimer); a wait that runs out sets the launch's error word (1 copy warp, 2 MMA
-// warp, 3 read-back warps: the first role that gave up) and the CTA winds down without
-// touching the device further.
+// warp per TMEM lane quarter and half and one packed `tcgen05.ld` of 128 columns per tile.
+// The sweep is bound by TMEM capacity over the accumulator round trip: the 512 columns hold
+// 64k accumulators, and each goes MMA -> commit -> read-back -> release (~1,400 cycles)
+// before its columns take the next tile, about 47 pairs per clock per SM against the
+// ~120 that the dense int8 peak allows at 64 MACs a pair.
+//
+// Every wait is bounded (about two seconds of %globaltimer); a wait that runs out sets the
+// launch's error word (1 copy warp, 2 MMA warp, 3 read-back warps: the first role that
+// gave up) and the CTA winds down without touching the device further.
 #include <cuda_runtime.h>
 #include <cstdint>
 
