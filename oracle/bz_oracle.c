@@ -1046,3 +1046,91 @@ int orc_prepare(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, in
     m_free(&b);
     return 0;
 }
+
+/* ------------------------------------------------------------------ codeaut collection
+ * The low-weight collector behind codeaut_bz_collect (cpp/codeaut/bz.cpp:55-117): for every
+ * subset size sw = 1..min(p, m) every sw-subset of G's rows is XORed, and the results of
+ * weight 1..keep are kept (the CollectSink of cpp/qsf/enum_core.hpp:90-103: weight 0, a
+ * dependent subset, is never kept); the kept rows are then sorted by their packed words,
+ * word 0 first (RowLess, bz.cpp:38-50), and duplicates dropped.  The combination count
+ * saturates at 2^62 per level and in total (COMBO_CAP, bz.cpp:29, 87-97).  Subsets are
+ * visited in the reference's lexicographic order (next_comb, cpp/qsf/combinatorics.hpp:
+ * 64-71); acc[i] holds the XOR of the rows pos[0..i]. */
+static int orc_stride_words;
+static int cmp_rows(const void* a, const void* b) {
+    const u64* x = (const u64*)a;
+    const u64* y = (const u64*)b;
+    for (int i = 0; i < orc_stride_words; ++i)
+        if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+    return 0;
+}
+
+long long orc_collect(const uint8_t* G, int m, int n, int p, int keep, uint64_t** out,
+                      long long* combos) {
+    const long long cap62 = (long long)1 << 62;
+    *out = NULL;
+    *combos = 0;
+    if (m <= 0 || n <= 0 || p <= 0) return 0;
+    const int s = words_for(n);
+    mat rows = m_from_dense(G, m, n);
+    const int maxsw = p < m ? p : m;
+    size_t nh = 0, caph = 1024;
+    u64* hits = (u64*)malloc(caph * s * sizeof(u64));
+    u64* acc = (u64*)calloc((size_t)maxsw * s, sizeof(u64));
+    int* pos = (int*)malloc(sizeof(int) * (size_t)maxsw);
+    if (!hits || !acc || !pos) { free(hits); free(acc); free(pos); m_free(&rows); return -1; }
+    for (int sw = 1; sw <= maxsw; ++sw) {
+        /* C(m, sw) with the reference's saturation */
+        unsigned long long c = 1;
+        int sat = 0;
+        for (int i = 1; i <= sw && !sat; ++i) {
+            unsigned __int128 t = (unsigned __int128)c * (unsigned)(m - sw + i) / (unsigned)i;
+            if (t > (unsigned __int128)cap62) sat = 1; else c = (unsigned long long)t;
+        }
+        const long long total = sat ? cap62 : (long long)c;
+        *combos = (*combos > cap62 - total) ? cap62 : *combos + total;
+        for (int i = 0; i < sw; ++i) pos[i] = i;
+        int from = 0;   /* first position whose prefix XOR must be rebuilt */
+        for (;;) {
+            for (int i = from; i < sw; ++i) {
+                u64* a = acc + (size_t)i * s;
+                const u64* r = m_row(&rows, pos[i]);
+                for (int w = 0; w < s; ++w) a[w] = (i ? acc[(size_t)(i - 1) * s + w] : 0) ^ r[w];
+            }
+            const u64* cw = acc + (size_t)(sw - 1) * s;
+            const int wt = v_weight(cw, s);
+            if (wt > 0 && wt <= keep) {
+                if (nh == caph) {
+                    caph *= 2;
+                    u64* nhits = (u64*)realloc(hits, caph * s * sizeof(u64));
+                    if (!nhits) { free(hits); free(acc); free(pos); m_free(&rows); return -1; }
+                    hits = nhits;
+                }
+                memcpy(hits + nh * s, cw, (size_t)s * sizeof(u64));
+                ++nh;
+            }
+            int j = sw - 1;
+            while (j >= 0 && pos[j] == m - sw + j) --j;
+            if (j < 0) break;
+            ++pos[j];
+            for (int t = j + 1; t < sw; ++t) pos[t] = pos[t - 1] + 1;
+            from = j;
+        }
+    }
+    orc_stride_words = s;
+    if (nh > 1) qsort(hits, nh, (size_t)s * sizeof(u64), cmp_rows);
+    size_t nu = 0;
+    for (size_t i = 0; i < nh; ++i) {
+        if (nu > 0 && memcmp(hits + (nu - 1) * s, hits + i * s, (size_t)s * sizeof(u64)) == 0)
+            continue;
+        if (nu != i) memcpy(hits + nu * s, hits + i * s, (size_t)s * sizeof(u64));
+        ++nu;
+    }
+    free(acc);
+    free(pos);
+    m_free(&rows);
+    *out = hits;
+    return (long long)nu;
+}
+
+void orc_free(void* ptr) { free(ptr); }

@@ -65,4 +65,13 @@ int orc_pauli_operator_weight(const uint8_t* G, int rows, int cols, const uint8_
 int orc_prepare(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br, int bc,
                 int* meta, int* ranks, int max_gamma);
 
+/* codeaut low-weight collection (cpp/codeaut/bz.cpp:55-117): the distinct nonzero XORs of
+ * size-1..p subsets of the m x n 0/1 rows of G with weight <= keep, sorted by packed 64-bit
+ * words (word 0 first).  Returns their count with the rows in *out (ceil(n/64) words each;
+ * release with orc_free) and the saturating combination count in *combos; -1 if memory
+ * runs out. */
+long long orc_collect(const uint8_t* G, int m, int n, int p, int keep, uint64_t** out,
+                      long long* combos);
+void orc_free(void* ptr);
+
 #endif

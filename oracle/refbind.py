@@ -49,6 +49,17 @@ def _u64p(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
 
 
+def unpack_rows(packed, n):
+    """0/1 rows of n columns from rows of little-endian 64-bit words (bit j of word w is
+    column 64 w + j)."""
+    packed = np.ascontiguousarray(packed, dtype=np.uint64)
+    if packed.shape[0] == 0:
+        return np.zeros((0, n), dtype=np.uint8)
+    bits = np.unpackbits(packed.view(np.uint8).reshape(packed.shape[0], -1), axis=1,
+                         bitorder="little")
+    return bits[:, :n].copy()
+
+
 def ref_available() -> bool:
     return REF_LIB.exists()
 
@@ -193,6 +204,34 @@ class Ref:
             "even": bool(even), "count_all": bool(count_all), "seed_upper": seed_upper,
         }
 
+
+    def collect(self, G, p, keep, threads=0):
+        """The reference's codeaut low-weight collector (``codeaut_bz_collect``,
+        cpp/codeaut/bz.cpp:55-117) on its CPU backend: ``(rows uint8[count, n], combos)``."""
+        L = self.lib
+        vp = ctypes.c_void_p
+        L.codeaut_bz_collect.restype = vp
+        L.codeaut_bz_collect.argtypes = [ctypes.POINTER(ctypes.c_uint8)] + [ctypes.c_int32] * 6
+        for name, rt in (("codeaut_bz_ok", ctypes.c_int32), ("codeaut_bz_count", ctypes.c_int64),
+                         ("codeaut_bz_combos", ctypes.c_int64)):
+            getattr(L, name).restype = rt
+            getattr(L, name).argtypes = [vp]
+        L.codeaut_bz_copy_rows.restype = None
+        L.codeaut_bz_copy_rows.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8)]
+        L.codeaut_bz_free.restype = None
+        L.codeaut_bz_free.argtypes = [vp]
+        g = u8(G)
+        m, n = g.shape
+        h = L.codeaut_bz_collect(_p(g), m, n, int(p), int(keep), 0, int(threads))
+        try:
+            assert L.codeaut_bz_ok(h) == 1
+            cnt = int(L.codeaut_bz_count(h))
+            rows = np.zeros((max(cnt, 1), n), dtype=np.uint8)
+            if cnt:
+                L.codeaut_bz_copy_rows(h, _p(rows))
+            return rows[:cnt], int(L.codeaut_bz_combos(h))
+        finally:
+            L.codeaut_bz_free(h)
 
 class OrcResult(ctypes.Structure):
     _fields_ = [("distance", ctypes.c_int), ("lower_bound", ctypes.c_int),
@@ -353,3 +392,28 @@ class Oracle:
         return {"n": m[0], "K": m[1], "ranks": [ranks[i] for i in range(m[2])],
                 "kcheck": m[3], "even": bool(m[4]), "count_all": bool(m[5]),
                 "seed_upper": m[6]}
+
+    def collect(self, G, p, keep):
+        """The C restatement of the codeaut collector: ``(rows uint8[count, n], combos)``."""
+        L = self.lib
+        pp = ctypes.POINTER(ctypes.c_uint64)
+        L.orc_collect.restype = ctypes.c_longlong
+        L.orc_collect.argtypes = [ctypes.POINTER(ctypes.c_uint8), ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(pp),
+                                  ctypes.POINTER(ctypes.c_longlong)]
+        L.orc_free.restype = None
+        L.orc_free.argtypes = [ctypes.c_void_p]
+        g = u8(G)
+        m, n = g.shape
+        out = pp()
+        combos = ctypes.c_longlong(0)
+        cnt = L.orc_collect(_p(g) if g.size else None, m, n, int(p), int(keep),
+                            ctypes.byref(out), ctypes.byref(combos))
+        assert cnt >= 0
+        s = (n + 63) // 64
+        try:
+            packed = (np.ctypeslib.as_array(out, shape=(cnt * s,)).copy() if cnt
+                      else np.zeros(0, np.uint64))
+        finally:
+            L.orc_free(ctypes.cast(out, ctypes.c_void_p))
+        return unpack_rows(packed.reshape(cnt, s), n), int(combos.value)
