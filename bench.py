@@ -177,11 +177,15 @@ def main():
     ap.add_argument("--only-resident", action="store_true",
                     help="time only the resident-input rounds (profiling runs)")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "css128", "classical128", "classical96"],
-                    help="batch = the 1024-code batch; the others certify one code")
+                    choices=["batch", "css128", "classical128", "classical96", "collect"],
+                    help="batch = the 1024-code batch; collect = the codeaut low-weight "
+                         "collector; the others certify one code")
     args = ap.parse_args()
 
     rank, world, local, pg = dist_setup(args.gpus)
+    if args.workload == "collect":
+        bench_collect(args, rank, world, local, pg)
+        return
     from qubitserf_b200 import workloads as W
     if args.workload == "batch":
         codes = W.batch_1024(args.codes)
@@ -332,8 +336,9 @@ def main():
             "peak_source": ("2 x measured bf16 dense (MEASURED_PEAKS.json bf16_tflops, burst)"
                             if bf16 else "2 x fallback bf16 1.59 PFLOP/s"),
             "numerator": "tensor-core codewords x 128 int8 ops (64 columns) / kernel time",
-            "binding": {"resource": "per-tile hand-off chain between the copy, MMA-issue and "
-                                    "TMEM read-back roles (ncu: tensor pipe, TMEM, L2 and DRAM "
+            "binding": {"resource": "TMEM capacity over the accumulator round trip: 64k "
+                                    "accumulators in flight, each MMA -> commit -> read-back -> "
+                                    "release before reuse (ncu: tensor pipe, TMEM, L2 and DRAM "
                                     "all below saturation)",
                         "tmem_columns_read_gbs": tc_cw * 4 / max(tc_s, 1e-12) / 1e9,
                         "tmem_bytes_per_clk_per_sm": tc_cw * 4 / max(tc_s, 1e-12) /
@@ -366,6 +371,113 @@ def main():
                                         np.arange(1, len(dists) + 1))),
     }
     print(json.dumps(line), flush=True)
+
+
+COLLECT = {"n": 128, "k": 64, "seed": 13, "p": 9, "keep": 20, "sample_p": 8}
+COLLECT_METRIC = "codeaut low-weight collection: subset combinations/s on 1 B200"
+
+
+def collect_reference_sample(G, p, keep, start=0):
+    """The reference's own codeaut_bz_collect (oracle/_ref, its CPU backend, all host
+    threads) on the bounded sample p = sample_p of the same generator."""
+    from oracle.refbind import Ref
+    ref = Ref()
+    t = time.perf_counter()
+    rows, combos = ref.collect(G, p, keep, threads=0)
+    dt = time.perf_counter() - t
+    return {"value": combos / dt, "unit": "combos/s", "cores": os.cpu_count(),
+            "kind": "reference", "rows": int(rows.shape[0]),
+            "sample": f"subset sizes 1..{p} of the same generator ({combos} combinations) "
+                      f"in {dt:.2f} s"}
+
+
+def bench_collect(args, rank, world, local, pg):
+    """The codeaut collector (codeaut_bz_collect): a step collects every XOR of 1..p rows
+    of a random systematic [n, k] generator with weight <= keep.  value = combinations per
+    second of device time (list generation + pair sweeps, G already packed on the device by
+    the call); e2e = the same combinations over the wall time of the public handle call
+    (host packing, upload, sweeps, download, host sort) plus copying the rows out."""
+    from qubitserf_b200 import workloads as W
+    c = COLLECT
+    G = W.collect_generator(c["n"], c["k"], c["seed"])
+    wname = f"codeaut_collect_systematic_n{c['n']}_k{c['k']}_p{c['p']}_keep{c['keep']}_seed{c['seed']}"
+    config = {"workload": wname, "n": c["n"], "k": c["k"], "p": c["p"], "keep": c["keep"],
+              "parallelism": f"replicas{world}",
+              "l2": "256 MiB L2 flush before every timed step (lists fit in L2)",
+              "timed": "list generation + pair sweeps, CUDA events of the call"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        for _ in range(min(args.warmup, 1)):
+            collect_reference_sample(G, 3, c["keep"])
+        vals, b = [], None
+        for _ in range(args.steps):
+            b = collect_reference_sample(G, c["sample_p"], c["keep"])
+            vals.append(b["value"])
+        v = float(np.mean(vals))
+        print(json.dumps({"metric": COLLECT_METRIC, "value": v, "unit": "combos/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                          "config": config, "impl": "reference",
+                          "cpu_baseline": {**b, "value": v},
+                          "e2e": {"value": v, "unit": "combos/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    from qubitserf_b200 import _native
+    if not _native.backend_available("gpu"):
+        raise SystemExit("no sm_100 device visible")
+    popc_peak = _native.microbench(0)
+    rows = None
+    for _ in range(args.warmup):
+        rows, combos, st = _native.collect(G, c["p"], c["keep"], stats=True)
+    barrier(pg)
+    dev_s, wall_s, launches, passes, hits = 0.0, 0.0, 0, 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            _native.lib().qsfb_flush_l2()
+            t = time.perf_counter()
+            rows2, combos, st = _native.collect(G, c["p"], c["keep"], stats=True)
+            wall_s += time.perf_counter() - t
+            dev_s += (st.gen_ms + st.pairs_ms) / 1e3
+            launches += st.launches
+            passes += st.passes
+            hits += st.hits
+            pairs_s = st.pairs_ms / 1e3
+            assert rows is None or np.array_equal(rows, rows2)
+            rows = rows2
+    dev_s = max_over_ranks(pg, dev_s)
+    wall_s = max_over_ranks(pg, wall_s)
+    value = combos * args.steps * world / dev_s
+    e2e = combos * args.steps * world / wall_s
+    if rank != 0:
+        return
+    S64 = (c["n"] + 63) // 64
+    alg_popc = 2 * S64            # POPC32 per combination of the full evaluation
+    achieved = combos * alg_popc / pairs_s
+    cpu = None if args.no_cpu_baseline else collect_reference_sample(G, c["sample_p"], c["keep"])
+    print(json.dumps({
+        "metric": COLLECT_METRIC, "value": value, "unit": "combos/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic", "config": config,
+        "rows": int(rows.shape[0]), "combos_per_step": combos,
+        "roofline": {"bound": "int-pipe (POPC on the XU pipe)", "kernel": "collect_pairs_kernel",
+                     "achieved": achieved / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc32/s",
+                     "frac": achieved / popc_peak, "traffic": None,
+                     "numerator": f"combinations/s of the pair sweeps x {alg_popc} POPC32 of "
+                                  "the full evaluation (2 per 64-bit word); the kernel issues "
+                                  f"{st.probe_words} per pair on its probe words",
+                     "kernel_frac": combos * st.probe_words / pairs_s / popc_peak,
+                     "peak_source": "measured: qsfb_microbench POPC chains over all SMs",
+                     "pass_rate": passes / max(combos * args.steps, 1),
+                     "gen_ms": st.gen_ms, "pairs_ms": st.pairs_ms},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "combos/s", "h2d_bytes_per_step": int(G.size),
+                "d2h_bytes_per_step": int(st.hits * S64 * 8),
+                "seconds_per_step": wall_s / args.steps},
+        "gpu_launches": launches, "clocks": clk.summary(),
+        "hits_per_step": hits // max(args.steps, 1)}), flush=True)
 
 
 def tc_traffic_per_launch(tc_cw_per_step):

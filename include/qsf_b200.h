@@ -279,6 +279,55 @@ int qsfb_flush_l2(void);
 const char* qsfb_device_name(void);
 int qsfb_device_sms(void);
 
+/* ---------------------------------------------------------------- Part 3: codeaut collector
+ * The Brouwer-Zimmermann low-weight collector of the reference's codeaut engine, with the
+ * handle ABI of cpp/codeaut/capi.h:51-72 that its Python (python/qubitserf/codeaut/
+ * lowweight.py:53-78) binds with ctypes.  Every sw-subset (sw = 1..min(p, m)) of the rows
+ * of the m x n 0/1 matrix G is XORed on the GPU; the distinct results of weight 1..keep
+ * come back sorted by their packed 64-bit words, word 0 first (bit j of word w is column
+ * 64 w + j), as the reference's handle holds them.  backend 0 ("cpu") is not run here: the
+ * handle comes back with ok = 0; 1 and 2 run on the GPU.  threads is ignored.  Sizes beyond
+ * n <= 1024, m <= 4096 and min(p, m) <= 64, or subset lists beyond device memory, also give
+ * ok = 0.  The Leon automorphism engine (qaut_leon_*) of the same header is not part of this
+ * library. */
+
+/* Replaces codeaut_bz_collect, cpp/codeaut/capi.h:57-59.  Never NULL unless host memory
+ * runs out; release with codeaut_bz_free. */
+void* codeaut_bz_collect(const uint8_t* G, int32_t m, int32_t n, int32_t p,
+                         int32_t keep_weight, int32_t backend, int32_t threads);
+/* Replace codeaut_bz_ok / _count / _combos / _copy_rows / _backend / _free,
+ * cpp/codeaut/capi.h:60-65. */
+int32_t codeaut_bz_ok(void* h);
+int64_t codeaut_bz_count(void* h);
+int64_t codeaut_bz_combos(void* h);
+void codeaut_bz_copy_rows(void* h, uint8_t* buf);
+const char* codeaut_bz_backend(void* h);
+void codeaut_bz_free(void* h);
+/* Replaces codeaut_backend_available, cpp/codeaut/capi.h:68: "gpu"/"cuda"/"auto" -> 1 when
+ * an sm_100 device is usable, anything else 0. */
+int32_t codeaut_backend_available(const char* name);
+/* Replaces codeaut_version, cpp/codeaut/capi.h:69. */
+const char* codeaut_version(void);
+
+/* No counterpart in the reference: what a collect handle's run did.  combos as
+ * codeaut_bz_combos; hits = appended codewords before deduplication; passes = pairs whose
+ * lower bound sent them to the exact evaluation; device times of the list generation and
+ * of the pair sweeps (the last pass when an overflow made the sweep run twice). */
+typedef struct {
+    int64_t combos;
+    int64_t hits;
+    int64_t passes;
+    int32_t probe_words;   /* 32-bit probe words per subset (1, 2, 4 or 8) */
+    int32_t pivots;        /* rows that own a private column */
+    int32_t launches;
+    int32_t reruns;        /* sweeps repeated after the output buffer overflowed */
+    double gen_ms;
+    double pairs_ms;
+    double seconds;        /* wall time of codeaut_bz_collect */
+    int32_t status;        /* 0, or the code of parts 1-2 that made ok = 0 */
+} QsfbCollectStats;
+int qsfb_collect_stats(void* h, QsfbCollectStats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,14 @@ class QsfbServeStats(ctypes.Structure):
                 ("elapsed_s", ctypes.c_double)]
 
 
+class QsfbCollectStats(ctypes.Structure):
+    _fields_ = [("combos", ctypes.c_int64), ("hits", ctypes.c_int64), ("passes", ctypes.c_int64),
+                ("probe_words", ctypes.c_int32), ("pivots", ctypes.c_int32),
+                ("launches", ctypes.c_int32), ("reruns", ctypes.c_int32),
+                ("gen_ms", ctypes.c_double), ("pairs_ms", ctypes.c_double),
+                ("seconds", ctypes.c_double), ("status", ctypes.c_int32)]
+
+
 # (name, restype, argtypes) of every exported function; tests check the export list.
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -139,6 +147,18 @@ SIGNATURES = [
     ("qsfb_tc_selftest", _i, [_i, _i, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
+    ("codeaut_bz_collect", ctypes.c_void_p, [_u8p, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32]),
+    ("codeaut_bz_ok", ctypes.c_int32, [ctypes.c_void_p]),
+    ("codeaut_bz_count", ctypes.c_int64, [ctypes.c_void_p]),
+    ("codeaut_bz_combos", ctypes.c_int64, [ctypes.c_void_p]),
+    ("codeaut_bz_copy_rows", None, [ctypes.c_void_p, _u8p]),
+    ("codeaut_bz_backend", _s, [ctypes.c_void_p]),
+    ("codeaut_bz_free", None, [ctypes.c_void_p]),
+    ("codeaut_backend_available", ctypes.c_int32, [_s]),
+    ("codeaut_version", _s, []),
+    ("qsfb_collect_stats", _i, [ctypes.c_void_p, ctypes.POINTER(QsfbCollectStats)]),
 ]
 
 _lib = None
@@ -483,3 +503,38 @@ def tc_selftest(ksteps, A, B, packed=False):
     _check(lib().qsfb_tc_selftest(int(ksteps), int(bool(packed)), A.ctypes.data, B.ctypes.data,
                                   D.ctypes.data), "qsfb_tc_selftest")
     return D
+
+
+_COLLECT_BACKEND = {"cpu": 0, "gpu": 1, "auto": 2}
+
+
+def collect(G, p, keep_weight, backend="gpu", threads=0, stats=False):
+    """Every distinct codeword of weight 1..keep_weight that is the XOR of a size-1..p subset
+    of the rows of G, as the reference's ``_collect_one_native`` returns them
+    (python/qubitserf/codeaut/lowweight.py:53-78): ``(rows uint8[count, n], combos)``, rows
+    sorted by their packed 64-bit words.  Raises RuntimeError when the handle is not ok
+    (backend "cpu", sizes beyond the engine's, no device).  stats=True appends the
+    QsfbCollectStats of the run."""
+    L = lib()
+    G = as_u8(G)
+    m, n = G.shape
+    be = _COLLECT_BACKEND.get(backend, backend)
+    h = L.codeaut_bz_collect(_p(G) if G.size else None, m, n, int(p), int(keep_weight),
+                             int(be), int(threads))
+    if not h:
+        raise RuntimeError("codeaut_bz_collect failed (no handle)")
+    try:
+        st = QsfbCollectStats()
+        L.qsfb_collect_stats(h, ctypes.byref(st))
+        if not L.codeaut_bz_ok(h):
+            raise RuntimeError(f"codeaut_bz_collect failed (rc={st.status}: "
+                               f"{ERRORS.get(st.status, 'error')})")
+        cnt = int(L.codeaut_bz_count(h))
+        combos = int(L.codeaut_bz_combos(h))
+        rows = np.zeros((max(cnt, 1), n), dtype=np.uint8)
+        if cnt:
+            L.codeaut_bz_copy_rows(h, _p(rows))
+        rows = rows[:cnt]
+    finally:
+        L.codeaut_bz_free(h)
+    return (rows, combos, st) if stats else (rows, combos)

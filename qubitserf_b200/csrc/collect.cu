@@ -1,0 +1,251 @@
+// sm_100a kernels of the low-weight collector (the codeaut_bz_* boundary): list generation
+// and the pair sweep that appends every subset XOR of weight 1..keep.
+//
+// Semantics kept from the reference (cpp/codeaut/bz.cpp:82-97 and the CollectSink of
+// cpp/qsf/enum_core.hpp:90-103): for every subset size sw the XOR of every sw-subset of the
+// generator's rows is a hit when its full Hamming weight lies in [1, keep]; duplicates are
+// allowed here and removed by the host.  The traversal is this engine's own
+// (collect_types.hpp): prefix/suffix lists of probe words and pivot counts, swept as
+// rectangles of pairs with the prefix entries in registers and the suffix entries
+// broadcast to the warp.
+//
+// The sweep is bound by the POPC (XU) pipe: per pair HP XORs, HP POPCs and an add give the
+// lower bound pivots + popc(probe); a three-input minimum folds eight of them per suffix
+// entry and only a minimum under keep + 1 sends the lane to the exact path, which unranks
+// both subsets, XORs their full rows and appends the codeword when its weight is in range.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "collect_types.hpp"
+#include "engine_types.hpp"
+#include "enum_device.cuh"
+
+namespace qsfb {
+namespace dev {
+
+constexpr int kCRX = kCollectTileX / 32;   // prefix entries per lane
+constexpr int kCFar = 1 << 20;             // pivot count of an empty register slot
+static_assert(kCRX == 8, "the minimum fold below takes eight register entries");
+
+// ---------------------------------------------------------------- list generation
+// One thread per run of kGenRun consecutive entries of a list: the first entry is unranked
+// over the binomial table, the next follow by the colex successor (the rows that leave and
+// enter change the XOR; usually one of each).
+__global__ void __launch_bounds__(256) collect_gen_kernel(const CollectListDesc* __restrict__ lists,
+                                                          int nlists, unsigned long long runs,
+                                                          CollectShared S,
+                                                          const unsigned long long* __restrict__ B) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long gr = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         gr < runs; gr += stride) {
+        int lo = 0, hi = nlists - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (lists[mid].run_base <= gr) lo = mid; else hi = mid - 1;
+        }
+        const CollectListDesc& D = lists[lo];
+        const unsigned long long e0 = (gr - D.run_base) * kGenRun;
+        const int n = (int)(D.count - e0 < (unsigned long long)kGenRun ? D.count - e0 : kGenRun);
+        const int s = D.size;
+        int c[kCollectMaxSize], top[kCollectMaxSize];
+        colex_unrank(B, e0, s, S.m, top);   // largest first
+        for (int i = 0; i < s; ++i) c[i] = top[s - 1 - i];
+        auto row_of = [&](int v) { return D.reflect ? S.m - 1 - v : v; };
+        uint32_t acc[kCollectMaxProbe];
+#pragma unroll
+        for (int h = 0; h < kCollectMaxProbe; ++h) acc[h] = 0u;
+        auto xor_row = [&](int r) {
+            const uint32_t* p = S.probe_rows + (size_t)r * S.HP;
+#pragma unroll
+            for (int h = 0; h < kCollectMaxProbe; ++h)
+                if (h < S.HP) acc[h] ^= __ldg(p + h);
+        };
+        int pc = 0;
+        for (int i = 0; i < s; ++i) {
+            const int r = row_of(c[i]);
+            xor_row(r);
+            pc += __ldg(S.piv + r);
+        }
+        for (int j = 0; j < n; ++j) {
+            const unsigned long long e = e0 + j;
+            uint32_t* o = D.probe + e * (unsigned long long)S.HP;
+#pragma unroll
+            for (int h = 0; h < kCollectMaxProbe; ++h)
+                if (h < S.HP) o[h] = acc[h];
+            D.pc[e] = (uint8_t)pc;
+            if (j + 1 == n) break;
+            // colex successor: lowest t with c[t] + 1 < c[t+1] (c[s] = m)
+            int t = 0;
+            while (t < s - 1 && c[t] + 1 == c[t + 1]) ++t;
+            for (int i = 0; i <= t; ++i) {
+                const int r_old = row_of(c[i]);
+                xor_row(r_old);
+                pc -= __ldg(S.piv + r_old);
+                c[i] = i < t ? i : c[i] + 1;
+                const int r_new = row_of(c[i]);
+                xor_row(r_new);
+                pc += __ldg(S.piv + r_new);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- pair sweep
+template <int HP>
+__device__ __forceinline__ void load_probe(const uint32_t* __restrict__ p, uint32_t (&v)[HP]) {
+    if constexpr (HP == 8) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
+        const uint4 b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else if constexpr (HP == 4) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else if constexpr (HP == 2) {
+        const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
+        v[0] = a.x; v[1] = a.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+
+template <int HP>
+__device__ __forceinline__ int probe_weight(const uint32_t (&x)[HP], const uint32_t (&y)[HP]) {
+    int s = 0;
+#pragma unroll
+    for (int h = 0; h < HP; ++h) s += __popc(x[h] ^ y[h]);
+    return s;
+}
+
+// Exact evaluation of the pair (prefix entry ex, suffix entry ey): both subsets unranked,
+// their full rows XORed, the codeword appended when its weight is in [1, keep].  The slot
+// counter keeps counting past the capacity so that the host learns the exact hit count.
+static __device__ __noinline__ void collect_exact(const CollectShared& S,
+                                                  const CollectLevelDesc& L,
+                                                  const unsigned long long* __restrict__ B,
+                                                  unsigned long long ex,
+                                                  unsigned long long ey) {
+    int c[kCollectMaxSize];
+    unsigned long long acc[kCollectMaxWords];
+#pragma unroll
+    for (int w = 0; w < kCollectMaxWords; ++w) acc[w] = 0ull;
+    auto xor_row = [&](int r) {
+        const unsigned long long* p = S.rows + (size_t)r * S.S64;
+#pragma unroll
+        for (int w = 0; w < kCollectMaxWords; ++w)
+            if (w < S.S64) acc[w] ^= __ldg(p + w);
+    };
+    colex_unrank(B, ex, L.a, S.m, c);
+    for (int i = 0; i < L.a; ++i) xor_row(c[i]);
+    colex_unrank(B, ey, L.b, S.m, c);
+    for (int i = 0; i < L.b; ++i) xor_row(S.m - 1 - c[i]);
+    int wt = 0;
+#pragma unroll
+    for (int w = 0; w < kCollectMaxWords; ++w)
+        if (w < S.S64) wt += __popcll(acc[w]);
+    if (wt < 1 || wt > S.keep) return;
+    const unsigned long long slot = atomicAdd(S.ctr, 1ull);
+    if (slot >= S.cap) return;
+    unsigned long long* o = S.out + slot * (unsigned long long)S.S64;
+#pragma unroll
+    for (int w = 0; w < kCollectMaxWords; ++w)
+        if (w < S.S64) o[w] = acc[w];
+}
+
+// One warp per job (a 256-entry prefix tile of one term against up to kCollectChunkY
+// suffix entries), jobs handed out by a per-level counter.
+template <int HP>
+__global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDesc* __restrict__ levels,
+                                                            int level, CollectShared S,
+                                                            const unsigned long long* __restrict__ B) {
+    const CollectLevelDesc& L = levels[level];
+    const int lane = threadIdx.x & 31;
+    unsigned long long passes = 0;
+    for (;;) {
+        unsigned long long job = 0;
+        if (lane == 0) job = atomicAdd(S.job_ctr + level, 1ull);
+        job = __shfl_sync(0xffffffffu, job, 0);
+        if (job >= L.jobs) break;
+        int lo = 0, hi = L.nterms - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (L.terms[mid].job_base <= job) lo = mid; else hi = mid - 1;
+        }
+        const CollectTerm& T = L.terms[lo];
+        const unsigned long long j = job - T.job_base;
+        const unsigned long long xt = j / T.ychunks, yc = j - xt * T.ychunks;
+        const unsigned long long xoff = xt * kCollectTileX;
+        uint32_t xv[kCRX][HP];
+        int xpc[kCRX];
+#pragma unroll
+        for (int i = 0; i < kCRX; ++i) {
+            const unsigned long long xo = xoff + (unsigned long long)(i * 32 + lane);
+            if (xo < T.nx) {
+                const unsigned long long e = T.x0 + xo;
+                load_probe<HP>(L.xp + e * HP, xv[i]);
+                xpc[i] = __ldg(L.xpc + e);
+            } else {
+#pragma unroll
+                for (int h = 0; h < HP; ++h) xv[i][h] = 0u;
+                xpc[i] = kCFar;
+            }
+        }
+        const unsigned long long y0 = yc * kCollectChunkY;
+        const unsigned long long y1 = T.ny < y0 + kCollectChunkY ? T.ny : y0 + kCollectChunkY;
+        const int lim = S.keep;
+        for (unsigned long long y = y0; y < y1; ++y) {
+            uint32_t yv[HP];
+            load_probe<HP>(L.yp + y * HP, yv);
+            const int ypc = __ldg(L.ypc + y);
+            int v[kCRX];
+#pragma unroll
+            for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_weight<HP>(xv[i], yv);
+            int mn = __vimin3_s32(v[0], v[1], v[2]);
+            mn = __vimin3_s32(mn, v[3], v[4]);
+            mn = __vimin3_s32(mn, v[5], v[6]);
+            mn = min(mn, v[7]);
+            if (mn + ypc <= lim) {
+#pragma unroll 1
+                for (int i = 0; i < kCRX; ++i) {
+                    if (v[i] + ypc > lim) continue;
+                    ++passes;
+                    collect_exact(S, L, B, T.x0 + xoff + (unsigned long long)(i * 32 + lane), y);
+                }
+            }
+        }
+    }
+    if (passes) atomicAdd(S.ctr + 1, passes);
+}
+
+}  // namespace dev
+
+cudaError_t launch_collect_gen(const CollectListDesc* d_lists, int nlists, unsigned long long runs,
+                               const CollectShared& S, const unsigned long long* d_binom,
+                               int num_sms, cudaStream_t st) {
+    if (runs == 0) return cudaSuccess;
+    const unsigned long long want = (runs + 255) / 256;
+    const unsigned long long cap = (unsigned long long)num_sms * 8;
+    const unsigned int grid = (unsigned int)(want < cap ? want : cap);
+    dev::collect_gen_kernel<<<grid, 256, 0, st>>>(d_lists, nlists, runs, S, d_binom);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_collect_pairs(const CollectLevelDesc* d_levels, int level,
+                                 unsigned long long jobs, const CollectShared& S,
+                                 const unsigned long long* d_binom, int num_sms,
+                                 cudaStream_t st) {
+    if (jobs == 0) return cudaSuccess;
+    const unsigned long long want = (jobs + 3) / 4;   // four warps per block
+    const unsigned long long cap = (unsigned long long)num_sms * 8;
+    const unsigned int grid = (unsigned int)(want < cap ? want : cap);
+    switch (S.HP) {
+        case 1: dev::collect_pairs_kernel<1><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
+        case 2: dev::collect_pairs_kernel<2><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
+        case 4: dev::collect_pairs_kernel<4><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
+        case 8: dev::collect_pairs_kernel<8><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace qsfb

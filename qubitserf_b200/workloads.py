@@ -189,3 +189,13 @@ def serving_stream(rate: float, num: int = 20000, seed: int = 4, pool: int = 256
             x = rng.integers(0, 2, n, dtype=np.uint8)
             reqs.append(Request(t, "opweight", (Hx, Hz, z, x), n))
     return reqs
+
+
+def collect_generator(n: int = 128, k: int = 64, seed: int = 13):
+    """Input of the low-weight collector benchmark: a random k x n generator in systematic
+    form on a random column set, as the reference's codeaut layer hands its information-set
+    generators to codeaut_bz_collect (python/qubitserf/codeaut/lowweight.py:117-126)."""
+    rng = np.random.default_rng(seed)
+    A = rng.integers(0, 2, size=(k, n - k), dtype=np.uint8)
+    G = np.concatenate([np.eye(k, dtype=np.uint8), A], axis=1)
+    return np.ascontiguousarray(G[:, rng.permutation(n)])

@@ -10,6 +10,12 @@ Runs only where the reference CPU library has been built from its sources
 
     python tests/golden/make_golden.py              # golden.npz + golden.json
     python tests/golden/make_golden.py --batch1024  # batch1024.json (all 1024 batch codes)
+    python tests/golden/make_golden.py --collect    # collect.npz (codeaut low-weight collector)
+
+* collect.npz  -- per case `<name>__G` (the generator rows), `<name>__meta` (p, keep, combos,
+                  count, n) and `<name>__rows` (the reference's collected rows, bit-packed
+                  with numpy.packbits along each row), from the reference's own
+                  codeaut_bz_collect on its CPU backend (cpp/codeaut/bz.cpp:55-117)
 """
 from __future__ import annotations
 
@@ -153,10 +159,65 @@ def batch1024():
     (HERE / "batch1024.json").write_text(json.dumps({"meta": meta, "codes": out}))
 
 
+def systematic(rng, k, n):
+    """A random full-rank k x n generator in systematic form on a random column set."""
+    while True:
+        A = rng.integers(0, 2, size=(k, n - k), dtype=np.uint8)
+        G = np.concatenate([np.eye(k, dtype=np.uint8), A], axis=1)
+        return G[:, rng.permutation(n)]
+
+
+def collect_cases():
+    """(name, G, p, keep) of the collector's golden cases."""
+    rng = np.random.default_rng(11)
+    out = []
+    H = C.hamming_parity(3)                      # [7,4] Hamming: generator = kernel of H
+    G7 = np.array([[1, 0, 0, 0, 0, 1, 1], [0, 1, 0, 0, 1, 0, 1], [0, 0, 1, 0, 1, 1, 0],
+                   [0, 0, 0, 1, 1, 1, 1]], np.uint8)
+    assert not ((G7 @ H.T) % 2).any()
+    out.append(("hamming7", G7, 4, 7))
+    out.append(("rm_1_5", C.reed_muller_generator(1, 5), 6, 16))
+    out.append(("rm_2_5", C.reed_muller_generator(2, 5), 4, 8))
+    out.append(("rm_1_6", C.reed_muller_generator(1, 6), 7, 32))
+    out.append(("rep_11", np.ones((1, 11), np.uint8), 3, 11))
+    out.append(("sys_40_20", systematic(rng, 20, 40), 4, 10))
+    out.append(("sys_96_32", systematic(rng, 32, 96), 4, 24))
+    out.append(("sys_130_24", systematic(rng, 24, 130), 3, 50))
+    out.append(("sys_200_40", systematic(rng, 40, 200), 3, 80))
+    G = rng.integers(0, 2, size=(12, 70), dtype=np.uint8)
+    G[3] = 0
+    G[7] = G[2]
+    G[9] = G[0] ^ G[1]
+    out.append(("dependent_12_70", G, 5, 30))
+    out.append(("dense_10_64", rng.integers(0, 2, size=(10, 64), dtype=np.uint8), 10, 64))
+    out.append(("keep0", systematic(rng, 8, 20), 3, 0))
+    out.append(("p_over_m", systematic(rng, 5, 17), 9, 9))
+    out.append(("one_col", rng.integers(0, 2, size=(6, 1), dtype=np.uint8), 3, 1))
+    return out
+
+
+def collect_goldens():
+    from oracle.refbind import Ref
+    ref = Ref()
+    arrays = {}
+    for name, G, p, keep in collect_cases():
+        rows, combos = ref.collect(G, p, keep)
+        arrays[f"{name}__G"] = np.asarray(G, np.uint8)
+        arrays[f"{name}__meta"] = np.array([p, keep, combos, rows.shape[0], G.shape[1]],
+                                           dtype=np.int64)
+        arrays[f"{name}__rows"] = np.packbits(rows, axis=1) if rows.size else \
+            np.zeros((0, (G.shape[1] + 7) // 8), np.uint8)
+        print(name, G.shape, p, keep, "->", rows.shape[0], "rows,", combos, "combos", flush=True)
+    np.savez_compressed(HERE / "collect.npz", **arrays)
+
+
 def main():
     sys.path.insert(0, str(ROOT))
     if "--batch1024" in sys.argv:
         batch1024()
+        return
+    if "--collect" in sys.argv:
+        collect_goldens()
         return
     arrays = {}
     results = {}

@@ -18,7 +18,7 @@ from conftest import ROOT
 def header_functions():
     text = (ROOT / "include" / "qsf_b200.h").read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(distfind_\w+|qsfb_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(distfind_\w+|qsfb_\w+|codeaut_\w+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol(native):
@@ -41,6 +41,47 @@ def test_struct_layouts_match_reference_abi(native):
     assert native.DistfindResult.seconds.offset == 16
     assert ctypes.sizeof(native.DistfindOpResult) == 3 * 4 + 4 + 8 + 16
     assert native.DistfindOpResult.seconds.offset == 16
+
+
+def _collect_handle(native, G, m, n, p, keep, backend):
+    L = native.lib()
+    ptr = native._p(G) if G is not None else None
+    h = L.codeaut_bz_collect(ptr, m, n, p, keep, backend, 0)
+    assert h
+    try:
+        st = native.QsfbCollectStats()
+        assert L.qsfb_collect_stats(h, ctypes.byref(st)) == 0
+        return (L.codeaut_bz_ok(h), L.codeaut_bz_count(h), L.codeaut_bz_combos(h),
+                L.codeaut_bz_backend(h), st.status)
+    finally:
+        L.codeaut_bz_free(h)
+
+
+def test_collect_handle_rules_without_device_work(native):
+    """The codeaut_bz_* handle answers these before any device work, as the reference's
+    does (cpp/codeaut/bz.cpp:55-97, capi.cpp): empty problems are complete with nothing
+    collected and no backend named; a nonpositive keep collects nothing but still counts
+    every combination (saturating per level at 2^62); backend 0 (cpu) is not run here."""
+    G = np.ones((3, 5), np.uint8)
+    assert _collect_handle(native, G, 0, 5, 3, 4, 1) == (1, 0, 0, b"", 0)
+    assert _collect_handle(native, G, 3, 0, 3, 4, 1) == (1, 0, 0, b"", 0)
+    assert _collect_handle(native, G, 3, 5, 0, 4, 1) == (1, 0, 0, b"", 0)
+    assert _collect_handle(native, None, 3, 5, 2, 4, 1)[0] == 0          # null G
+    ok, cnt, combos, be, status = _collect_handle(native, G, 3, 5, 2, 4, 0)
+    assert (ok, cnt, status) == (0, 0, 5)
+    G2 = np.zeros((40, 9), np.uint8)
+    ok, cnt, combos, be, status = _collect_handle(native, G2, 40, 9, 6, 0, 1)
+    assert (ok, cnt, be, status) == (1, 0, b"cuda", 0)
+    assert combos == sum(__import__("math").comb(40, s) for s in range(1, 7))
+    # p > m: subset sizes stop at m
+    ok, cnt, combos, _, _ = _collect_handle(native, G2[:4], 4, 9, 9, -3, 2)
+    assert (ok, combos) == (1, 15)
+    # C(4000, 30) > 2^62 for every size from 10 up: each level adds the cap, the sum saturates
+    G3 = np.zeros((4000, 2), np.uint8)
+    ok, _, combos, _, _ = _collect_handle(native, G3, 4000, 2, 30, 0, 1)
+    assert (ok, combos) == (1, 1 << 62)
+    assert native.lib().codeaut_backend_available(b"cpu") == 0
+    assert native.lib().codeaut_version() == b"0.1.0"
 
 
 def test_version(native):

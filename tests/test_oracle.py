@@ -122,3 +122,46 @@ def test_oracle_problem_ranks_match_reference(orc, ref, golden):
         b = ref.problem_gammas(kind, *mats)
         assert a["ranks"] == b["ranks"] and a["K"] == b["K"], name
         assert a["seed_upper"] == b["seed_upper"] and a["even"] == b["even"], name
+
+
+def load_collect_goldens():
+    """(name, G, p, keep, combos, rows) of tests/golden/collect.npz (made by the reference's
+    own codeaut_bz_collect, tests/golden/make_golden.py --collect)."""
+    from conftest import GOLDEN_DIR
+    z = np.load(GOLDEN_DIR / "collect.npz")
+    names = sorted({k.split("__")[0] for k in z.files})
+    out = []
+    for nm in names:
+        p, keep, combos, count, n = (int(v) for v in z[f"{nm}__meta"])
+        rows = np.unpackbits(z[f"{nm}__rows"], axis=1)[:, :n] if count else \
+            np.zeros((0, n), np.uint8)
+        out.append((nm, z[f"{nm}__G"], p, keep, combos, rows))
+    return out
+
+
+def test_collect_oracle_matches_golden(orc):
+    cases = load_collect_goldens()
+    assert len(cases) >= 12
+    for name, G, p, keep, combos, rows in cases:
+        got, got_combos = orc.collect(G, p, keep)
+        assert got_combos == combos, name
+        assert np.array_equal(got, rows), name
+
+
+def test_collect_oracle_matches_reference_random(orc, ref):
+    if ref is None:
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(21)
+    for trial in range(40):
+        m = int(rng.integers(1, 18))
+        n = int(rng.integers(1, 200))
+        p = int(rng.integers(1, 7))
+        keep = int(rng.integers(-2, n // 2 + 3))
+        G = rng.integers(0, 2, size=(m, n), dtype=np.uint8)
+        if trial % 4 == 0:
+            G[:, : min(m, n)] = np.eye(m, dtype=np.uint8)[:, : min(m, n)]
+        if trial % 5 == 0:
+            G[rng.integers(0, m)] = 0
+        a, ca = ref.collect(G, p, keep)
+        b, cb = orc.collect(G, p, keep)
+        assert ca == cb and np.array_equal(a, b), (trial, m, n, p, keep)
