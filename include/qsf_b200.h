@@ -318,6 +318,8 @@ typedef struct {
     int64_t hits;
     int64_t passes;
     int32_t probe_words;   /* 32-bit probe words per subset (1, 2, 4 or 8) */
+    int32_t filter;        /* lower bound on their popcount: 0 exact sum, 2 / 4 popc of the
+                              OR of 2 / 4 words, 6 carry-save over four words */
     int32_t pivots;        /* rows that own a private column */
     int32_t launches;
     int32_t reruns;        /* sweeps repeated after the output buffer overflowed */

@@ -94,7 +94,8 @@ class QsfbServeStats(ctypes.Structure):
 
 class QsfbCollectStats(ctypes.Structure):
     _fields_ = [("combos", ctypes.c_int64), ("hits", ctypes.c_int64), ("passes", ctypes.c_int64),
-                ("probe_words", ctypes.c_int32), ("pivots", ctypes.c_int32),
+                ("probe_words", ctypes.c_int32), ("filter", ctypes.c_int32),
+                ("pivots", ctypes.c_int32),
                 ("launches", ctypes.c_int32), ("reruns", ctypes.c_int32),
                 ("gen_ms", ctypes.c_double), ("pairs_ms", ctypes.c_double),
                 ("seconds", ctypes.c_double), ("status", ctypes.c_int32)]

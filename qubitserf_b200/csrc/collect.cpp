@@ -24,6 +24,7 @@
 
 #include "collect_types.hpp"
 #include "engine.hpp"
+#include "filter_plan.hpp"
 
 namespace qsfb {
 
@@ -71,21 +72,32 @@ double binom_cdf_half(int bits, int t) {
     return std::min(acc, 1.0);
 }
 
-// Probe width: the fewest words whose expected cost per pair (HP POPCs, plus ~256 POPCs of
-// exact evaluation for every pair that passes) is least; QSFB_COLLECT_HP forces a width.
-int choose_probe(int n_np, int t) {
-    if (const char* e = std::getenv("QSFB_COLLECT_HP")) {
-        const int f = std::atoi(e);
-        if (f == 1 || f == 2 || f == 4 || f == 8) return f;
-    }
+// Probe variant (width HP, bound FILT of collect.cu's probe_bound): the least expected cost
+// per pair in POPC-pipe cycles, max(POPCs, other integer ops / 4) (the ALU pipe issues four
+// times the POPC rate), plus ~256 for every pair that passes to the exact evaluation, at
+// the fair-coin pass rates of filter_plan.cpp.  QSFB_COLLECT_HP / QSFB_COLLECT_FILT force
+// a width / bound (tests cover every variant this way).
+struct ProbeVariant { int hp, filt; };
+
+ProbeVariant choose_probe(int n_np, int t) {
+    struct Cand { int hp, filt; double popc, alu; };
+    const Cand cands[7] = {{1, 0, 1, 2.5}, {2, 0, 2, 4.5}, {2, 2, 1, 3.5}, {4, 0, 4, 8.5},
+                           {4, 4, 1, 5.5}, {4, 6, 2, 11.5}, {8, 0, 8, 16.5}};
+    int force_hp = 0, force_f = -1;
+    if (const char* e = std::getenv("QSFB_COLLECT_HP")) force_hp = std::atoi(e);
+    if (const char* e = std::getenv("QSFB_COLLECT_FILT")) force_f = std::atoi(e);
     const int need = std::max(1, (n_np + 31) / 32);
-    int best = 1;
+    ProbeVariant best{1, 0};
     double best_cost = 1e300;
-    for (int hp : {1, 2, 4, 8}) {
-        const int bits = std::min(32 * hp, n_np);
-        const double cost = hp + 256.0 * binom_cdf_half(bits, t);
-        if (cost < best_cost) { best_cost = cost; best = hp; }
-        if (hp >= need) break;   // wider probes only add zero words
+    for (const Cand& c : cands) {
+        if (force_hp > 0 && c.hp != force_hp) continue;
+        if (force_f >= 0 && c.filt != force_f) continue;
+        // wider probes than the non-private columns only add zero words
+        if (force_hp <= 0 && c.hp > 1 && c.hp / 2 >= need) continue;
+        const double pass = c.filt == 0 ? binom_cdf_half(std::min(32 * c.hp, n_np), t)
+                                        : filter_pass_rate(c.filt, n_np, t);
+        const double cost = std::max(c.popc, c.alu / 4.0) + 256.0 * pass;
+        if (cost < best_cost) { best_cost = cost; best = {c.hp, c.filt}; }
     }
     return best;
 }
@@ -174,13 +186,15 @@ int run_collect(const uint8_t* G, int m, int n, int p, int keep, CollectHandle* 
     const int n_np = (int)np_cols.size();
     // threshold on the probe weight of the heaviest level's pairs (their fewest pivots)
     const int t = keep - std::max(0, maxsw - (m - npiv));
-    const int HP = choose_probe(n_np, t);
+    const ProbeVariant pv = choose_probe(n_np, t);
+    const int HP = pv.hp;
     std::vector<uint32_t> probe_rows((size_t)m * HP, 0u);
     for (int r = 0; r < m; ++r)
         for (int b = 0; b < 32 * HP && b < n_np; ++b)
             if (G[(size_t)r * n + np_cols[b]] & 1)
                 probe_rows[(size_t)r * HP + (b >> 5)] |= 1u << (b & 31);
     H->st.probe_words = HP;
+    H->st.filter = pv.filt;
     H->st.pivots = npiv;
 
     // ---- lists: colex a-subsets (a = ceil(sw/2)) and reflected b-subsets (b = floor(sw/2))
@@ -298,7 +312,7 @@ int run_collect(const uint8_t* G, int m, int n, int p, int keep, CollectHandle* 
     S.rows = (const unsigned long long*)(d_static + o_rows);
     S.ctr = (unsigned long long*)(d_static + o_ctr);
     S.job_ctr = S.ctr + 2;
-    S.m = m; S.S64 = S64; S.HP = HP; S.keep = keep;
+    S.m = m; S.S64 = S64; S.HP = HP; S.keep = keep; S.filt = pv.filt;
     const CollectLevelDesc* d_levels = (const CollectLevelDesc*)(d_static + o_lv);
 
     SessionLease lease(dev);

@@ -9,10 +9,11 @@
 // rectangles of pairs with the prefix entries in registers and the suffix entries
 // broadcast to the warp.
 //
-// The sweep is bound by the POPC (XU) pipe: per pair HP XORs, HP POPCs and an add give the
-// lower bound pivots + popc(probe); a three-input minimum folds eight of them per suffix
-// entry and only a minimum under keep + 1 sends the lane to the exact path, which unranks
-// both subsets, XORs their full rows and appends the codeword when its weight is in range.
+// The sweep is bound by the POPC (XU) pipe: per pair a few XORs/ORs and one or two POPCs
+// give a lower bound on pivots + popc(probe) (probe_bound below); a three-input minimum
+// folds eight of them per suffix entry and only a minimum under keep + 1 sends the lane to
+// the exact path, which unranks both subsets, XORs their full rows and appends the
+// codeword when its weight is in range.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -109,12 +110,31 @@ __device__ __forceinline__ void load_probe(const uint32_t* __restrict__ p, uint3
     }
 }
 
-template <int HP>
-__device__ __forceinline__ int probe_weight(const uint32_t (&x)[HP], const uint32_t (&y)[HP]) {
-    int s = 0;
+// Lower bound on the probe weight of a pair (the popcount of the XORed probe words):
+//   FILT 0: the exact sum, HP POPCs;
+//   FILT 2 / 4: popc of the OR of the 2 / 4 XORed words, one POPC;
+//   FILT 6: carry-save over four words, popc(a^b^c^d) + 2 popc(maj(a,b,c) | (a^b^c)&d),
+//           exact except that a column set in all four counts 2 (two POPCs).
+template <int HP, int FILT>
+__device__ __forceinline__ int probe_bound(const uint32_t (&x)[HP], const uint32_t (&y)[HP]) {
+    if constexpr (FILT == 0) {
+        int s = 0;
 #pragma unroll
-    for (int h = 0; h < HP; ++h) s += __popc(x[h] ^ y[h]);
-    return s;
+        for (int h = 0; h < HP; ++h) s += __popc(x[h] ^ y[h]);
+        return s;
+    } else if constexpr (FILT == 2) {
+        static_assert(HP >= 2, "FILT 2 reads two probe words");
+        return __popc((x[0] ^ y[0]) | (x[1] ^ y[1]));
+    } else if constexpr (FILT == 4) {
+        static_assert(HP >= 4, "FILT 4 reads four probe words");
+        return __popc((x[0] ^ y[0]) | (x[1] ^ y[1]) | (x[2] ^ y[2]) | (x[3] ^ y[3]));
+    } else {
+        static_assert(FILT == 6 && HP >= 4, "FILT 6 reads four probe words");
+        const uint32_t a = x[0] ^ y[0], b = x[1] ^ y[1], c = x[2] ^ y[2], d = x[3] ^ y[3];
+        const uint32_t s3 = a ^ b ^ c;
+        const uint32_t carry = ((a & b) | (a & c) | (b & c)) | (s3 & d);
+        return __popc(s3 ^ d) + 2 * __popc(carry);
+    }
 }
 
 // Exact evaluation of the pair (prefix entry ex, suffix entry ey): both subsets unranked,
@@ -154,7 +174,7 @@ static __device__ __noinline__ void collect_exact(const CollectShared& S,
 
 // One warp per job (a 256-entry prefix tile of one term against up to kCollectChunkY
 // suffix entries), jobs handed out by a per-level counter.
-template <int HP>
+template <int HP, int FILT>
 __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDesc* __restrict__ levels,
                                                             int level, CollectShared S,
                                                             const unsigned long long* __restrict__ B) {
@@ -199,7 +219,7 @@ __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDe
             const int ypc = __ldg(L.ypc + y);
             int v[kCRX];
 #pragma unroll
-            for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_weight<HP>(xv[i], yv);
+            for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_bound<HP, FILT>(xv[i], yv);
             int mn = __vimin3_s32(v[0], v[1], v[2]);
             mn = __vimin3_s32(mn, v[3], v[4]);
             mn = __vimin3_s32(mn, v[5], v[6]);
@@ -238,13 +258,20 @@ cudaError_t launch_collect_pairs(const CollectLevelDesc* d_levels, int level,
     const unsigned long long want = (jobs + 3) / 4;   // four warps per block
     const unsigned long long cap = (unsigned long long)num_sms * 8;
     const unsigned int grid = (unsigned int)(want < cap ? want : cap);
-    switch (S.HP) {
-        case 1: dev::collect_pairs_kernel<1><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
-        case 2: dev::collect_pairs_kernel<2><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
-        case 4: dev::collect_pairs_kernel<4><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
-        case 8: dev::collect_pairs_kernel<8><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom); break;
-        default: return cudaErrorInvalidValue;
+#define QSFB_COLLECT_CASE(H, F)                                                              \
+    if (S.HP == H && S.filt == F) {                                                          \
+        dev::collect_pairs_kernel<H, F><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom);  \
+        return cudaGetLastError();                                                           \
     }
+    QSFB_COLLECT_CASE(1, 0)
+    QSFB_COLLECT_CASE(2, 0)
+    QSFB_COLLECT_CASE(2, 2)
+    QSFB_COLLECT_CASE(4, 0)
+    QSFB_COLLECT_CASE(4, 4)
+    QSFB_COLLECT_CASE(4, 6)
+    QSFB_COLLECT_CASE(8, 0)
+#undef QSFB_COLLECT_CASE
+    return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 

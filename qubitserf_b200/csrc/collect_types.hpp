@@ -67,6 +67,7 @@ struct CollectShared {
     unsigned long long* job_ctr;  // one dynamic job counter per level
     unsigned long long cap;
     int m, S64, HP, keep;
+    int filt;                     // probe_bound variant (collect.cu): 0 exact, 2/4 OR, 6 CSA
 };
 
 }  // namespace qsfb

@@ -22,15 +22,15 @@ def systematic(rng, k, n):
 
 
 @pytest.fixture
-def force_hp():
-    """Set QSFB_COLLECT_HP for one call (the library reads it on every call)."""
-    def set_hp(v):
-        if v is None:
-            os.environ.pop("QSFB_COLLECT_HP", None)
-        else:
-            os.environ["QSFB_COLLECT_HP"] = str(v)
-    yield set_hp
+def force_probe():
+    """Force the probe width and bound for the calls of one test (the library reads
+    QSFB_COLLECT_HP / QSFB_COLLECT_FILT on every call)."""
+    def set_probe(hp, filt):
+        os.environ["QSFB_COLLECT_HP"] = str(hp)
+        os.environ["QSFB_COLLECT_FILT"] = str(filt)
+    yield set_probe
     os.environ.pop("QSFB_COLLECT_HP", None)
+    os.environ.pop("QSFB_COLLECT_FILT", None)
 
 
 def test_collect_matches_reference_goldens(native):
@@ -40,10 +40,10 @@ def test_collect_matches_reference_goldens(native):
         assert np.array_equal(got, rows), name
 
 
-@pytest.mark.parametrize("hp", [1, 2, 4, 8])
-def test_collect_every_probe_width_equals_oracle(native, orc, force_hp, hp):
-    rng = np.random.default_rng(100 + hp)
-    force_hp(hp)
+@pytest.mark.parametrize("hp,filt", [(1, 0), (2, 0), (2, 2), (4, 0), (4, 4), (4, 6), (8, 0)])
+def test_collect_every_probe_variant_equals_oracle(native, orc, force_probe, hp, filt):
+    rng = np.random.default_rng(100 + 10 * hp + filt)
+    force_probe(hp, filt)
     for trial in range(12):
         m = int(rng.integers(1, 26))
         n = int(rng.integers(1, 300))
@@ -55,7 +55,7 @@ def test_collect_every_probe_width_equals_oracle(native, orc, force_hp, hp):
         if trial % 5 == 0:
             G[rng.integers(0, m)] = 0
         got, combos, st = native.collect(G, p, keep, stats=True)
-        assert st.probe_words == hp
+        assert (st.probe_words, st.filter) == (hp, filt)
         want, want_combos = orc.collect(G, p, keep)
         assert combos == want_combos
         assert np.array_equal(got, want), (trial, m, n, p, keep)
