@@ -177,7 +177,7 @@ def main():
     ap.add_argument("--only-resident", action="store_true",
                     help="time only the resident-input rounds (profiling runs)")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "css128", "classical128", "classical96", "collect"],
+                    choices=["batch", "css128", "classical128", "classical96", "collect", "mitm"],
                     help="batch = the 1024-code batch; collect = the codeaut low-weight "
                          "collector; the others certify one code")
     args = ap.parse_args()
@@ -185,6 +185,9 @@ def main():
     rank, world, local, pg = dist_setup(args.gpus)
     if args.workload == "collect":
         bench_collect(args, rank, world, local, pg)
+        return
+    if args.workload == "mitm":
+        bench_mitm(args, rank, world, local, pg)
         return
     from qubitserf_b200 import workloads as W
     if args.workload == "batch":
@@ -478,6 +481,77 @@ def bench_collect(args, rank, world, local, pg):
                 "seconds_per_step": wall_s / args.steps},
         "gpu_launches": launches, "clocks": clk.summary(),
         "hits_per_step": hits // max(args.steps, 1)}), flush=True)
+
+
+MITM_L = 7
+MITM_METRIC = "method mitm: certificates/s (exact CSS min distance) on 1 B200"
+
+
+def bench_mitm(args, rank, world, local, pg):
+    """Method "mitm" (meet in the middle) on the [[98, 2, 7]] toric code, which='min': a step
+    is one distfind_css_distance call (host reduction, device tables and probes, one
+    certificate); value and e2e are both its wall time (the inputs are two 49 x 98 matrices)."""
+    from qubitserf_b200 import workloads as W
+    Hx, Hz = W.toric_code(MITM_L)
+    config = {"workload": f"toric_L{MITM_L}_n{2 * MITM_L * MITM_L}_mitm_min", "which": "min",
+              "method": "mitm", "parallelism": f"replicas{world}",
+              "timed": "wall time of distfind_css_distance (no L2 flush: tables are rebuilt "
+                       "every call)"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle.refbind import Ref
+        ref = Ref()
+        Lw = W.toric_code(5)
+        for _ in range(min(args.warmup, 1)):
+            ref.css(*Lw, "M", method="mitm")
+        ts = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            r = ref.css(Hx, Hz, "M", method="mitm")
+            ts.append(time.perf_counter() - t)
+        v = args.steps / sum(ts)
+        b = {"value": v, "unit": "certs/s", "cores": os.cpu_count(), "kind": "reference",
+             "sample": f"the full workload ({args.steps} certificate(s), distance {r.distance})"}
+        print(json.dumps({"metric": MITM_METRIC, "value": v, "unit": "certs/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                          "config": config, "impl": "reference", "cpu_baseline": b,
+                          "e2e": {"value": v, "unit": "certs/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    from qubitserf_b200 import _native
+    if not _native.backend_available("gpu"):
+        raise SystemExit("no sm_100 device visible")
+    for _ in range(args.warmup):
+        r = _native.css_distance_raw(Hx, Hz, "mitm", "M", "gpu", 0, False)
+    barrier(pg)
+    ts, rep = [], None
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            r = _native.css_distance_raw(Hx, Hz, "mitm", "M", "gpu", 0, False)
+            ts.append(time.perf_counter() - t)
+            rep = _native.last_report()
+    assert (r.distance, r.proven) == (MITM_L, 1)
+    wall = max_over_ranks(pg, sum(ts))
+    value = args.steps * world / wall
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": MITM_METRIC, "value": value, "unit": "certs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic", "config": config, "distance": r.distance, "levels": r.levels,
+        "parts_per_step": rep.codewords, "parts_per_s": rep.codewords * args.steps / wall,
+        "roofline": {"bound": "memory latency (random 8-byte tag reads of the table probes)",
+                     "kernel": "mitm_probe_kernel", "achieved": None, "peak": None,
+                     "frac": None, "traffic": None},
+        "cpu_baseline": None,
+        "e2e": {"value": value, "unit": "certs/s",
+                "h2d_bytes_per_step": int(Hx.size + Hz.size), "d2h_bytes_per_step": 48},
+        "gpu_launches": rep.kernel_launches, "clocks": clk.summary()}), flush=True)
 
 
 def tc_traffic_per_launch(tc_cw_per_step):

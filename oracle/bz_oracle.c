@@ -874,12 +874,244 @@ static void bz_min(const problem* pz, const problem* px, const orc_options* opt,
     side_free(&X);
 }
 
+
+/* ------------------------------------------------------------------ meet in the middle
+ * method "mitm", cpp/distfind/mitm.cpp:1-552: with H = nullspace(code_gen), level d hits when
+ * a left part (coordinates [0, nL)) and a right part ([nL, ncoord)) of weights wL + wR = d
+ * share their syndrome (XOR of H's columns) and, unless every codeword counts, differ in
+ * their logical fingerprint (XOR of the detector's columns).  Symplectic problems split
+ * qubits and give each chosen qubit Z, X or Y (enumerate_side_sym, mitm.cpp:158-199).  The
+ * reference joins with a hash map; this restatement sorts the left parts by (syndrome,
+ * fingerprint) and binary-searches every right part. */
+typedef struct {
+    int sw, lw, kw;          /* u64 words: syndrome, fingerprint, record */
+    int ncoord, nL, qubits, sym, count_all;
+    u64* cols;               /* ncols x kw: syndrome then fingerprint of each column */
+} mitm_view;
+
+static int mitm_kw;
+static int cmp_rec(const void* a, const void* b) {
+    const u64* x = (const u64*)a;
+    const u64* y = (const u64*)b;
+    for (int i = 0; i < mitm_kw; ++i)
+        if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+    return 0;
+}
+
+static mitm_view mitm_view_of(const problem* p) {
+    mitm_view v;
+    mat H = m_nullspace(&p->gen);
+    v.sym = p->symplectic;
+    v.qubits = p->qubits;
+    v.count_all = p->count_all;
+    v.ncoord = v.sym ? p->qubits : p->n;
+    v.nL = v.ncoord / 2;
+    v.sw = words_for(H.rows);
+    v.lw = v.count_all ? 0 : words_for(p->check.rows);
+    v.kw = v.sw + v.lw;
+    if (v.kw == 0) v.kw = 1;   /* a record of one zero word */
+    v.cols = (u64*)calloc((size_t)p->n * v.kw + 1, sizeof(u64));
+    for (int j = 0; j < p->n; ++j) {
+        u64* c = v.cols + (size_t)j * v.kw;
+        for (int i = 0; i < H.rows; ++i)
+            if (m_get(&H, i, j)) c[i >> 6] |= 1ull << (i & 63);
+        if (!v.count_all)
+            for (int i = 0; i < p->check.rows; ++i)
+                if (m_get(&p->check, i, j)) c[v.sw + (i >> 6)] |= 1ull << (i & 63);
+    }
+    m_free(&H);
+    return v;
+}
+
+/* every part of weight w over coordinates [first, first + m): records of kw words */
+static u64* mitm_parts(const mitm_view* v, int first, int m, int w, size_t* count) {
+    size_t n = 1;
+    for (int i = 1; i <= w; ++i) n = n * (size_t)(m - w + i) / (size_t)i;
+    size_t p3 = 1;
+    if (v->sym)
+        for (int i = 0; i < w; ++i) p3 *= 3;
+    *count = n * p3;
+    u64* out = (u64*)calloc(*count * v->kw + 1, sizeof(u64));
+    int* pos = (int*)malloc(sizeof(int) * (size_t)(w + 1));
+    int* pa = (int*)calloc((size_t)w + 1, sizeof(int));
+    for (int i = 0; i < w; ++i) pos[i] = i;
+    size_t k = 0;
+    for (;;) {
+        for (size_t q = 0; q < p3; ++q) {
+            /* base-3 odometer value q: digit i picks Z (0), X (1) or Y (2) on qubit pos[i] */
+            size_t t = q;
+            for (int i = 0; i < w; ++i) { pa[i] = (int)(t % 3); t /= 3; }
+            u64* r = out + k * v->kw;
+            for (int i = 0; i < w; ++i) {
+                const int coord = first + pos[i];
+                if (!v->sym) {
+                    v_xor(r, v->cols + (size_t)coord * v->kw, v->kw);
+                } else {
+                    if (pa[i] != 1) v_xor(r, v->cols + (size_t)coord * v->kw, v->kw);
+                    if (pa[i] != 0) v_xor(r, v->cols + (size_t)(v->qubits + coord) * v->kw, v->kw);
+                }
+            }
+            ++k;
+        }
+        int j = w - 1;
+        while (j >= 0 && pos[j] == m - w + j) --j;
+        if (j < 0) break;
+        ++pos[j];
+        for (int t2 = j + 1; t2 < w; ++t2) pos[t2] = pos[t2 - 1] + 1;
+    }
+    free(pos);
+    free(pa);
+    return out;
+}
+
+/* has_codeword_of_weight(_sym), cpp/distfind/mitm.cpp:201-316 */
+static int mitm_level(const mitm_view* v, int d) {
+    const int nR = v->ncoord - v->nL;
+    for (int wL = 0; wL <= d; ++wL) {
+        const int wR = d - wL;
+        if (wL > v->nL || wR > nR) continue;
+        size_t nl, nr;
+        u64* L = mitm_parts(v, 0, v->nL, wL, &nl);
+        u64* R = mitm_parts(v, v->nL, nR, wR, &nr);
+        mitm_kw = v->kw;
+        qsort(L, nl, (size_t)v->kw * sizeof(u64), cmp_rec);
+        int hit = 0;
+        for (size_t i = 0; i < nr && !hit; ++i) {
+            const u64* r = R + i * v->kw;
+            /* first left record with syndrome >= r's */
+            size_t lo = 0, hi = nl;
+            while (lo < hi) {
+                const size_t mid = (lo + hi) / 2;
+                int c = 0;
+                for (int q = 0; q < v->sw && !c; ++q) {
+                    const u64 a = L[mid * v->kw + q], b = r[q];
+                    c = a < b ? -1 : (a > b ? 1 : 0);
+                }
+                if (c < 0) lo = mid + 1; else hi = mid;
+            }
+            for (size_t j = lo; j < nl && !hit; ++j) {
+                const u64* l = L + j * v->kw;
+                int same = 1;
+                for (int q = 0; q < v->sw && same; ++q) same = l[q] == r[q];
+                if (!same) break;
+                if (v->count_all) { hit = 1; break; }
+                for (int q = v->sw; q < v->sw + v->lw; ++q)
+                    if (l[q] != r[q]) { hit = 1; break; }
+            }
+        }
+        free(L);
+        free(R);
+        if (hit) return 1;
+    }
+    return 0;
+}
+
+typedef struct {
+    int has, target, seed_upper, found, level, resolved, confirmed;
+    mitm_view v;
+} mitm_side;
+
+static void mitm_side_init(mitm_side* s, const problem* p) {
+    memset(s, 0, sizeof(*s));
+    s->found = -1;
+    s->has = !(p->gen.rows == 0 || (!p->count_all && p->check.rows == 0));
+    if (!s->has) { s->resolved = s->confirmed = 1; return; }
+    s->v = mitm_view_of(p);
+    s->seed_upper = p->seed_upper;
+    s->target = p->seed_upper > 0 ? (p->seed_upper < s->v.ncoord ? p->seed_upper : s->v.ncoord)
+                                  : s->v.ncoord;
+}
+
+static void mitm_side_free(mitm_side* s) {
+    if (s->has) free(s->v.cols);
+}
+
+/* mitm_distance, cpp/distfind/mitm.cpp:318-380 */
+static void mitm_single(const problem* p, orc_result* r) {
+    memset(r, 0, sizeof(*r));
+    mitm_side s;
+    mitm_side_init(&s, p);
+    if (s.has) {
+        for (int d = 1; d <= s.target; ++d) {
+            ++s.level;
+            if (mitm_level(&s.v, d)) { s.found = d; break; }
+        }
+        if (s.found < 0 && s.seed_upper > 0 && s.target == s.seed_upper) s.found = s.seed_upper;
+    }
+    r->distance = s.found;
+    r->levels = s.level;
+    r->lower_bound = s.found >= 0 ? s.found : 0;
+    r->proven = s.found >= 0;
+    mitm_side_free(&s);
+}
+
+/* mitm_min_interleaved with cap_to_min, cpp/distfind/mitm.cpp:447-521 */
+static void mitm_min(const problem* pz, const problem* px, orc_result* r) {
+    memset(r, 0, sizeof(*r));
+    mitm_side Z, X;
+    mitm_side_init(&Z, pz);
+    mitm_side_init(&X, px);
+    mitm_side* sides[2] = {&Z, &X};
+    int best = ORC_WEIGHT_NONE;
+    if (Z.has && Z.seed_upper > 0 && Z.seed_upper < best) best = Z.seed_upper;
+    if (X.has && X.seed_upper > 0 && X.seed_upper < best) best = X.seed_upper;
+    const int tz = Z.has ? Z.target : 0, tx = X.has ? X.target : 0;
+    const int maxd = tz > tx ? tz : tx;
+    for (int d = 1; d <= maxd; ++d) {
+        for (int k = 0; k < 2; ++k) {
+            mitm_side* S = sides[k];
+            if (S->resolved) continue;
+            if (d > S->target) {
+                if (S->seed_upper > 0 && S->target == S->seed_upper) {
+                    S->found = S->seed_upper;
+                    S->confirmed = 1;
+                    if (S->found < best) best = S->found;
+                }
+                S->resolved = 1;
+                continue;
+            }
+            if (d >= best) {
+                S->confirmed = 1;
+                if (S->seed_upper > 0 && best == S->seed_upper) S->found = best;
+                S->resolved = 1;
+                continue;
+            }
+            ++S->level;
+            if (mitm_level(&S->v, d)) {
+                S->found = d;
+                if (d < best) best = d;
+                S->confirmed = 1;
+                S->resolved = 1;
+            }
+        }
+        if (Z.resolved && X.resolved) break;
+    }
+    const int vz = Z.found >= 0 ? Z.found : ORC_WEIGHT_NONE;
+    const int vx = X.found >= 0 ? X.found : ORC_WEIGHT_NONE;
+    const int dist = vz < vx ? vz : vx;
+    r->distance = dist >= ORC_WEIGHT_NONE ? -1 : dist;
+    r->lower_bound = dist >= ORC_WEIGHT_NONE ? 0 : dist;
+    r->levels = Z.level > X.level ? Z.level : X.level;
+    r->proven = Z.confirmed && X.confirmed && dist < ORC_WEIGHT_NONE;
+    mitm_side_free(&Z);
+    mitm_side_free(&X);
+}
+
+/* the method switch of cpp/distfind/capi.cpp:53-60: "mitm" or BZ */
+static void solve_single(const problem* p, const orc_options* opt, orc_result* r) {
+    if (opt && opt->mitm) mitm_single(p, r); else bz_single(p, opt, r);
+}
+static void solve_min(const problem* pz, const problem* px, const orc_options* opt,
+                      orc_result* r) {
+    if (opt && opt->mitm) mitm_min(pz, px, r); else bz_min(pz, px, opt, r);
+}
+
 /* ------------------------------------------------------------------ public entry points */
 int orc_classical_distance(const uint8_t* H, int rows, int cols, const orc_options* opt,
                            orc_result* out) {
     mat h = m_from_dense(H, rows, cols);
     problem p = classical_problem(&h);
-    bz_single(&p, opt, out);
+    solve_single(&p, opt, out);
     p_free(&p);
     m_free(&h);
     return 0;
@@ -890,14 +1122,14 @@ static int css_like(mat* A, mat* B, int subsystem, char which, const orc_options
     if (which == 'Z' || which == 'X') {
         problem p = subsystem ? subsystem_problem(A, B, which)
                               : (which == 'X' ? build(B, A) : build(A, B));
-        bz_single(&p, opt, out);
+        solve_single(&p, opt, out);
         p_free(&p);
     } else if (subsystem) {
         /* not interleaved, cpp/distfind/capi.cpp:256-274 */
         problem pz = subsystem_problem(A, B, 'Z'), px = subsystem_problem(A, B, 'X');
         orc_result rz, rx;
-        bz_single(&pz, opt, &rz);
-        bz_single(&px, opt, &rx);
+        solve_single(&pz, opt, &rz);
+        solve_single(&px, opt, &rx);
         const int vz = rz.distance < 0 ? (1 << 30) : rz.distance;
         const int vx = rx.distance < 0 ? (1 << 30) : rx.distance;
         *out = vx < vz ? rx : rz;
@@ -910,7 +1142,7 @@ static int css_like(mat* A, mat* B, int subsystem, char which, const orc_options
         p_free(&px);
     } else {
         problem pz = build(A, B), px = build(B, A);
-        bz_min(&pz, &px, opt, out);
+        solve_min(&pz, &px, opt, out);
         p_free(&pz);
         p_free(&px);
     }
@@ -944,7 +1176,7 @@ static int coset_weight(const mat* G, const uint8_t* vec, const orc_options* opt
     } else {
         problem p = coset_problem(G, v);
         orc_result r;
-        bz_single(&p, opt, &r);
+        solve_single(&p, opt, &r);
         res = r.distance;
         p_free(&p);
     }
@@ -979,6 +1211,14 @@ int orc_stabilizer_distance(const uint8_t* S, int rows, int cols, int subsystem,
     }
     mat Sn = subsystem ? sympl_center(&G) : m_copy(&G);
     problem sp = sympl_problem(&Sn, &G);
+    if (opt && opt->mitm) {
+        /* mitm enumerates symplectic parts directly (capi.cpp:333-335) */
+        mitm_single(&sp, out);
+        p_free(&sp);
+        m_free(&Sn);
+        m_free(&G);
+        return 0;
+    }
     problem e = isometry(&sp);
     bz_single(&e, opt, out);
     if (out->distance > 0) out->distance /= 2;
@@ -1004,11 +1244,15 @@ int orc_pauli_operator_weight(const uint8_t* Gm, int rows, int cols, const uint8
         p.symplectic = 1;
         p.qubits = cols / 2;
         p.seed_upper = sw_weight(v, p.qubits);
-        problem e = isometry(&p);
-        bz_single(&e, opt, out);
-        if (out->distance > 0) out->distance /= 2;
-        if (out->lower_bound > 0) out->lower_bound /= 2;
-        p_free(&e);
+        if (opt && opt->mitm) {
+            mitm_single(&p, out);   /* capi.cpp:275-282 */
+        } else {
+            problem e = isometry(&p);
+            bz_single(&e, opt, out);
+            if (out->distance > 0) out->distance /= 2;
+            if (out->lower_bound > 0) out->lower_bound /= 2;
+            p_free(&e);
+        }
         p_free(&p);
     }
     free(v);

@@ -29,6 +29,7 @@ typedef struct {
     int* levels_w;
     int* levels_active;
     int* levels_side;
+    int mitm;               /* method "mitm": meet in the middle (cpp/distfind/mitm.cpp) */
 } orc_options;
 
 /* One level, brute force: cpp/qsf/backend.hpp:84-100 evaluated over every combination in

@@ -105,66 +105,66 @@ class Ref:
                                          ctypes.POINTER(ctypes.c_uint64), ctypes.c_longlong,
                                          ctypes.POINTER(ctypes.c_uint64), ctypes.c_longlong]
 
-    def classical(self, H, threads=0):
+    def classical(self, H, threads=0, method="bz"):
         a = u8(H)
         out = DistfindResult()
-        rc = self.lib.distfind_classical_distance(_p(a), a.shape[0], a.shape[1], b"bz", b"cpu",
+        rc = self.lib.distfind_classical_distance(_p(a), a.shape[0], a.shape[1], method.encode(), b"cpu",
                                                   threads, 0, ctypes.byref(out))
         assert rc == 0
         return out
 
-    def css(self, Hx, Hz, which="M", threads=0):
+    def css(self, Hx, Hz, which="M", threads=0, method="bz"):
         ax, az = u8(Hx), u8(Hz)
         out = DistfindResult()
         rc = self.lib.distfind_css_distance(_p(ax), ax.shape[0], ax.shape[1], _p(az),
-                                            az.shape[0], az.shape[1], b"bz", which.encode(),
+                                            az.shape[0], az.shape[1], method.encode(), which.encode(),
                                             b"cpu", threads, 0, ctypes.byref(out))
         assert rc == 0
         return out
 
-    def subsystem(self, Gx, Gz, which="M", threads=0):
+    def subsystem(self, Gx, Gz, which="M", threads=0, method="bz"):
         ax, az = u8(Gx), u8(Gz)
         out = DistfindResult()
         rc = self.lib.distfind_subsystem_distance(_p(ax), ax.shape[0], ax.shape[1], _p(az),
-                                                  az.shape[0], az.shape[1], b"bz",
+                                                  az.shape[0], az.shape[1], method.encode(),
                                                   which.encode(), b"cpu", threads, 0,
                                                   ctypes.byref(out))
         assert rc == 0
         return out
 
-    def operator_weight(self, Gx, Gz, z, x, threads=0):
+    def operator_weight(self, Gx, Gz, z, x, threads=0, method="bz"):
         ax, az = u8(Gx), u8(Gz)
         zz, xx = u8(z).reshape(-1), u8(x).reshape(-1)
         out = DistfindOpResult()
         rc = self.lib.distfind_operator_weight(_p(ax), ax.shape[0], ax.shape[1], _p(az),
                                                az.shape[0], az.shape[1], _p(zz), _p(xx),
-                                               ax.shape[1], b"bz", b"cpu", threads, 0,
+                                               ax.shape[1], method.encode(), b"cpu", threads, 0,
                                                ctypes.byref(out))
         assert rc == 0
         return out
 
-    def stabilizer(self, S, which="M", threads=0):
+    def stabilizer(self, S, which="M", threads=0, method="bz"):
         a = u8(S)
         out = DistfindResult()
-        rc = self.lib.distfind_stabilizer_distance(_p(a), a.shape[0], a.shape[1], b"bz",
+        rc = self.lib.distfind_stabilizer_distance(_p(a), a.shape[0], a.shape[1], method.encode(),
                                                    which.encode(), b"cpu", threads, 0,
                                                    ctypes.byref(out))
         return rc, out
 
-    def subsystem_stabilizer(self, G, which="M", threads=0):
+    def subsystem_stabilizer(self, G, which="M", threads=0, method="bz"):
         a = u8(G)
         out = DistfindResult()
         rc = self.lib.distfind_subsystem_stabilizer_distance(_p(a), a.shape[0], a.shape[1],
-                                                             b"bz", which.encode(), b"cpu",
+                                                             method.encode(), which.encode(), b"cpu",
                                                              threads, 0, ctypes.byref(out))
         return rc, out
 
-    def pauli_operator_weight(self, G, op, threads=0):
+    def pauli_operator_weight(self, G, op, threads=0, method="bz"):
         a = u8(G)
         o = u8(op).reshape(-1)
         out = DistfindResult()
         rc = self.lib.distfind_stabilizer_operator_weight(_p(a), a.shape[0], a.shape[1], _p(o),
-                                                          o.shape[0], b"bz", b"cpu", threads, 0,
+                                                          o.shape[0], method.encode(), b"cpu", threads, 0,
                                                           ctypes.byref(out))
         return rc, out
 
@@ -243,7 +243,7 @@ class OrcOptions(ctypes.Structure):
     _fields_ = [("no_early_stop", ctypes.c_int), ("seed_trials", ctypes.c_int),
                 ("cap", ctypes.c_int), ("levels_w", ctypes.POINTER(ctypes.c_int)),
                 ("levels_active", ctypes.POINTER(ctypes.c_int)),
-                ("levels_side", ctypes.POINTER(ctypes.c_int))]
+                ("levels_side", ctypes.POINTER(ctypes.c_int)), ("mitm", ctypes.c_int)]
 
 
 class Oracle:
@@ -277,8 +277,9 @@ class Oracle:
                                   ctypes.POINTER(i), i]
 
     @staticmethod
-    def _opts(no_early_stop=False, seed_trials=0, trace_cap=0):
+    def _opts(no_early_stop=False, seed_trials=0, trace_cap=0, method="bz"):
         o = OrcOptions()
+        o.mitm = 1 if method == "mitm" else 0
         o.no_early_stop = 1 if no_early_stop else 0
         o.seed_trials = seed_trials
         bufs = None

@@ -1,7 +1,9 @@
 """Distance API of the B200 engine, mirroring the reference's
 python/qubitserf/distfind/api.py:75-251 (same names, keyword arguments, return values and
-exceptions).  Every call runs Brouwer-Zimmermann on the GPU; ``backend`` accepts
-"auto"/"gpu" ("cpu" raises: this engine has no CPU path), ``method`` accepts "bz".
+exceptions).  Every call runs on the GPU; ``backend`` accepts "auto"/"gpu" ("cpu" raises:
+this engine has no CPU path); ``method`` "bz" runs Brouwer-Zimmermann, "mitm" the
+meet-in-the-middle syndrome join, "cc" (connected cluster) raises where the reference would
+run its cc solver and falls back as the reference does elsewhere.
 """
 from __future__ import annotations
 

@@ -1,6 +1,7 @@
 // extern "C" boundary of libqsfb200.so.  The distfind_* functions keep the reference's
 // signatures, result structs, dispatch and return codes (cpp/distfind/capi.cpp:144-420);
-// every accepted call runs the BZ enumeration on the GPU and there is no CPU path.
+// every accepted call runs on the GPU (method "bz": the BZ enumeration; "mitm": the
+// meet-in-the-middle join of mitm.cu) and there is no CPU path.
 #include "../../include/qsf_b200.h"
 
 #include <algorithm>
@@ -15,6 +16,7 @@
 
 #include "bz.hpp"
 #include "engine.hpp"
+#include "mitm.hpp"
 #include "problem.hpp"
 
 using namespace qsfb;
@@ -78,11 +80,14 @@ void fill(DistfindResult* out, const BzResult& r) {
     out->backend[sizeof(out->backend) - 1] = '\0';
 }
 
-// Only method "bz" on an accelerator backend runs here.
+// Method "mitm" runs the meet-in-the-middle join and any other name BZ, as in the
+// reference's dispatch (cpp/distfind/capi.cpp:53-60, 79); "cc" (connected cluster) is not
+// run here: callers that the reference sends to its cc solver get rc 5, the others map it
+// before this check.  Only accelerator backends run.
 int check_dispatch(const char* method, const char* backend) {
     const std::string m = method ? method : "bz";
     const std::string b = backend ? backend : "auto";
-    if (m != "bz") return kErrUnsupported;
+    if (m == "cc") return kErrUnsupported;
     if (b != "auto" && b != "gpu" && b != "cuda") return kErrUnsupported;
     return kOk;
 }
@@ -97,6 +102,13 @@ BzOptions options(int verbose) {
     BzOptions o;
     o.verbose = verbose != 0;
     return o;
+}
+
+bool is_mitm(const char* method) { return method && std::strcmp(method, "mitm") == 0; }
+
+// One subproblem by the requested method (cpp/distfind/capi.cpp:53-56, 79, 139-142).
+int solve_one(Device* dev, const Problem& p, bool mitm, int verbose, BzResult& r) {
+    return mitm ? mitm_distance(dev, p, r) : bz_distance(dev, p, options(verbose), r);
 }
 
 // Merge for the (non-interleaved) subsystem min, cpp/distfind/capi.cpp:265-274.
@@ -119,8 +131,8 @@ BzResult min_of(const BzResult& z, const BzResult& x) {
 }
 
 // CSS routing shared by distfind_css_distance and the symplectic CSS fast path.
-int css_like(Device* dev, const Mat& A, const Mat& B, bool subsystem, char which, int verbose,
-             DistfindResult* out) {
+int css_like(Device* dev, const Mat& A, const Mat& B, bool subsystem, char which, bool mitm,
+             int verbose, DistfindResult* out) {
     auto prob = [&](char w) {
         return subsystem ? subsystem_problem(A, B, w) : css_problem(A, B, w);
     };
@@ -130,18 +142,19 @@ int css_like(Device* dev, const Mat& A, const Mat& B, bool subsystem, char which
     if (which == 'Z' || which == 'X') {
         Problem p = prob(which);
         nbits = p.n;
-        rc = bz_distance(dev, p, options(verbose), r);
+        rc = solve_one(dev, p, mitm, verbose, r);
     } else if (subsystem) {
         Problem pz = prob('Z'), px = prob('X');
         nbits = pz.n;
         BzResult rz, rx;
-        rc = bz_distance(dev, pz, options(verbose), rz);
-        if (rc == kOk) rc = bz_distance(dev, px, options(verbose), rx);
+        rc = solve_one(dev, pz, mitm, verbose, rz);
+        if (rc == kOk) rc = solve_one(dev, px, mitm, verbose, rx);
         if (rc == kOk) r = min_of(rz, rx);
     } else {
         auto pr = css_problem_pair(A, B);
         nbits = pr.first.n;
-        rc = bz_min_interleaved(dev, pr.first, pr.second, options(verbose), r);
+        rc = mitm ? mitm_min_interleaved(dev, pr.first, pr.second, r)
+                  : bz_min_interleaved(dev, pr.first, pr.second, options(verbose), r);
     }
     if (rc != kOk) return rc;
     fill(out, r);
@@ -161,12 +174,15 @@ int symplectic_driver(const Mat& gauge, bool subsystem, const char* method, char
     if (!dev) return rc;
     if (css) {
         auto hxhz = split_css(gauge);
-        return css_like(dev, hxhz.first, hxhz.second, subsystem, which, verbose, out);
+        return css_like(dev, hxhz.first, hxhz.second, subsystem, which, is_mitm(method), verbose,
+                        out);
     }
     Mat Snorm = subsystem ? symplectic_center(gauge) : gauge;
     Problem sp = symplectic_problem(Snorm, gauge);
     BzResult r;
-    rc = symplectic_bz_distance(dev, sp, options(verbose), r);
+    // mitm enumerates symplectic parts directly; bz goes through the isometry
+    rc = is_mitm(method) ? mitm_distance(dev, sp, r)
+                         : symplectic_bz_distance(dev, sp, options(verbose), r);
     if (rc != kOk) return rc;
     fill(out, r);
     record(r, 3 * sp.qubits);
@@ -207,7 +223,7 @@ int distfind_css_distance(const uint8_t* Hx, int hx_rows, int hx_cols, const uin
     Device* dev = device_or(&rc);
     if (!dev) return rc;
     Mat A = from_dense(Hx, hx_rows, hx_cols), B = from_dense(Hz, hz_rows, hz_cols);
-    return css_like(dev, A, B, false, which, verbose, out);
+    return css_like(dev, A, B, false, which, is_mitm(method), verbose, out);
 }
 
 int distfind_classical_distance(const uint8_t* H, int rows, int cols, const char* method,
@@ -215,13 +231,15 @@ int distfind_classical_distance(const uint8_t* H, int rows, int cols, const char
                                 DistfindResult* out) {
     (void)threads;
     if (!out || !H) return kErrNull;
-    int rc = check_dispatch(method, backend);
+    // the classical path has no cc form: the reference runs BZ for it (capi.cpp:79)
+    const bool mitm = is_mitm(method);
+    int rc = check_dispatch(mitm ? "mitm" : "bz", backend);
     if (rc != kOk) return rc;
     Device* dev = device_or(&rc);
     if (!dev) return rc;
     Problem p = classical_problem(from_dense(H, rows, cols));
     BzResult r;
-    rc = bz_distance(dev, p, options(verbose), r);
+    rc = solve_one(dev, p, mitm, verbose, r);
     if (rc != kOk) return rc;
     fill(out, r);
     record(r, p.n);
@@ -256,7 +274,7 @@ int distfind_operator_weight(const uint8_t* Gx, int gx_rows, int gx_cols, const 
         if (in_rowspace(G, vec)) { *res = 0; return kOk; }
         Problem p = coset_problem(G, vec);
         BzResult r;
-        const int e = bz_distance(dev, p, options(verbose), r);
+        const int e = solve_one(dev, p, m == "mitm", verbose, r);
         if (e != kOk) return e;
         secs += r.seconds;
         proven = proven && r.proven;
@@ -290,7 +308,7 @@ int distfind_subsystem_distance(const uint8_t* Gx, int gx_rows, int gx_cols, con
     Device* dev = device_or(&rc);
     if (!dev) return rc;
     Mat A = from_dense(Gx, gx_rows, gx_cols), B = from_dense(Gz, gz_rows, gz_cols);
-    return css_like(dev, A, B, true, which, verbose, out);
+    return css_like(dev, A, B, true, which, is_mitm(method), verbose, out);
 }
 
 int distfind_stabilizer_distance(const uint8_t* S, int rows, int cols, const char* method,
@@ -317,7 +335,14 @@ int distfind_stabilizer_operator_weight(const uint8_t* G, int rows, int cols, co
     (void)threads;
     if (!out || !G || !op) return kErrNull;
     if (cols % 2 != 0 || op_len != cols) return kErrShape;
-    int rc = check_dispatch(method, backend);
+    std::string m = method ? method : "bz";
+    if (m == "cc") {   // cpp/distfind/capi.cpp:277-282
+        std::fprintf(stderr,
+                     "distfind: connected-cluster has no operator-weight form; using the "
+                     "symplectic meet-in-the-middle search instead.\n");
+        m = "mitm";
+    }
+    int rc = check_dispatch(m.c_str(), backend);
     if (rc != kOk) return rc;
     Mat mG = from_dense(G, rows, cols);
     BzResult r;
@@ -332,7 +357,8 @@ int distfind_stabilizer_operator_weight(const uint8_t* G, int rows, int cols, co
     Device* dev = device_or(&rc);
     if (!dev) return rc;
     Problem sp = symplectic_coset_problem(mG, op);
-    rc = symplectic_bz_distance(dev, sp, options(verbose), r);
+    rc = m == "mitm" ? mitm_distance(dev, sp, r)
+                     : symplectic_bz_distance(dev, sp, options(verbose), r);
     if (rc != kOk) return rc;
     fill(out, r);
     record(r, 3 * sp.qubits);

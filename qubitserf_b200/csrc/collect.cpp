@@ -5,9 +5,11 @@
 // does: pack G; find each row's private column (the probe words skip them, the pivot count
 // stands in for them); choose the probe width; generate every prefix/suffix list the levels
 // need in one launch; one pair-sweep launch per subset size into one output buffer; one
-// synchronisation.  The hit counter is exact even when the buffer is too small, so an
-// overflow re-runs the sweeps once with the exact capacity (the reference recomputes the
-// level on its CPU backend instead; there is no CPU path here).  The sort and
+// synchronisation.  The sweeps append the rare pairs that pass their lower bound as
+// candidates; one more kernel evaluates those exactly and appends the hits.  Both counters
+// are exact even when their buffers are too small, so an overflow re-runs the stage once
+// with the exact capacity (the reference recomputes the level on its CPU backend instead;
+// there is no CPU path here).  The sort and
 // deduplication stay on the host as in the reference.
 #include "../../include/qsf_b200.h"
 
@@ -31,6 +33,8 @@ namespace qsfb {
 cudaError_t launch_collect_gen(const CollectListDesc* d_lists, int nlists, unsigned long long runs,
                                const CollectShared& S, const unsigned long long* d_binom,
                                int num_sms, cudaStream_t st);
+cudaError_t launch_collect_exact(const CollectLevelDesc* d_levels, const CollectShared& S,
+                                 const unsigned long long* d_binom, int num_sms, cudaStream_t st);
 cudaError_t launch_collect_pairs(const CollectLevelDesc* d_levels, int level,
                                  unsigned long long jobs, const CollectShared& S,
                                  const unsigned long long* d_binom, int num_sms,
@@ -40,6 +44,7 @@ namespace {
 
 constexpr long long kComboCap = 1LL << 62;     // bz.cpp:29
 constexpr unsigned long long kFirstCap = 1ull << 16;   // output rows before the first run
+constexpr unsigned long long kFirstCand = 1ull << 20;  // candidate pairs before the first run
 
 struct CollectHandle {
     int n = 0, stride = 0;
@@ -330,10 +335,19 @@ int run_collect(const uint8_t* G, int m, int n, int p, int keep, CollectHandle* 
     if (cudaEventRecord(s->ev_tc1, st) != cudaSuccess) return fail();
     H->st.launches = runs_total ? 1 : 0;
 
+    unsigned long long cand_cap = kFirstCand;
+    unsigned long long* d_cand = (unsigned long long*)bufs.get(cand_cap * 16);
+    if (!d_cand) return kErrMemory;
     unsigned long long h_ctr[2] = {0, 0};
+    auto read_ctr = [&]() -> bool {
+        return cudaMemcpyAsync(h_ctr, S.ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+               cudaStreamSynchronize(st) == cudaSuccess;
+    };
     for (int pass = 0; pass < 2; ++pass) {
         S.out = d_out;
         S.cap = cap;
+        S.cand = d_cand;
+        S.cand_cap = cand_cap;
         if (cudaMemsetAsync(S.ctr, 0, b_ctr, st) != cudaSuccess) return fail();
         if (cudaEventRecord(s->ev0, st) != cudaSuccess) return fail();
         for (int sw = 1; sw <= maxsw; ++sw) {
@@ -343,24 +357,41 @@ int run_collect(const uint8_t* G, int m, int n, int p, int keep, CollectHandle* 
                 return fail();
             ++H->st.launches;
         }
-        if (cudaEventRecord(s->ev1, st) != cudaSuccess) return fail();
-        if (cudaMemcpyAsync(h_ctr, S.ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        if (launch_collect_exact(d_levels, S, dev->d_binom, dev->num_sms, st) != cudaSuccess)
             return fail();
-        if (cudaStreamSynchronize(st) != cudaSuccess) return fail();
-        float ms = 0.f;
+        ++H->st.launches;
+        if (cudaEventRecord(s->ev1, st) != cudaSuccess) return fail();
+        if (!read_ctr()) return fail();
         if (pass == 0) {
             float gen_ms = 0.f;
             cudaEventElapsedTime(&gen_ms, s->ev_tc0, s->ev_tc1);
             H->st.gen_ms = gen_ms;
         }
+        float ms = 0.f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
         H->st.pairs_ms = ms;
-        if (h_ctr[0] <= cap) break;
-        // the counter is exact: run again into a buffer of exactly that many rows
+        if (h_ctr[1] <= cand_cap) break;
+        // more candidates than slots (the counter is exact): sweep again into enough slots
+        ++H->st.reruns;
+        cand_cap = h_ctr[1];
+        d_cand = (unsigned long long*)bufs.get(cand_cap * 16);
+        if (!d_cand) return kErrMemory;
+    }
+    if (h_ctr[1] > cand_cap) return kErrDevice;
+    if (h_ctr[0] > cap) {
+        // more hits than output rows: evaluate the (complete) candidates again into enough rows
         ++H->st.reruns;
         cap = h_ctr[0];
         d_out = (unsigned long long*)bufs.get(cap * S64 * 8);
         if (!d_out) return kErrMemory;
+        S.out = d_out;
+        S.cap = cap;
+        if (cudaMemsetAsync(S.ctr, 0, 8, st) != cudaSuccess) return fail();
+        if (launch_collect_exact(d_levels, S, dev->d_binom, dev->num_sms, st) != cudaSuccess)
+            return fail();
+        ++H->st.launches;
+        if (!read_ctr()) return fail();
+        if (h_ctr[0] > cap) return kErrDevice;
     }
     const unsigned long long hits = h_ctr[0];
     H->st.hits = (int64_t)hits;

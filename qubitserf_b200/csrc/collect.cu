@@ -11,9 +11,9 @@
 //
 // The sweep is bound by the POPC (XU) pipe: per pair a few XORs/ORs and one or two POPCs
 // give a lower bound on pivots + popc(probe) (probe_bound below); a three-input minimum
-// folds eight of them per suffix entry and only a minimum under keep + 1 sends the lane to
-// the exact path, which unranks both subsets, XORs their full rows and appends the
-// codeword when its weight is in range.
+// folds eight of them per suffix entry and only a minimum under keep + 1 makes the lane
+// append its candidate pairs.  collect_exact_kernel then unranks both subsets of every
+// candidate, XORs their full rows and appends the codeword when its weight is in range.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -137,50 +137,58 @@ __device__ __forceinline__ int probe_bound(const uint32_t (&x)[HP], const uint32
     }
 }
 
-// Exact evaluation of the pair (prefix entry ex, suffix entry ey): both subsets unranked,
-// their full rows XORed, the codeword appended when its weight is in [1, keep].  The slot
-// counter keeps counting past the capacity so that the host learns the exact hit count.
-static __device__ __noinline__ void collect_exact(const CollectShared& S,
-                                                  const CollectLevelDesc& L,
-                                                  const unsigned long long* __restrict__ B,
-                                                  unsigned long long ex,
-                                                  unsigned long long ey) {
-    int c[kCollectMaxSize];
-    unsigned long long acc[kCollectMaxWords];
+// Exact evaluation of the candidates (prefix entry, suffix entry, subset size): both subsets
+// unranked, their full rows XORed, the codeword appended when its weight is in [1, keep].
+// The candidate count is read on the device; the hit counter keeps counting past the
+// output capacity so that the host learns the exact hit count.
+__global__ void __launch_bounds__(256) collect_exact_kernel(const CollectLevelDesc* __restrict__ levels,
+                                                            CollectShared S,
+                                                            const unsigned long long* __restrict__ B) {
+    const unsigned long long nc = S.ctr[1] < S.cand_cap ? S.ctr[1] : S.cand_cap;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < nc;
+         i += stride) {
+        const unsigned long long w0 = S.cand[2 * i], ey = S.cand[2 * i + 1];
+        const int sw = (int)(w0 >> 56);
+        const unsigned long long ex = w0 & ((1ull << 56) - 1);
+        const CollectLevelDesc& L = levels[sw - 1];
+        int c[kCollectMaxSize];
+        unsigned long long acc[kCollectMaxWords];
 #pragma unroll
-    for (int w = 0; w < kCollectMaxWords; ++w) acc[w] = 0ull;
-    auto xor_row = [&](int r) {
-        const unsigned long long* p = S.rows + (size_t)r * S.S64;
+        for (int w = 0; w < kCollectMaxWords; ++w) acc[w] = 0ull;
+        auto xor_row = [&](int r) {
+            const unsigned long long* p = S.rows + (size_t)r * S.S64;
+#pragma unroll
+            for (int w = 0; w < kCollectMaxWords; ++w)
+                if (w < S.S64) acc[w] ^= __ldg(p + w);
+        };
+        colex_unrank(B, ex, L.a, S.m, c);
+        for (int k = 0; k < L.a; ++k) xor_row(c[k]);
+        colex_unrank(B, ey, L.b, S.m, c);
+        for (int k = 0; k < L.b; ++k) xor_row(S.m - 1 - c[k]);
+        int wt = 0;
 #pragma unroll
         for (int w = 0; w < kCollectMaxWords; ++w)
-            if (w < S.S64) acc[w] ^= __ldg(p + w);
-    };
-    colex_unrank(B, ex, L.a, S.m, c);
-    for (int i = 0; i < L.a; ++i) xor_row(c[i]);
-    colex_unrank(B, ey, L.b, S.m, c);
-    for (int i = 0; i < L.b; ++i) xor_row(S.m - 1 - c[i]);
-    int wt = 0;
+            if (w < S.S64) wt += __popcll(acc[w]);
+        if (wt < 1 || wt > S.keep) continue;
+        const unsigned long long slot = atomicAdd(S.ctr, 1ull);
+        if (slot >= S.cap) continue;
+        unsigned long long* o = S.out + slot * (unsigned long long)S.S64;
 #pragma unroll
-    for (int w = 0; w < kCollectMaxWords; ++w)
-        if (w < S.S64) wt += __popcll(acc[w]);
-    if (wt < 1 || wt > S.keep) return;
-    const unsigned long long slot = atomicAdd(S.ctr, 1ull);
-    if (slot >= S.cap) return;
-    unsigned long long* o = S.out + slot * (unsigned long long)S.S64;
-#pragma unroll
-    for (int w = 0; w < kCollectMaxWords; ++w)
-        if (w < S.S64) o[w] = acc[w];
+        for (int w = 0; w < kCollectMaxWords; ++w)
+            if (w < S.S64) o[w] = acc[w];
+    }
 }
 
 // One warp per job (a 256-entry prefix tile of one term against up to kCollectChunkY
-// suffix entries), jobs handed out by a per-level counter.
+// suffix entries), jobs handed out by a per-level counter.  A pair whose bound is under
+// keep + 1 is appended to the candidates (rare: the probe filter is sized for it).
 template <int HP, int FILT>
 __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDesc* __restrict__ levels,
                                                             int level, CollectShared S,
                                                             const unsigned long long* __restrict__ B) {
     const CollectLevelDesc& L = levels[level];
     const int lane = threadIdx.x & 31;
-    unsigned long long passes = 0;
     for (;;) {
         unsigned long long job = 0;
         if (lane == 0) job = atomicAdd(S.job_ctr + level, 1ull);
@@ -213,28 +221,42 @@ __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDe
         const unsigned long long y0 = yc * kCollectChunkY;
         const unsigned long long y1 = T.ny < y0 + kCollectChunkY ? T.ny : y0 + kCollectChunkY;
         const int lim = S.keep;
-        for (unsigned long long y = y0; y < y1; ++y) {
-            uint32_t yv[HP];
-            load_probe<HP>(L.yp + y * HP, yv);
-            const int ypc = __ldg(L.ypc + y);
+        // the suffix entry of the next iteration is loaded one iteration ahead (the last
+        // iteration reloads its own entry), so its latency hides behind eight pairs
+        const int cnt = (int)(y1 - y0);
+        const uint32_t* yp = L.yp + y0 * HP;
+        const uint8_t* yq = L.ypc + y0;
+        uint32_t ya[HP];
+        load_probe<HP>(yp, ya);
+        int pa = __ldg(yq);
+        for (int k = 0; k < cnt; ++k) {
+            const int kn = k + 1 < cnt ? k + 1 : k;
+            uint32_t yb[HP];
+            load_probe<HP>(yp + (size_t)kn * HP, yb);
+            const int pb = __ldg(yq + kn);
             int v[kCRX];
 #pragma unroll
-            for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_bound<HP, FILT>(xv[i], yv);
+            for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_bound<HP, FILT>(xv[i], ya);
             int mn = __vimin3_s32(v[0], v[1], v[2]);
             mn = __vimin3_s32(mn, v[3], v[4]);
             mn = __vimin3_s32(mn, v[5], v[6]);
             mn = min(mn, v[7]);
-            if (mn + ypc <= lim) {
+            if (mn + pa <= lim) {
 #pragma unroll 1
                 for (int i = 0; i < kCRX; ++i) {
-                    if (v[i] + ypc > lim) continue;
-                    ++passes;
-                    collect_exact(S, L, B, T.x0 + xoff + (unsigned long long)(i * 32 + lane), y);
+                    if (v[i] + pa > lim) continue;
+                    const unsigned long long slot = atomicAdd(S.ctr + 1, 1ull);
+                    if (slot >= S.cand_cap) continue;
+                    S.cand[2 * slot] = (T.x0 + xoff + (unsigned long long)(i * 32 + lane)) |
+                                       ((unsigned long long)(level + 1) << 56);
+                    S.cand[2 * slot + 1] = y0 + (unsigned long long)k;
                 }
             }
+#pragma unroll
+            for (int h = 0; h < HP; ++h) ya[h] = yb[h];
+            pa = pb;
         }
     }
-    if (passes) atomicAdd(S.ctr + 1, passes);
 }
 
 }  // namespace dev
@@ -250,16 +272,27 @@ cudaError_t launch_collect_gen(const CollectListDesc* d_lists, int nlists, unsig
     return cudaGetLastError();
 }
 
+cudaError_t launch_collect_exact(const CollectLevelDesc* d_levels, const CollectShared& S,
+                                 const unsigned long long* d_binom, int num_sms, cudaStream_t st) {
+    dev::collect_exact_kernel<<<num_sms * 4, 256, 0, st>>>(d_levels, S, d_binom);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_collect_pairs(const CollectLevelDesc* d_levels, int level,
                                  unsigned long long jobs, const CollectShared& S,
                                  const unsigned long long* d_binom, int num_sms,
                                  cudaStream_t st) {
     if (jobs == 0) return cudaSuccess;
+    // as many blocks as fit on the device at once (jobs are handed out dynamically)
     const unsigned long long want = (jobs + 3) / 4;   // four warps per block
-    const unsigned long long cap = (unsigned long long)num_sms * 8;
-    const unsigned int grid = (unsigned int)(want < cap ? want : cap);
 #define QSFB_COLLECT_CASE(H, F)                                                              \
     if (S.HP == H && S.filt == F) {                                                          \
+        static int per_sm = 0;                                                               \
+        if (per_sm == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(                    \
+                               &per_sm, dev::collect_pairs_kernel<H, F>, 128, 0) != cudaSuccess) \
+            return cudaGetLastError();                                                       \
+        const unsigned long long cap = (unsigned long long)num_sms * (per_sm > 0 ? per_sm : 1); \
+        const unsigned int grid = (unsigned int)(want < cap ? want : cap);                   \
         dev::collect_pairs_kernel<H, F><<<grid, 128, 0, st>>>(d_levels, level, S, d_binom);  \
         return cudaGetLastError();                                                           \
     }

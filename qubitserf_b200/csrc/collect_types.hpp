@@ -13,7 +13,8 @@
 // own a private column).  A row's private column is a column whose only 1 is in that row;
 // a subset sets it exactly when the row is in the subset, so
 //     weight(S) >= pivots(S) + popc(probe(S)),
-// which is the sweep's filter; pairs under keep + 1 are re-evaluated over the full rows.
+// which is the sweep's filter; the pairs under keep + 1 become candidates that a second
+// kernel re-evaluates over the full rows.
 #pragma once
 #include <cstdint>
 
@@ -63,9 +64,11 @@ struct CollectShared {
     const uint8_t* piv;           // m: 1 if the row owns a private column
     const unsigned long long* rows;   // m x S64 full rows (the caller's column order)
     unsigned long long* out;      // cap x S64 collected codewords
-    unsigned long long* ctr;      // [0] hits (counted past cap), [1] pairs passing the filter
+    unsigned long long* cand;     // cand_cap x 2: pairs that passed the filter
+                                  //   [0] prefix entry | subset size << 56, [1] suffix entry
+    unsigned long long* ctr;      // [0] hits, [1] candidates (both counted past capacity)
     unsigned long long* job_ctr;  // one dynamic job counter per level
-    unsigned long long cap;
+    unsigned long long cap, cand_cap;
     int m, S64, HP, keep;
     int filt;                     // probe_bound variant (collect.cu): 0 exact, 2/4 OR, 6 CSA
 };

@@ -199,3 +199,16 @@ def collect_generator(n: int = 128, k: int = 64, seed: int = 13):
     A = rng.integers(0, 2, size=(k, n - k), dtype=np.uint8)
     G = np.concatenate([np.eye(k, dtype=np.uint8), A], axis=1)
     return np.ascontiguousarray(G[:, rng.permutation(n)])
+
+
+def toric_code(L: int):
+    """(Hx, Hz) of the [[2 L^2, 2, L]] toric code: the hypergraph product of the L x L check
+    matrix of the cyclic repetition code with itself (edges of an L x L torus; X checks on
+    vertices, Z checks on faces)."""
+    H = np.zeros((L, L), dtype=np.uint8)
+    for i in range(L):
+        H[i, i] = H[i, (i + 1) % L] = 1
+    I = np.eye(L, dtype=np.uint8)
+    Hx = np.concatenate([np.kron(H, I), np.kron(I, H.T)], axis=1) % 2
+    Hz = np.concatenate([np.kron(I, H), np.kron(H.T, I)], axis=1) % 2
+    return Hx.astype(np.uint8), Hz.astype(np.uint8)

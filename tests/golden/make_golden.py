@@ -11,7 +11,11 @@ Runs only where the reference CPU library has been built from its sources
     python tests/golden/make_golden.py              # golden.npz + golden.json
     python tests/golden/make_golden.py --batch1024  # batch1024.json (all 1024 batch codes)
     python tests/golden/make_golden.py --collect    # collect.npz (codeaut low-weight collector)
+    python tests/golden/make_golden.py --mitm       # mitm.json (method "mitm" on the golden codes)
 
+* mitm.json    -- per golden case small enough for the reference's meet-in-the-middle on the
+                  host: its [distance, lower_bound, proven, levels] with method "mitm"
+                  ([z_weight, x_weight, proven] for operator weights)
 * collect.npz  -- per case `<name>__G` (the generator rows), `<name>__meta` (p, keep, combos,
                   count, n) and `<name>__rows` (the reference's collected rows, bit-packed
                   with numpy.packbits along each row), from the reference's own
@@ -211,8 +215,52 @@ def collect_goldens():
     np.savez_compressed(HERE / "collect.npz", **arrays)
 
 
+def mitm_goldens(max_parts=3e7):
+    """The reference's own method "mitm" on every golden case whose meet-in-the-middle
+    search stays small (parts of the larger half up to its BZ distance)."""
+    from math import comb
+    from oracle.refbind import Ref
+    ref = Ref()
+    results = json.loads((HERE / "golden.json").read_text())
+    arrays = np.load(HERE / "golden.npz")
+    out = {}
+    for name, res in sorted(results.items()):
+        mats = tuple(arrays[f"{name}__{i}"] for i in range(res["nmats"]))
+        kind = res["kind"]
+        n = mats[0].shape[1]
+        sym = kind == "stabilizer"
+        coords = n // 2 if sym else n
+        d = res.get("distance")
+        if kind == "opweight":
+            d = max(res["z_weight"], res["x_weight"])
+        half = coords - coords // 2
+        parts = sum(comb(half, w) * (3 ** w if sym else 1) for w in range(0, d + 1))
+        if d is None or d < 0 or parts > max_parts:
+            continue
+        if kind == "classical":
+            r = ref.classical(mats[0], method="mitm")
+        elif kind == "css":
+            r = ref.css(mats[0], mats[1], res.get("which", "M"), method="mitm")
+        elif kind == "subsystem":
+            r = ref.subsystem(mats[0], mats[1], res.get("which", "M"), method="mitm")
+        elif kind == "stabilizer":
+            rc, r = ref.stabilizer(mats[0], res.get("which", "M"), method="mitm")
+            assert rc == 0
+        else:
+            r = ref.operator_weight(*mats, method="mitm")
+            out[name] = [int(r.z_weight), int(r.x_weight), int(r.proven)]
+            print(name, out[name], flush=True)
+            continue
+        out[name] = [int(r.distance), int(r.lower_bound), int(r.proven), int(r.levels)]
+        print(name, out[name], flush=True)
+    (HERE / "mitm.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+
+
 def main():
     sys.path.insert(0, str(ROOT))
+    if "--mitm" in sys.argv:
+        mitm_goldens()
+        return
     if "--batch1024" in sys.argv:
         batch1024()
         return

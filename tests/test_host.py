@@ -154,14 +154,24 @@ def test_matroid_partition_cases_bit_exact(native, ref):
 
 def test_dispatch_rules_without_device(native, golden):
     """No CPU path: without an sm_100 device every distance call fails with rc 4, and the
-    unsupported methods/backends with rc 5, before touching any device."""
+    unsupported methods/backends with rc 5, before touching any device.  Method "cc" is
+    unsupported where the reference runs its connected-cluster solver (CSS, subsystem); the
+    classical path maps it to BZ, as the reference does."""
     lib = native.lib()
     H = golden.mats("hamming3")[0]
     a = native.as_u8(H)
     out = native.DistfindResult()
     p = a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
-    assert lib.distfind_classical_distance(p, a.shape[0], a.shape[1], b"mitm", b"gpu", 0, 0,
-                                           ctypes.byref(out)) == 5
+    hx, hz = (native.as_u8(m) for m in golden.mats("steane"))
+    px = hx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    pz = hz.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    for which in (b"Z", b"M"):
+        assert lib.distfind_css_distance(px, hx.shape[0], hx.shape[1], pz, hz.shape[0],
+                                         hz.shape[1], b"cc", which, b"gpu", 0, 0,
+                                         ctypes.byref(out)) == 5
+        assert lib.distfind_subsystem_distance(px, hx.shape[0], hx.shape[1], pz, hz.shape[0],
+                                               hz.shape[1], b"cc", which, b"gpu", 0, 0,
+                                               ctypes.byref(out)) == 5
     assert lib.distfind_classical_distance(p, a.shape[0], a.shape[1], b"bz", b"cpu", 0, 0,
                                            ctypes.byref(out)) == 5
     assert lib.distfind_classical_distance(None, 1, 1, b"bz", b"gpu", 0, 0,
@@ -172,9 +182,10 @@ def test_dispatch_rules_without_device(native, golden):
         ctypes.byref(out)) == 2
     if lib.qsfb_device_sms() == 0:
         assert lib.distfind_backend_available(b"gpu") == 0
-        rc = lib.distfind_classical_distance(p, a.shape[0], a.shape[1], b"bz", b"gpu", 0, 0,
-                                             ctypes.byref(out))
-        assert rc == 4
+        for method in (b"bz", b"mitm", b"cc"):
+            rc = lib.distfind_classical_distance(p, a.shape[0], a.shape[1], method, b"gpu", 0,
+                                                 0, ctypes.byref(out))
+            assert rc == 4
         with pytest.raises(RuntimeError):
             native.classical_distance_raw(H, "bz", "auto", 0, False)
     assert lib.distfind_backend_available(b"cpu") == 0

@@ -165,3 +165,59 @@ def test_collect_oracle_matches_reference_random(orc, ref):
         a, ca = ref.collect(G, p, keep)
         b, cb = orc.collect(G, p, keep)
         assert ca == cb and np.array_equal(a, b), (trial, m, n, p, keep)
+
+
+def mitm_case(engine, kind, mats, res, **kw):
+    """(distance, lower_bound, proven, levels) of method "mitm" on a golden case, or
+    (z_weight, x_weight, proven) for an operator weight, from the oracle or the reference."""
+    which = res.get("which", "M")
+    if kind == "classical":
+        r = engine.classical(mats[0], method="mitm", **kw)
+    elif kind == "css":
+        r = engine.css(mats[0], mats[1], which, method="mitm", **kw)
+    elif kind == "subsystem":
+        r = engine.subsystem(mats[0], mats[1], which, method="mitm", **kw)
+    elif kind == "stabilizer":
+        r = engine.stabilizer(mats[0], which, method="mitm", **kw)
+        r = r[1] if isinstance(r, tuple) else r
+    else:
+        r = engine.operator_weight(*mats, method="mitm", **kw)
+        if isinstance(r, tuple):
+            return [int(r[0]), int(r[1])]
+        return [int(r.z_weight), int(r.x_weight)]
+    return [int(r.distance), int(r.lower_bound), int(r.proven), int(r.levels)]
+
+
+def test_mitm_oracle_matches_golden(golden, orc):
+    import json
+    from conftest import GOLDEN_DIR
+    want = json.loads((GOLDEN_DIR / "mitm.json").read_text())
+    assert len(want) >= 40
+    for name, exp in want.items():
+        res = golden.results[name]
+        got = mitm_case(orc, res["kind"], golden.mats(name), res)
+        assert got == exp[:len(got)], (name, got, exp)
+
+
+def test_mitm_oracle_matches_reference_random(orc, ref):
+    if ref is None:
+        pytest.skip("oracle/_ref not built")
+    import codes as C
+    from qubitserf_b200 import workloads as W
+    rng = np.random.default_rng(31)
+    for trial in range(12):
+        n = int(rng.integers(10, 34))
+        Hx, Hz = W.css_from_rng(rng, n, int(rng.integers(2, n // 3 + 1)),
+                                int(rng.integers(2, n // 3 + 1)))
+        for which in "ZXM":
+            a = ref.css(Hx, Hz, which, method="mitm")
+            b = orc.css(Hx, Hz, which, method="mitm")
+            assert (a.distance, a.lower_bound, a.proven, a.levels) == \
+                   (b.distance, b.lower_bound, b.proven, b.levels), (trial, which)
+    for trial in range(8):
+        S = C.random_isotropic(rng, int(rng.integers(5, 10)), int(rng.integers(2, 5)))
+        rc, a = ref.stabilizer(S, "M", method="mitm")
+        b = orc.stabilizer(S, "M", method="mitm")
+        assert rc == 0
+        assert (a.distance, a.lower_bound, a.proven, a.levels) == \
+               (b.distance, b.lower_bound, b.proven, b.levels), trial
