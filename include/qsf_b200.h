@@ -4,14 +4,17 @@
  * signatures, struct layouts and return codes of the reference's
  * cpp/distfind/capi.h:12-111 (Quantinuum/Qubitserf), which its Python layer binds with
  * ctypes (python/qubitserf/distfind/_native.py:15-107).  Pointing QUBITSERF_LIB at this
- * library makes the unchanged reference Python call it.  Only method "bz" on backend
- * "gpu"/"auto" runs here; there is no CPU fallback.
+ * library makes the unchanged reference Python call it.  Methods "bz" (Brouwer-Zimmermann)
+ * and "mitm" (meet in the middle) run on backend "gpu"/"auto", with the reference's
+ * method dispatch (any other name is BZ; "cc" falls back where the reference falls back);
+ * there is no CPU fallback.
  *
  * Return codes: 0 ok; 1 null pointer; 2 not a [z|x] matrix / bad operator length;
  * 3 method "cc" on a non-CSS code (the reference's own codes, capi.cpp:152-404);
  * 4 no usable sm_100 device or a CUDA error; 5 method/backend/size this engine does not
- * run (e.g. "mitm", "cc", backend "cpu", n > 1024 after pivot removal); 6 device memory
- * exhausted.  Codes 4-6 surface in the reference Python as RuntimeError.
+ * run (method "cc" where the reference runs its connected-cluster solver, backend "cpu",
+ * n > 1024 after pivot removal); 6 device memory exhausted.  Codes 4-6 surface in the
+ * reference Python as RuntimeError.
  *
  * Part 2 (qsfb_*) adds what the reference has no ABI for: the per-level enumeration on a
  * raw plan, the host problem reduction, the witness and per-level counts of the last
