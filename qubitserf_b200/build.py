@@ -18,6 +18,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libqsfb200.so"
+CLI_SRC = PKG / "cli" / "distfind_cli.cpp"
+CLI = PKG / "qsfb-distfind"
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -69,7 +71,21 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         cmd = [NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"]
         _compile(cmd)
         shutil.move(str(tmp), str(LIB))
+    build_cli(force)
     return LIB
+
+
+def build_cli(force: bool = False) -> Path:
+    """The qsfb-distfind command line: a thin executable over the library's C ABI (found
+    next to it through an $ORIGIN run path)."""
+    if not force and CLI.exists() and CLI.stat().st_mtime > max(CLI_SRC.stat().st_mtime,
+                                                                LIB.stat().st_mtime):
+        return CLI
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", "-Wextra",
+           f"-I{ROOT / 'include'}", str(CLI_SRC), "-o", str(CLI), f"-L{PKG}", "-lqsfb200",
+           "-Wl,-rpath,$ORIGIN"]
+    _compile(cmd)
+    return CLI
 
 
 if __name__ == "__main__":

@@ -216,3 +216,49 @@ def test_workloads_are_deterministic():
     assert W.gf2_rank(Hx) == 40 and W.gf2_rank(Hz) == 40
     b = W.batch_1024(8)
     assert [c.kind for c in b] == ["classical"] * 4 + ["css"] * 4
+
+
+def _cli(args, stdin=""):
+    exe = ROOT / "qubitserf_b200" / "qsfb-distfind"
+    p = subprocess.run([str(exe), *args], input=stdin, capture_output=True, text=True,
+                       timeout=120)
+    return p.returncode, p.stdout, p.stderr
+
+
+def test_cli_usage_errors_exit_2(tmp_path):
+    """qsfb-distfind keeps the reference CLI's input rules (cpp/distfind/cli/
+    distfind_cli.cpp:100-433): usage errors exit 2 with a message on stderr, before any
+    device work."""
+    rc, out, _ = _cli(["--help"])
+    assert rc == 0 and out.startswith("Usage: qsfb-distfind")
+    for args, stdin, msg in [
+        (["--frobnicate"], "", "unrecognised argument"),
+        (["--zx", "--z"], "XXI\n", "--zx cannot be combined"),
+        (["--hx", "a.txt"], "", "--hx and --hz must be given together"),
+        ([], "", "no stabilisers on stdin"),
+        ([], "XXZ\n", "mixes X and Z"),
+        ([], "XYI\n", "contains a Y"),
+        ([], "XXI\nZZ\n", "differing lengths"),
+        ([], "XQI\n", "unrecognised character"),
+        (["-o", "XX"], "XXI\n", "operator length"),
+        (["--threads", "x"], "", "non-negative integer"),
+    ]:
+        rc, out, err = _cli(args, stdin)
+        assert rc == 2 and msg in err and out == "", (args, err)
+    bad = tmp_path / "ragged.txt"
+    bad.write_text("1 0 1\n0 1\n")
+    good = tmp_path / "good.txt"
+    good.write_text("1 1 0\n")
+    rc, _, err = _cli(["--hx", str(bad), "--hz", str(good)])
+    assert rc == 2 and "ragged matrix" in err
+    two = tmp_path / "two.txt"
+    two.write_text("1 2 0\n")
+    rc, _, err = _cli(["--hx", str(two), "--hz", str(good)])
+    assert rc == 2 and "non-binary token" in err
+
+
+def test_cli_without_device_fails_cleanly(native):
+    if native.lib().qsfb_device_sms() != 0:
+        pytest.skip("a device is present")
+    rc, out, err = _cli([], "XXXXIII\nZZZZIII\n")
+    assert rc == 1 and out == "" and "rc=4" in err
