@@ -92,11 +92,11 @@ def test_collect_overflow_reruns_with_exact_capacity(native, orc):
     assert np.array_equal(got, want)
     # a full-rank G gives distinct XORs for distinct subsets: nothing was dropped
     assert got.shape[0] == combos and st.hits == combos
-    # 21 rows: 1,097,970 candidate pairs, over the first candidate buffer as well: the
-    # sweeps run again into enough candidate slots, then the hits into enough rows
-    G = rng.integers(0, 2, size=(21, 40), dtype=np.uint8)
-    got, combos, st = native.collect(G, 10, 40, stats=True)
-    want, want_combos = orc.collect(G, 10, 40)
+    # 22 rows, p = 9: 1,097,789 candidate pairs, over the first candidate buffer (2^20) as
+    # well: the sweeps run again into enough candidate slots, then the hits into enough rows
+    G = rng.integers(0, 2, size=(22, 40), dtype=np.uint8)
+    got, combos, st = native.collect(G, 9, 40, stats=True)
+    want, want_combos = orc.collect(G, 9, 40)
     assert st.reruns == 2 and st.passes == combos == want_combos
     assert np.array_equal(got, want)
 
