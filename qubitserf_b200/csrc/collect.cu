@@ -92,6 +92,23 @@ __global__ void __launch_bounds__(256) collect_gen_kernel(const CollectListDesc*
 }
 
 // ---------------------------------------------------------------- pair sweep
+// HP probe words of one staged suffix entry (16-byte aligned for HP >= 4, 8 for HP = 2).
+template <int HP>
+__device__ __forceinline__ void stage_probe(const uint32_t* p, uint32_t (&v)[HP]) {
+    if constexpr (HP >= 4) {
+#pragma unroll
+        for (int h = 0; h < HP; h += 4) {
+            const uint4 a = *reinterpret_cast<const uint4*>(p + h);
+            v[h] = a.x; v[h + 1] = a.y; v[h + 2] = a.z; v[h + 3] = a.w;
+        }
+    } else if constexpr (HP == 2) {
+        const uint2 a = *reinterpret_cast<const uint2*>(p);
+        v[0] = a.x; v[1] = a.y;
+    } else {
+        v[0] = p[0];
+    }
+}
+
 template <int HP>
 __device__ __forceinline__ void load_probe(const uint32_t* __restrict__ p, uint32_t (&v)[HP]) {
     if constexpr (HP == 8) {
@@ -181,14 +198,19 @@ __global__ void __launch_bounds__(256) collect_exact_kernel(const CollectLevelDe
 }
 
 // One warp per job (a 256-entry prefix tile of one term against up to kCollectChunkY
-// suffix entries), jobs handed out by a per-level counter.  A pair whose bound is under
+// suffix entries, staged in the warp's slice of shared memory), jobs handed out by a
+// per-level counter; four warps per block.  A pair whose bound is under
 // keep + 1 is appended to the candidates (rare: the probe filter is sized for it).
 template <int HP, int FILT>
 __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDesc* __restrict__ levels,
                                                             int level, CollectShared S,
                                                             const unsigned long long* __restrict__ B) {
     const CollectLevelDesc& L = levels[level];
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ __align__(16) uint32_t ys_all[4][kCollectChunkY * HP];
+    __shared__ uint8_t yq_all[4][kCollectChunkY];
+    uint32_t* ys = ys_all[warp];
+    uint8_t* yq = yq_all[warp];
     for (;;) {
         unsigned long long job = 0;
         if (lane == 0) job = atomicAdd(S.job_ctr + level, 1ull);
@@ -220,20 +242,24 @@ __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDe
         }
         const unsigned long long y0 = yc * kCollectChunkY;
         const unsigned long long y1 = T.ny < y0 + kCollectChunkY ? T.ny : y0 + kCollectChunkY;
-        const int lim = S.keep;
-        // the suffix entry of the next iteration is loaded one iteration ahead (the last
-        // iteration reloads its own entry), so its latency hides behind eight pairs
         const int cnt = (int)(y1 - y0);
-        const uint32_t* yp = L.yp + y0 * HP;
-        const uint8_t* yq = L.ypc + y0;
-        uint32_t ya[HP];
-        load_probe<HP>(yp, ya);
-        int pa = __ldg(yq);
+        const int lim = S.keep;
+        // the job's suffix entries go to this warp's shared-memory stage (coalesced), and the
+        // pair loop reads them back as broadcasts
+        __syncwarp();   // every lane is done with the previous job's stage
+        for (int e = lane; e < cnt; e += 32) {
+            uint32_t v[HP];
+            load_probe<HP>(L.yp + (y0 + (unsigned long long)e) * HP, v);
+#pragma unroll
+            for (int h = 0; h < HP; ++h) ys[e * HP + h] = v[h];
+            yq[e] = __ldg(L.ypc + y0 + e);
+        }
+        __syncwarp();
+#pragma unroll 2
         for (int k = 0; k < cnt; ++k) {
-            const int kn = k + 1 < cnt ? k + 1 : k;
-            uint32_t yb[HP];
-            load_probe<HP>(yp + (size_t)kn * HP, yb);
-            const int pb = __ldg(yq + kn);
+            uint32_t ya[HP];
+            stage_probe<HP>(ys + k * HP, ya);
+            const int pa = yq[k];
             int v[kCRX];
 #pragma unroll
             for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_bound<HP, FILT>(xv[i], ya);
@@ -252,9 +278,6 @@ __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDe
                     S.cand[2 * slot + 1] = y0 + (unsigned long long)k;
                 }
             }
-#pragma unroll
-            for (int h = 0; h < HP; ++h) ya[h] = yb[h];
-            pa = pb;
         }
     }
 }

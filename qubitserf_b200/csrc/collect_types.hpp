@@ -24,7 +24,7 @@ constexpr int kCollectMaxProbe = 8;     // probe words per entry (1, 2, 4 or 8)
 constexpr int kCollectMaxWords = 16;    // 64-bit words per codeword: n <= 1024
 constexpr int kCollectMaxSize = 64;     // subset size (binomial table columns)
 constexpr int kCollectTileX = 256;      // prefix entries per warp job (32 lanes x 8)
-constexpr int kCollectChunkY = 512;     // suffix entries per warp job
+constexpr int kCollectChunkY = 256;     // suffix entries per warp job (staged in shared memory)
 
 // One list: `count` entries of `size`-subsets of [0, m), colex (reflect = 0) or reflected
 // colex (rows m - 1 - c, reflect = 1).  `run_base` numbers the runs of kGenRun entries of
