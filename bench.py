@@ -458,6 +458,9 @@ def bench_collect(args, rank, world, local, pg):
     S64 = (c["n"] + 63) // 64
     alg_popc = 2 * S64            # POPC32 per combination of the full evaluation
     achieved = combos * alg_popc / pairs_s
+    # POPC32 the sweep issues per pair: the exact sum over its probe words, one for the OR
+    # bounds, two for the carry-save bound
+    issued = {0: st.probe_words, 2: 1, 4: 1, 6: 2}[st.filter]
     cpu = None if args.no_cpu_baseline else collect_reference_sample(G, c["sample_p"], c["keep"])
     print(json.dumps({
         "metric": COLLECT_METRIC, "value": value, "unit": "combos/s", "n_gpus": world,
@@ -470,8 +473,9 @@ def bench_collect(args, rank, world, local, pg):
                      "frac": achieved / popc_peak, "traffic": None,
                      "numerator": f"combinations/s of the pair sweeps x {alg_popc} POPC32 of "
                                   "the full evaluation (2 per 64-bit word); the kernel issues "
-                                  f"{st.probe_words} per pair on its probe words",
-                     "kernel_frac": combos * st.probe_words / pairs_s / popc_peak,
+                                  f"{issued} per pair (probe bound {st.filter} over "
+                                  f"{st.probe_words} words)",
+                     "kernel_frac": combos * issued / pairs_s / popc_peak,
                      "peak_source": "measured: qsfb_microbench POPC chains over all SMs",
                      "pass_rate": passes / max(combos * args.steps, 1),
                      "gen_ms": st.gen_ms, "pairs_ms": st.pairs_ms},

@@ -197,6 +197,47 @@ __global__ void __launch_bounds__(256) collect_exact_kernel(const CollectLevelDe
     }
 }
 
+// The probe words of four consecutive staged entries (16-byte aligned: k is a multiple of 4).
+template <int HP>
+__device__ __forceinline__ void stage_group(const uint32_t* p, uint32_t (&v)[4][HP]) {
+    if constexpr (HP == 1) {
+        const uint4 a = *reinterpret_cast<const uint4*>(p);
+        v[0][0] = a.x; v[1][0] = a.y; v[2][0] = a.z; v[3][0] = a.w;
+    } else {
+#pragma unroll
+        for (int g = 0; g < 4; ++g) stage_probe<HP>(p + g * HP, v[g]);
+    }
+}
+
+// The lane's eight prefix entries against one suffix entry: a bound per pair, one minimum,
+// and for the rare pairs under keep + 1 an appended candidate.
+template <int HP, int FILT>
+__device__ __forceinline__ void pair_step(const CollectShared& S, const CollectTerm& T,
+                                          const uint32_t (&xv)[kCRX][HP], const int (&xpc)[kCRX],
+                                          const uint32_t (&ya)[HP], int pa, int lim, int level,
+                                          unsigned long long xoff, int lane,
+                                          unsigned long long ey) {
+    int v[kCRX];
+#pragma unroll
+    for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_bound<HP, FILT>(xv[i], ya);
+    int mn = __vimin3_s32(v[0], v[1], v[2]);
+    mn = __vimin3_s32(mn, v[3], v[4]);
+    mn = __vimin3_s32(mn, v[5], v[6]);
+    mn = min(mn, v[7]);
+    if (mn + pa <= lim) {
+        // unrolled: a run-time index into v[] would move it to local memory for every step
+#pragma unroll
+        for (int i = 0; i < kCRX; ++i) {
+            if (v[i] + pa > lim) continue;
+            const unsigned long long slot = atomicAdd(S.ctr + 1, 1ull);
+            if (slot >= S.cand_cap) continue;
+            S.cand[2 * slot] = (T.x0 + xoff + (unsigned long long)(i * 32 + lane)) |
+                               ((unsigned long long)(level + 1) << 56);
+            S.cand[2 * slot + 1] = ey;
+        }
+    }
+}
+
 // One warp per job (a 256-entry prefix tile of one term against up to kCollectChunkY
 // suffix entries, staged in the warp's slice of shared memory), jobs handed out by a
 // per-level counter; four warps per block.  A pair whose bound is under
@@ -208,7 +249,7 @@ __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDe
     const CollectLevelDesc& L = levels[level];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __shared__ __align__(16) uint32_t ys_all[4][kCollectChunkY * HP];
-    __shared__ uint8_t yq_all[4][kCollectChunkY];
+    __shared__ __align__(16) uint8_t yq_all[4][kCollectChunkY];
     uint32_t* ys = ys_all[warp];
     uint8_t* yq = yq_all[warp];
     for (;;) {
@@ -255,29 +296,23 @@ __global__ void __launch_bounds__(128) collect_pairs_kernel(const CollectLevelDe
             yq[e] = __ldg(L.ypc + y0 + e);
         }
         __syncwarp();
-#pragma unroll 2
-        for (int k = 0; k < cnt; ++k) {
+        // four staged entries per step: their probe words in 16-byte loads and their pivot
+        // counts in one 32-bit word; the ragged end of the chunk goes one entry at a time
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            uint32_t yv[4][HP];
+            stage_group<HP>(ys + k * HP, yv);
+            const uint32_t pcs = *reinterpret_cast<const uint32_t*>(yq + k);
+#pragma unroll
+            for (int g = 0; g < 4; ++g)
+                pair_step<HP, FILT>(S, T, xv, xpc, yv[g], (int)((pcs >> (8 * g)) & 0xffu), lim,
+                                    level, xoff, lane, y0 + (unsigned long long)(k + g));
+        }
+        for (; k < cnt; ++k) {
             uint32_t ya[HP];
             stage_probe<HP>(ys + k * HP, ya);
-            const int pa = yq[k];
-            int v[kCRX];
-#pragma unroll
-            for (int i = 0; i < kCRX; ++i) v[i] = xpc[i] + probe_bound<HP, FILT>(xv[i], ya);
-            int mn = __vimin3_s32(v[0], v[1], v[2]);
-            mn = __vimin3_s32(mn, v[3], v[4]);
-            mn = __vimin3_s32(mn, v[5], v[6]);
-            mn = min(mn, v[7]);
-            if (mn + pa <= lim) {
-#pragma unroll 1
-                for (int i = 0; i < kCRX; ++i) {
-                    if (v[i] + pa > lim) continue;
-                    const unsigned long long slot = atomicAdd(S.ctr + 1, 1ull);
-                    if (slot >= S.cand_cap) continue;
-                    S.cand[2 * slot] = (T.x0 + xoff + (unsigned long long)(i * 32 + lane)) |
-                                       ((unsigned long long)(level + 1) << 56);
-                    S.cand[2 * slot + 1] = y0 + (unsigned long long)k;
-                }
-            }
+            pair_step<HP, FILT>(S, T, xv, xpc, ya, (int)yq[k], lim, level, xoff, lane,
+                                y0 + (unsigned long long)k);
         }
     }
 }
