@@ -301,17 +301,21 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
                     for (int i = 0; i < RX; ++i) m[i] = fold_min<FILT>(x[i], y0, pcy, m[i]);
                 }
             }
-            bool any = false;
+            // entries whose chunk minimum reached the bound, as a bit mask: walking it keeps
+            // m[], thr[] and pcr[] indexed by constants only (a run-time index would move
+            // them to local memory, and m[] is updated for every loop entry)
+            uint32_t flagged = 0u;
 #pragma unroll
-            for (int i = 0; i < RX; ++i) any |= ZERO ? (m[i] == 0 && thr[i] > 0) : m[i] < thr[i];
-            if (any) {
-#pragma unroll 1
-                for (int i = 0; i < RX; ++i) {
-                    if (ZERO ? (m[i] == 0 && thr[i] > 0) : m[i] < thr[i]) {
-                        const unsigned long long e = reg0 + lane + 32 * i;
-                        T = survivor_scan(D, B, regX, xoff, e, pcr[i],
-                                          loop0 + (unsigned long long)c0, cn, T);
-                    }
+            for (int i = 0; i < RX; ++i)
+                flagged |= (ZERO ? (m[i] == 0 && thr[i] > 0) : m[i] < thr[i]) ? (1u << i) : 0u;
+            if (flagged) {
+                while (flagged) {
+                    const int i = __ffs(flagged) - 1;
+                    flagged &= flagged - 1u;
+                    const unsigned long long e = reg0 + lane + 32 * i;
+                    const int pc = FULL ? (regX ? D.a : D.b) : (int)regpc[e];
+                    T = survivor_scan(D, B, regX, xoff, e, pc, loop0 + (unsigned long long)c0,
+                                      cn, T);
                 }
 #pragma unroll
                 for (int i = 0; i < RX; ++i)
