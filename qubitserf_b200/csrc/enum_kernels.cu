@@ -32,12 +32,89 @@ constexpr int kChunk = 32;      // loop entries between survivor checks
 // One thread per run of kGenRun consecutive entries of a list: the first entry is unranked
 // (binary searches over the binomial table), the next ones follow by the colex successor
 // (raise the lowest element that can move, reset the ones below it), so the XOR of the
-// rows changes by the few rows that leave and enter -- usually one of each.
+// rows changes by the few rows that leave and enter -- usually one of each.  Lists over at
+// most 128 rows keep the subset as a bit mask in registers (gen_run_mask); longer ones
+// keep its elements in an array.
 __device__ __forceinline__ void xor_row(const GenDesc& D, int row, uint32_t (&acc)[4]) {
     const uint32_t* r = D.red + (size_t)row * D.W32;
 #pragma unroll
     for (int h = 0; h < 4; ++h)
         if (h < D.HP && h < D.W32) acc[h] ^= __ldg(r + h);
+}
+
+// Write entry e of list D: its probe words, pivot count and (where a tensor plan reads it)
+// its +-1 row.
+__device__ __forceinline__ void put_entry(const GenDesc& D, unsigned long long e,
+                                          const uint32_t (&acc)[4], int pc) {
+    uint32_t* o = D.out + e * (unsigned long long)D.HP;
+    if (D.HP == 4) {
+        *reinterpret_cast<uint4*>(o) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+    } else if (D.HP == 2) {
+        *reinterpret_cast<uint2*>(o) = make_uint2(acc[0], acc[1]);
+    } else {
+        o[0] = acc[0];
+    }
+    if (D.pc) D.pc[e] = (uint8_t)pc;
+    if (D.pm && e >= D.pm_lo && e < D.pm_hi)   // +-1 form of the rows a tensor plan reads
+        write_pm_row(D.pm, e, acc[0], acc[1], D.n_enc);
+}
+
+// Lists over K <= 128 rows: the subset is a 128-bit mask in registers.  Entry e0 is
+// unranked straight into the mask; the colex successor of a k-subset is the next larger
+// integer with the same popcount (add the lowest set bit, then move the bits that the carry
+// cleared back to the bottom), and the XOR of the rows changes by the bits that flip.
+__device__ __forceinline__ void gen_run_mask(const GenDesc& D, const unsigned long long* B,
+                                             unsigned long long e0, int n) {
+    typedef unsigned __int128 u128;
+    const int s = D.size, K = D.K;
+    u128 x = 0;
+    {
+        unsigned long long r = e0;
+        int hi = K;
+        for (int i = s; i >= 1; --i) {   // colex unrank, largest element first
+            int lo = i - 1, top = hi - 1;
+            while (lo < top) {
+                const int mid = (lo + top + 1) >> 1;
+                if (binom(B, mid, i) <= r) lo = mid; else top = mid - 1;
+            }
+            x |= (u128)1 << lo;
+            r -= binom(B, lo, i);
+            hi = lo;
+        }
+    }
+    // element v stands for row v (colex) or row K - 1 - v (reflected); pivot rows are < rank
+    u128 piv = 0;
+    if (D.rank > 0) {
+        const u128 low = D.rank >= 128 ? ~(u128)0 : (((u128)1 << D.rank) - 1);
+        piv = D.reflect ? (low << (K - D.rank)) : low;
+    }
+    auto flip = [&](u128 d, uint32_t (&acc)[4]) {
+        for (int half = 0; half < 2; ++half) {
+            unsigned long long w = (unsigned long long)(d >> (64 * half));
+            while (w) {
+                const int b = 64 * half + __ffsll((long long)w) - 1;
+                w &= w - 1;
+                xor_row(D, D.reflect ? K - 1 - b : b, acc);
+            }
+        }
+    };
+    auto popc128 = [](u128 v) {
+        return __popcll((unsigned long long)v) + __popcll((unsigned long long)(v >> 64));
+    };
+    uint32_t acc[4] = {0u, 0u, 0u, 0u};
+    flip(x, acc);
+    for (int j = 0; j < n; ++j) {
+        put_entry(D, e0 + j, acc, popc128(x & piv));
+        if (j + 1 == n) break;
+        const unsigned long long lo64 = (unsigned long long)x;
+        const int p = lo64 ? __ffsll((long long)lo64) - 1
+                           : 64 + __ffsll((long long)(unsigned long long)(x >> 64)) - 1;
+        const u128 v = x + ((u128)1 << p);
+        const u128 moved = (v ^ x);
+        const u128 next = v | (p + 2 < 128 ? (moved >> (p + 2)) : (u128)0);
+        flip(x ^ next, acc);
+        x = next;
+    }
 }
 
 __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restrict__ descs,
@@ -54,6 +131,10 @@ __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restric
         const GenDesc& D = descs[lo];
         const unsigned long long e0 = (gr - D.entry_base) * kGenRun;
         const int n = (int)(D.count - e0 < (unsigned long long)kGenRun ? D.count - e0 : kGenRun);
+        if (D.K <= 128) {
+            gen_run_mask(D, B, e0, n);
+            continue;
+        }
         const int s = D.size;
         // colex combination, ascending: c[0] < c[1] < ... < c[s-1]
         int c[kMaxW], top[kMaxW];
@@ -68,18 +149,7 @@ __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restric
             pc += r < D.rank;
         }
         for (int j = 0; j < n; ++j) {
-            const unsigned long long e = e0 + j;
-            uint32_t* o = D.out + e * (unsigned long long)D.HP;
-            if (D.HP == 4) {
-                *reinterpret_cast<uint4*>(o) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
-            } else if (D.HP == 2) {
-                *reinterpret_cast<uint2*>(o) = make_uint2(acc[0], acc[1]);
-            } else {
-                o[0] = acc[0];
-            }
-            if (D.pc) D.pc[e] = (uint8_t)pc;
-            if (D.pm && e >= D.pm_lo && e < D.pm_hi)   // +-1 form of the rows a tensor plan reads
-                write_pm_row(D.pm, e, acc[0], acc[1], D.n_enc);
+            put_entry(D, e0 + j, acc, pc);
             if (j + 1 == n) break;
             // colex successor: lowest t with c[t] + 1 < c[t+1] (c[s] = K)
             int t = 0;
