@@ -79,6 +79,70 @@ __device__ __forceinline__ unsigned long long syn_hash(const uint32_t (&syn)[kMi
     return h;
 }
 
+constexpr int kMitmRun = 8;   // consecutive parts per thread
+
+// Walk parts [id0, id0 + cnt) of weight w over coordinates [first, first + count), calling
+// f(syn, lg) for each.  Bit parts of a half of at most 64 coordinates keep the subset as a
+// 64-bit mask: the first is unranked into it, the next follow by the colex successor (the
+// next integer of the same popcount) and only the columns of the bits that flip are XORed
+// in.  Other parts (symplectic, or wider halves) are unranked one by one.
+template <class F>
+__device__ __forceinline__ void for_run(const MitmShared& S, const unsigned long long* B,
+                                        unsigned long long id0, int cnt, int first, int count,
+                                        int w, unsigned long long pw3, F&& f) {
+    uint32_t syn[kMitmMaxSynWords], lg[kMitmMaxLogWords];
+    if (S.sym || count > 64) {
+        for (int j = 0; j < cnt; ++j) {
+            part_words(S, B, id0 + j, first, count, w, pw3, syn, lg);
+            f(syn, lg);
+        }
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < kMitmMaxSynWords; ++k) syn[k] = 0u;
+#pragma unroll
+    for (int k = 0; k < kMitmMaxLogWords; ++k) lg[k] = 0u;
+    unsigned long long x = 0ull;
+    {
+        unsigned long long r = id0;
+        int hi = count;
+        for (int i = w; i >= 1; --i) {   // colex unrank, largest element first
+            int lo = i - 1, top = hi - 1;
+            while (lo < top) {
+                const int mid = (lo + top + 1) >> 1;
+                if (binom(B, mid, i) <= r) lo = mid; else top = mid - 1;
+            }
+            x |= 1ull << lo;
+            r -= binom(B, lo, i);
+            hi = lo;
+        }
+    }
+    auto flip = [&](unsigned long long d) {
+        while (d) {
+            const int b = __ffsll((long long)d) - 1;
+            d &= d - 1;
+            const uint32_t* sp = S.syn_cols + (size_t)(first + b) * S.SW;
+#pragma unroll
+            for (int k = 0; k < kMitmMaxSynWords; ++k)
+                if (k < S.SW) syn[k] ^= __ldg(sp + k);
+            const uint32_t* lp = S.log_cols + (size_t)(first + b) * S.LW;
+#pragma unroll
+            for (int k = 0; k < kMitmMaxLogWords; ++k)
+                if (k < S.LW) lg[k] ^= __ldg(lp + k);
+        }
+    };
+    flip(x);
+    for (int j = 0; j < cnt; ++j) {
+        f(syn, lg);
+        if (j + 1 == cnt) break;
+        const int p = __ffsll((long long)x) - 1;
+        const unsigned long long v = x + (1ull << p);
+        const unsigned long long next = v | (p + 2 < 64 ? ((v ^ x) >> (p + 2)) : 0ull);
+        flip(x ^ next);
+        x = next;
+    }
+}
+
 // Pass 1: every left part claims the slot of its tag (first empty slot on its probe
 // sequence, or the slot its tag already owns) and the claimer writes syndrome + fingerprint.
 __global__ void __launch_bounds__(256) mitm_claim_kernel(MitmShared S, MitmTable T, int first,
@@ -86,32 +150,36 @@ __global__ void __launch_bounds__(256) mitm_claim_kernel(MitmShared S, MitmTable
                                                          unsigned long long pw3,
                                                          const unsigned long long* __restrict__ B) {
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long runs = (n + kMitmRun - 1) / kMitmRun;
     const int KW = S.SW + S.LW;
-    for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-         id < n; id += stride) {
-        uint32_t syn[kMitmMaxSynWords], lg[kMitmMaxLogWords];
-        part_words(S, B, id, first, count, w, pw3, syn, lg);
-        const unsigned long long h = syn_hash(syn, S.SW, T.seed);
-        const unsigned long long tg = (h & T.tag_mask) | 1ull;
-        unsigned long long slot = h & T.mask;
-        bool placed = false;
-        for (unsigned long long it = 0; it <= T.mask; ++it) {
-            const unsigned long long old = atomicCAS(T.tag + slot, 0ull, tg);
-            if (old == 0ull) {
-                uint32_t* k = T.key + slot * (unsigned long long)KW;
+    for (unsigned long long r = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         r < runs; r += stride) {
+        const unsigned long long id0 = r * kMitmRun;
+        const int cnt = (int)(n - id0 < (unsigned long long)kMitmRun ? n - id0 : kMitmRun);
+        for_run(S, B, id0, cnt, first, count, w, pw3,
+                [&](const uint32_t (&syn)[kMitmMaxSynWords], const uint32_t (&lg)[kMitmMaxLogWords]) {
+            const unsigned long long h = syn_hash(syn, S.SW, T.seed);
+            const unsigned long long tg = (h & T.tag_mask) | 1ull;
+            unsigned long long slot = h & T.mask;
+            bool placed = false;
+            for (unsigned long long it = 0; it <= T.mask; ++it) {
+                const unsigned long long old = atomicCAS(T.tag + slot, 0ull, tg);
+                if (old == 0ull) {
+                    uint32_t* k = T.key + slot * (unsigned long long)KW;
 #pragma unroll
-                for (int q = 0; q < kMitmMaxSynWords; ++q)
-                    if (q < S.SW) k[q] = syn[q];
+                    for (int q = 0; q < kMitmMaxSynWords; ++q)
+                        if (q < S.SW) k[q] = syn[q];
 #pragma unroll
-                for (int q = 0; q < kMitmMaxLogWords; ++q)
-                    if (q < S.LW) k[S.SW + q] = lg[q];
-                placed = true;
-                break;
+                    for (int q = 0; q < kMitmMaxLogWords; ++q)
+                        if (q < S.LW) k[S.SW + q] = lg[q];
+                    placed = true;
+                    break;
+                }
+                if (old == tg) { placed = true; break; }
+                slot = (slot + 1) & T.mask;
             }
-            if (old == tg) { placed = true; break; }
-            slot = (slot + 1) & T.mask;
-        }
-        if (!placed) atomicOr(S.status + kMitmOverrun, 1);
+            if (!placed) atomicOr(S.status + kMitmOverrun, 1);
+        });
     }
 }
 
@@ -123,33 +191,37 @@ __global__ void __launch_bounds__(256) mitm_verify_kernel(MitmShared S, MitmTabl
                                                           unsigned long long pw3,
                                                           const unsigned long long* __restrict__ B) {
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long runs = (n + kMitmRun - 1) / kMitmRun;
     const int KW = S.SW + S.LW;
-    for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-         id < n; id += stride) {
-        uint32_t syn[kMitmMaxSynWords], lg[kMitmMaxLogWords];
-        part_words(S, B, id, first, count, w, pw3, syn, lg);
-        const unsigned long long h = syn_hash(syn, S.SW, T.seed);
-        const unsigned long long tg = (h & T.tag_mask) | 1ull;
-        unsigned long long slot = h & T.mask;
-        bool seen = false;
-        for (unsigned long long it = 0; it <= T.mask; ++it) {
-            const unsigned long long t = T.tag[slot];
-            if (t == tg) { seen = true; break; }
-            if (t == 0ull) break;
-            slot = (slot + 1) & T.mask;
-        }
-        if (!seen) { atomicOr(S.status + kMitmOverrun, 1); continue; }
-        const uint32_t* k = T.key + slot * (unsigned long long)KW;
-        bool same = true;
+    for (unsigned long long r = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         r < runs; r += stride) {
+        const unsigned long long id0 = r * kMitmRun;
+        const int cnt = (int)(n - id0 < (unsigned long long)kMitmRun ? n - id0 : kMitmRun);
+        for_run(S, B, id0, cnt, first, count, w, pw3,
+                [&](const uint32_t (&syn)[kMitmMaxSynWords], const uint32_t (&lg)[kMitmMaxLogWords]) {
+            const unsigned long long h = syn_hash(syn, S.SW, T.seed);
+            const unsigned long long tg = (h & T.tag_mask) | 1ull;
+            unsigned long long slot = h & T.mask;
+            bool seen = false;
+            for (unsigned long long it = 0; it <= T.mask; ++it) {
+                const unsigned long long t = T.tag[slot];
+                if (t == tg) { seen = true; break; }
+                if (t == 0ull) break;
+                slot = (slot + 1) & T.mask;
+            }
+            if (!seen) { atomicOr(S.status + kMitmOverrun, 1); return; }
+            const uint32_t* k = T.key + slot * (unsigned long long)KW;
+            bool same = true;
 #pragma unroll
-        for (int q = 0; q < kMitmMaxSynWords; ++q)
-            if (q < S.SW) same = same && (k[q] == syn[q]);
-        if (!same) { atomicOr(S.status + kMitmCollision, 1); continue; }
-        bool diff = false;
+            for (int q = 0; q < kMitmMaxSynWords; ++q)
+                if (q < S.SW) same = same && (k[q] == syn[q]);
+            if (!same) { atomicOr(S.status + kMitmCollision, 1); return; }
+            bool diff = false;
 #pragma unroll
-        for (int q = 0; q < kMitmMaxLogWords; ++q)
-            if (q < S.LW) diff = diff || (k[S.SW + q] != lg[q]);
-        if (diff && (T.flags[slot] & 1u) == 0u) atomicOr(T.flags + slot, 1u);
+            for (int q = 0; q < kMitmMaxLogWords; ++q)
+                if (q < S.LW) diff = diff || (k[S.SW + q] != lg[q]);
+            if (diff && (T.flags[slot] & 1u) == 0u) atomicOr(T.flags + slot, 1u);
+        });
     }
 }
 
@@ -160,40 +232,42 @@ __global__ void __launch_bounds__(256) mitm_probe_kernel(MitmShared S, MitmTable
                                                          unsigned long long pw3, int count_all,
                                                          const unsigned long long* __restrict__ B) {
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long runs = (n + kMitmRun - 1) / kMitmRun;
     const int KW = S.SW + S.LW;
     volatile int* found = S.status + kMitmFound;
-    for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-         id < n; id += stride) {
+    for (unsigned long long r = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         r < runs; r += stride) {
         if (*found) return;   // the level already hit
-        uint32_t syn[kMitmMaxSynWords], lg[kMitmMaxLogWords];
-        part_words(S, B, id, first, count, w, pw3, syn, lg);
-        const unsigned long long h = syn_hash(syn, S.SW, T.seed);
-        const unsigned long long tg = (h & T.tag_mask) | 1ull;
-        unsigned long long slot = h & T.mask;
-        bool done = false;
-        for (unsigned long long it = 0; it <= T.mask && !done; ++it) {
-            const unsigned long long t = T.tag[slot];
-            if (t == 0ull) { done = true; break; }
-            if (t == tg) {
-                // the only slot this syndrome can own: a left part with the same syndrome
-                // but another slot would have joined this one and been reported
-                done = true;
-                const uint32_t* k = T.key + slot * (unsigned long long)KW;
-                bool same = true;
+        const unsigned long long id0 = r * kMitmRun;
+        const int cnt = (int)(n - id0 < (unsigned long long)kMitmRun ? n - id0 : kMitmRun);
+        for_run(S, B, id0, cnt, first, count, w, pw3,
+                [&](const uint32_t (&syn)[kMitmMaxSynWords], const uint32_t (&lg)[kMitmMaxLogWords]) {
+            const unsigned long long h = syn_hash(syn, S.SW, T.seed);
+            const unsigned long long tg = (h & T.tag_mask) | 1ull;
+            unsigned long long slot = h & T.mask;
+            for (unsigned long long it = 0; it <= T.mask; ++it) {
+                const unsigned long long t = T.tag[slot];
+                if (t == 0ull) return;
+                if (t == tg) {
+                    // the only slot this syndrome can own: a left part with the same syndrome
+                    // but another slot would have joined this one and been reported
+                    const uint32_t* k = T.key + slot * (unsigned long long)KW;
+                    bool same = true;
 #pragma unroll
-                for (int q = 0; q < kMitmMaxSynWords; ++q)
-                    if (q < S.SW) same = same && (k[q] == syn[q]);
-                if (!same) break;
-                bool hit = count_all != 0 || (T.flags[slot] & 1u) != 0u;
+                    for (int q = 0; q < kMitmMaxSynWords; ++q)
+                        if (q < S.SW) same = same && (k[q] == syn[q]);
+                    if (!same) return;
+                    bool hit = count_all != 0 || (T.flags[slot] & 1u) != 0u;
 #pragma unroll
-                for (int q = 0; q < kMitmMaxLogWords; ++q)
-                    if (q < S.LW) hit = hit || (k[S.SW + q] != lg[q]);
-                if (hit) atomicExch(S.status + kMitmFound, 1);
-                break;
+                    for (int q = 0; q < kMitmMaxLogWords; ++q)
+                        if (q < S.LW) hit = hit || (k[S.SW + q] != lg[q]);
+                    if (hit) atomicExch(S.status + kMitmFound, 1);
+                    return;
+                }
+                slot = (slot + 1) & T.mask;
             }
-            slot = (slot + 1) & T.mask;
-        }
-        if (!done) atomicOr(S.status + kMitmOverrun, 1);
+            atomicOr(S.status + kMitmOverrun, 1);
+        });
     }
 }
 
@@ -201,7 +275,8 @@ __global__ void __launch_bounds__(256) mitm_probe_kernel(MitmShared S, MitmTable
 
 namespace {
 unsigned int grid_for(unsigned long long n, int num_sms) {
-    const unsigned long long want = (n + 255) / 256;
+    const unsigned long long runs = (n + dev::kMitmRun - 1) / dev::kMitmRun;
+    const unsigned long long want = (runs + 255) / 256;
     const unsigned long long cap = (unsigned long long)num_sms * 16;
     return (unsigned int)(want < cap ? (want > 0 ? want : 1) : cap);
 }
