@@ -203,7 +203,10 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
 /* Two-phase form: prepare does the host reduction, information sets and seed bounds of
  * every query and leaves the packed rows resident on the device; execute runs (or re-runs
  * from the post-prepare state) all BZ rounds and fills out[nq]; free releases everything.
- * A handle is used by one thread at a time. */
+ * Execute steps the queries as interleaved groups (QSFB_EXEC_GROUPS, default 3, at least 64
+ * queries per group), each with its own stream and host thread, so that one group's host
+ * planning overlaps the others' kernels; the answers do not depend on the grouping, and
+ * device_span_ms is the span over all groups.  A handle is used by one thread at a time. */
 typedef struct QsfbBatchHandle QsfbBatchHandle;
 int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
                        QsfbBatchHandle** handle);

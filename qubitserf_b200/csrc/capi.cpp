@@ -211,6 +211,160 @@ struct QsfbBatchHandle {
     }
 };
 
+namespace {
+
+// The rounds of a prepared batch.  The jobs are independent, so they run as `groups`
+// interleaved job groups (QSFB_EXEC_GROUPS, default 3; jobs dealt round robin), each
+// stepping its own rounds on its own session and host thread: while one group's kernels
+// run, the others plan and apply on the host, which hides the host share of each round.
+// The span is the union over the groups, from one start event that every group's stream
+// waits on to the last group's end event.
+int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_ms,
+                   int max_groups) {
+    const char* ge = std::getenv("QSFB_EXEC_GROUPS");   // read per call (benchmarks switch it)
+    const int groups_env = std::max(1, std::min(ge ? std::atoi(ge) : 3, 8));
+    const int G = std::max(1, std::min({groups_env, max_groups, (int)H->ptrs.size() / 64}));
+    if (G == 1) return run_rounds(H->lease->s, H->ptrs, rs, rounds, span_ms);
+    std::vector<std::vector<BzJob*>> part(G);
+    for (size_t j = 0; j < H->ptrs.size(); ++j) part[j % G].push_back(H->ptrs[j]);
+    std::vector<std::unique_ptr<SessionLease>> extra;
+    std::vector<Session*> sess{H->lease->s};
+    for (int g = 1; g < G; ++g) {
+        extra.emplace_back(new SessionLease(H->dev));
+        if (!extra.back()->s) return kErrDevice;
+        sess.push_back(extra.back()->s);
+    }
+    cudaEvent_t start = nullptr;
+    std::vector<cudaEvent_t> end(G, nullptr);
+    bool ev_ok = cudaEventCreate(&start) == cudaSuccess;
+    for (int g = 0; g < G && ev_ok; ++g) ev_ok = cudaEventCreate(&end[g]) == cudaSuccess;
+    ev_ok = ev_ok && cudaEventRecord(start, sess[0]->stream) == cudaSuccess;
+    for (int g = 1; g < G && ev_ok; ++g)
+        ev_ok = cudaStreamWaitEvent(sess[g]->stream, start, 0) == cudaSuccess;
+    if (!ev_ok) {
+        cudaGetLastError();
+        if (start) cudaEventDestroy(start);
+        for (cudaEvent_t e : end) if (e) cudaEventDestroy(e);
+        return kErrDevice;
+    }
+    std::vector<RunStats> st(G);
+    std::vector<int> rr(G, 0), rcs(G, kOk);
+    std::vector<std::thread> th;
+    for (int g = 0; g < G; ++g)
+        th.emplace_back([&, g]() {
+            rcs[g] = run_rounds(sess[g], part[g], &st[g], &rr[g], nullptr);
+            if (cudaEventRecord(end[g], sess[g]->stream) != cudaSuccess) rcs[g] = kErrDevice;
+        });
+    for (std::thread& t : th) t.join();
+    int rc = kOk;
+    float span = 0.f;
+    for (int g = 0; g < G; ++g) {
+        if (rcs[g] != kOk && rc == kOk) rc = rcs[g];
+        float ms = 0.f;
+        if (cudaEventSynchronize(end[g]) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, start, end[g]) == cudaSuccess)
+            span = std::max(span, ms);
+        else if (rc == kOk)
+            rc = kErrDevice;
+        rs->host_plan_s += st[g].host_plan_s;
+        rs->host_apply_s += st[g].host_apply_s;
+        rs->ms_gen += st[g].ms_gen;
+        rs->ms_pairs += st[g].ms_pairs;
+        rs->ms_tc += st[g].ms_tc;
+        rs->jobs += st[g].jobs;
+        rs->codewords += st[g].codewords;
+        rs->popc_issued += st[g].popc_issued;
+        rs->zero_codewords += st[g].zero_codewords;
+        rs->tc_codewords += st[g].tc_codewords;
+        rs->launches += st[g].launches;
+        *rounds = std::max(*rounds, rr[g]);
+    }
+    cudaGetLastError();
+    cudaEventDestroy(start);
+    for (cudaEvent_t e : end) cudaEventDestroy(e);
+    if (span_ms) *span_ms = span;
+    return rc;
+}
+
+int batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats, int max_groups) {
+    if (!H || (!out && !H->map.empty())) return kErrNull;
+    const double t0 = now_seconds();
+    if (H->executed)
+        for (BzJob* j : H->ptrs) j->reset();
+    H->executed = true;
+    RunStats rs;
+    int rounds = 0;
+    double span = 0.0;
+    int rc = execute_groups(H, &rs, &rounds, &span, max_groups);
+    if (rc != kOk) return rc;
+    auto& jobs = H->jobs;
+    // Results (witness rebuild + host verification) are independent per job: spread them
+    // over the host cores.
+    std::vector<BzResult> res(jobs.size());
+    {
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (size_t k; (k = next.fetch_add(1)) < jobs.size();) res[k] = jobs[k]->result();
+        };
+        const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
+                                                  (int)jobs.size() / 8 + 1));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nth; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto& th : pool) th.join();
+    }
+    for (size_t i = 0; i < H->map.size(); ++i) {
+        QsfbAnswer& a = out[i];
+        std::memset(&a, 0, sizeof(a));
+        const auto& m = H->map[i];
+        if (H->kinds[i] == 2) {
+            BzResult rz, rx;
+            int zw = m.zw, xw = m.xw;
+            bool ok = true, proven = true;
+            if (m.job0 >= 0) { rz = res[m.job0]; zw = rz.distance; ok &= rz.witness_ok || zw <= 0; proven &= rz.proven; }
+            if (m.job1 >= 0) { rx = res[m.job1]; xw = rx.distance; ok &= rx.witness_ok || xw <= 0; proven &= rx.proven; }
+            a.z_weight = zw;
+            a.x_weight = xw;
+            a.distance = std::max(zw, xw);
+            a.proven = proven ? 1 : 0;
+            a.witness_ok = ok ? 1 : 0;
+            a.levels = std::max(m.job0 >= 0 ? rz.levels : 0, m.job1 >= 0 ? rx.levels : 0);
+        } else {
+            const BzResult& r = res[m.job0];
+            a.distance = r.distance;
+            a.lower_bound = r.lower_bound;
+            a.proven = r.proven ? 1 : 0;
+            a.levels = r.levels;
+            a.witness_ok = (r.witness_ok || r.distance < 0) ? 1 : 0;
+            a.z_weight = a.x_weight = -1;
+        }
+    }
+    if (stats) {
+        stats->seconds = now_seconds() - t0;
+        stats->prepare_seconds = H->prepare_s;
+        stats->host_setup_seconds = H->setup.host_setup_s;
+        stats->device_seed_seconds = H->setup.device_seed_s;
+        stats->device_ms = rs.ms_gen + rs.ms_pairs;
+        stats->device_span_ms = span;
+        stats->pair_ms = rs.ms_pairs;
+        stats->tc_ms = rs.ms_tc;
+        stats->codewords = rs.codewords;
+        stats->popc_issued = rs.popc_issued;
+        stats->zero_codewords = rs.zero_codewords;
+        stats->tc_codewords = rs.tc_codewords;
+        stats->rounds = rounds;
+        stats->kernel_launches = rs.launches;
+        stats->certificates = (int)jobs.size();
+        stats->device_bytes = (long long)H->arena->bytes();
+        stats->gen_ms = rs.ms_gen;
+        stats->host_plan_seconds = rs.host_plan_s;
+        stats->host_apply_seconds = rs.host_apply_s;
+    }
+    return kOk;
+}
+
+}  // namespace
+
 extern "C" {
 
 int distfind_css_distance(const uint8_t* Hx, int hx_rows, int hx_cols, const uint8_t* Hz,
@@ -562,81 +716,9 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
 }
 
 int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats) {
-    if (!H || (!out && !H->map.empty())) return kErrNull;
-    const double t0 = now_seconds();
-    if (H->executed)
-        for (BzJob* j : H->ptrs) j->reset();
-    H->executed = true;
-    RunStats rs;
-    int rounds = 0;
-    double span = 0.0;
-    int rc = run_rounds(H->lease->s, H->ptrs, &rs, &rounds, &span);
-    if (rc != kOk) return rc;
-    auto& jobs = H->jobs;
-    // Results (witness rebuild + host verification) are independent per job: spread them
-    // over the host cores.
-    std::vector<BzResult> res(jobs.size());
-    {
-        std::atomic<size_t> next{0};
-        auto worker = [&]() {
-            for (size_t k; (k = next.fetch_add(1)) < jobs.size();) res[k] = jobs[k]->result();
-        };
-        const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
-                                                  (int)jobs.size() / 8 + 1));
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nth; ++t) pool.emplace_back(worker);
-        worker();
-        for (auto& th : pool) th.join();
-    }
-    for (size_t i = 0; i < H->map.size(); ++i) {
-        QsfbAnswer& a = out[i];
-        std::memset(&a, 0, sizeof(a));
-        const auto& m = H->map[i];
-        if (H->kinds[i] == 2) {
-            BzResult rz, rx;
-            int zw = m.zw, xw = m.xw;
-            bool ok = true, proven = true;
-            if (m.job0 >= 0) { rz = res[m.job0]; zw = rz.distance; ok &= rz.witness_ok || zw <= 0; proven &= rz.proven; }
-            if (m.job1 >= 0) { rx = res[m.job1]; xw = rx.distance; ok &= rx.witness_ok || xw <= 0; proven &= rx.proven; }
-            a.z_weight = zw;
-            a.x_weight = xw;
-            a.distance = std::max(zw, xw);
-            a.proven = proven ? 1 : 0;
-            a.witness_ok = ok ? 1 : 0;
-            a.levels = std::max(m.job0 >= 0 ? rz.levels : 0, m.job1 >= 0 ? rx.levels : 0);
-        } else {
-            const BzResult& r = res[m.job0];
-            a.distance = r.distance;
-            a.lower_bound = r.lower_bound;
-            a.proven = r.proven ? 1 : 0;
-            a.levels = r.levels;
-            a.witness_ok = (r.witness_ok || r.distance < 0) ? 1 : 0;
-            a.z_weight = a.x_weight = -1;
-        }
-    }
-    if (stats) {
-        stats->seconds = now_seconds() - t0;
-        stats->prepare_seconds = H->prepare_s;
-        stats->host_setup_seconds = H->setup.host_setup_s;
-        stats->device_seed_seconds = H->setup.device_seed_s;
-        stats->device_ms = rs.ms_gen + rs.ms_pairs;
-        stats->device_span_ms = span;
-        stats->pair_ms = rs.ms_pairs;
-        stats->tc_ms = rs.ms_tc;
-        stats->codewords = rs.codewords;
-        stats->popc_issued = rs.popc_issued;
-        stats->zero_codewords = rs.zero_codewords;
-        stats->tc_codewords = rs.tc_codewords;
-        stats->rounds = rounds;
-        stats->kernel_launches = rs.launches;
-        stats->certificates = (int)jobs.size();
-        stats->device_bytes = (long long)H->arena->bytes();
-        stats->gen_ms = rs.ms_gen;
-        stats->host_plan_seconds = rs.host_plan_s;
-        stats->host_apply_seconds = rs.host_apply_s;
-    }
-    return kOk;
+    return batch_execute(H, out, stats, 8);
 }
+
 
 void qsfb_batch_free(QsfbBatchHandle* H) { delete H; }
 
@@ -683,7 +765,9 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
         if (rc == kOk) {
             QsfbBatchStats st;
             std::memset(&st, 0, sizeof(st));
-            rc = qsfb_batch_execute(H[c], out ? out + cut[c] : nullptr, &st);
+            // one job group while the next chunk is being prepared beside it (the groups'
+            // host threads would compete with the preparation), grouped for the last chunk
+            rc = batch_execute(H[c], out ? out + cut[c] : nullptr, &st, c + 1 < nchunks ? 1 : 8);
             total.prepare_seconds += st.prepare_seconds;
             total.host_setup_seconds += st.host_setup_seconds;
             total.device_seed_seconds += st.device_seed_seconds;

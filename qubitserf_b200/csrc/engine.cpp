@@ -209,6 +209,7 @@ Arena::~Arena() {
 }
 
 void* Arena::alloc(size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu_);
     bytes = align_up(std::max<size_t>(bytes, 16), 256);
     if (chunks_.empty() || used_ + bytes > chunks_.back().second) {
         const size_t sz = round_bucket(std::max<size_t>(bytes, 64ull << 20));

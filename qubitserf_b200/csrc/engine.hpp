@@ -133,6 +133,7 @@ public:
 
 private:
     Device* dev_;
+    std::mutex mu_;   // the rounds of several job groups may carve lists concurrently
     std::vector<std::pair<char*, size_t>> chunks_;
     size_t used_ = 0, total_ = 0;
 };
