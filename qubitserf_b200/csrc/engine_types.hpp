@@ -54,7 +54,7 @@ struct LevelDesc {
     int pad_;
 };
 
-constexpr int kGenRun = 8;         // consecutive list entries generated by one thread
+constexpr int kGenRun = 4;         // consecutive list entries generated by one thread (measured: 2, 8 and 32 are slower)
 constexpr int kPmRowBytes = 64;    // +-1 row: 64 int8 columns (the first two probe words)
 constexpr int kPmPadRows = 256;    // zero rows after every +-1 list (whole-tile copies)
 
