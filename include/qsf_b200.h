@@ -193,10 +193,10 @@ typedef struct {
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free.  Batches of 256 queries or more are pipelined in
- * chunks (three by default, QSFB_BATCH_CHUNKS to change; the host reduction and seeds of
- * one chunk run while the device enumerates the previous one); the answers are those of
- * one batch, and the stats sum the chunks (rounds, codewords, phase times; device_bytes
- * is the largest chunk's). */
+ * chunks (two by default, QSFB_BATCH_CHUNKS to change; the host reduction and seeds of one
+ * chunk run, on all host cores but four, while the device enumerates the previous one as
+ * two job groups); the answers are those of one batch, and the stats sum the chunks
+ * (rounds, codewords, phase times; device_bytes is the largest chunk's). */
 int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
                QsfbBatchStats* stats);
 

@@ -731,14 +731,10 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
                QsfbBatchStats* stats) {
     const double t0 = now_seconds();
     constexpr int kPipeMin = 256;   // below this the batch runs in one piece
-    // QSFB_BATCH_CHUNKS: number of pipeline chunks (default 3, the fastest measured for the
-    // 1024-code batch: 1 chunk 97 ms, 2: 74-83, 3: 76-77, 4: 76-81, 6: 81, 8: 87; 1 = one
-    // piece)
-    static const int chunks = [] {
-        const char* e = std::getenv("QSFB_BATCH_CHUNKS");
-        const int c = e ? std::atoi(e) : 3;
-        return std::max(1, std::min(c, 16));
-    }();
+    // QSFB_BATCH_CHUNKS: number of pipeline chunks (default 2; 1 = one piece), read per
+    // call.  1024-code batch, end to end: 2 chunks 17.4-17.8k certs/s, 3 chunks 17.3-17.4k.
+    const char* ce = std::getenv("QSFB_BATCH_CHUNKS");
+    const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : 2, 16));
     std::vector<int> cut{0};
     if (nq >= kPipeMin && chunks > 1) {
         const int first = std::max(32, nq / (2 * chunks));
@@ -751,8 +747,20 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     const int nchunks = (int)cut.size() - 1;
     std::vector<QsfbBatchHandle*> H(nchunks, nullptr);
     std::vector<int> prc(nchunks, kOk);
+    // Preparations that run beside an execution leave four host cores to its job groups'
+    // round planning (QSFB_OVERLAP_PREP_THREADS to set the count); overlapped executions
+    // step QSFB_OVERLAP_GROUPS job groups (default 2).  Measured on the 1024-code batch (16
+    // host cores): all cores + 1 group 15.5-16.3k certs/s end to end, 12 cores + 2 groups
+    // 17.1-17.8k.
+    const char* pe = std::getenv("QSFB_OVERLAP_PREP_THREADS");
+    const char* ge = std::getenv("QSFB_OVERLAP_GROUPS");
+    const int all = host_threads > 0 ? host_threads
+                                     : std::max(1, (int)std::thread::hardware_concurrency());
+    const int overlap_threads = pe ? std::max(1, std::atoi(pe)) : std::max(1, all - 4);
+    const int overlap_groups = ge ? std::max(1, std::atoi(ge)) : 2;
     auto prepare = [&](int c) {
-        prc[c] = qsfb_batch_prepare(queries + cut[c], cut[c + 1] - cut[c], host_threads, &H[c]);
+        prc[c] = qsfb_batch_prepare(queries + cut[c], cut[c + 1] - cut[c],
+                                    c == 0 ? host_threads : overlap_threads, &H[c]);
     };
     QsfbBatchStats total;
     std::memset(&total, 0, sizeof(total));
@@ -767,7 +775,8 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
             std::memset(&st, 0, sizeof(st));
             // one job group while the next chunk is being prepared beside it (the groups'
             // host threads would compete with the preparation), grouped for the last chunk
-            rc = batch_execute(H[c], out ? out + cut[c] : nullptr, &st, c + 1 < nchunks ? 1 : 8);
+            rc = batch_execute(H[c], out ? out + cut[c] : nullptr, &st,
+                               c + 1 < nchunks ? overlap_groups : 8);
             total.prepare_seconds += st.prepare_seconds;
             total.host_setup_seconds += st.host_setup_seconds;
             total.device_seed_seconds += st.device_seed_seconds;
