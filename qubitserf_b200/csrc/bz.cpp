@@ -132,6 +132,24 @@ std::vector<int> seed_orders(int n, int trials, unsigned seed, int only) {
 }
 
 namespace {
+std::mutex g_bytes_mu;
+std::map<std::tuple<int, int, unsigned>, std::shared_ptr<const std::vector<uint8_t>>> g_bytes;
+}  // namespace
+
+std::shared_ptr<const std::vector<uint8_t>> seed_order_bytes(int n, int trials, unsigned seed) {
+    const auto key = std::make_tuple(n, trials, seed);
+    {
+        std::lock_guard<std::mutex> lk(g_bytes_mu);
+        auto it = g_bytes.find(key);
+        if (it != g_bytes.end()) return it->second;
+    }
+    const std::vector<int> ord = seed_orders(n, trials, seed);
+    auto v = std::make_shared<const std::vector<uint8_t>>(ord.begin(), ord.end());
+    std::lock_guard<std::mutex> lk(g_bytes_mu);
+    return g_bytes.emplace(key, v).first->second;
+}
+
+namespace {
 std::vector<int> seed_orders_uncached(int n, int trials, unsigned seed, int only) {
     int nth = (int)std::thread::hardware_concurrency();
     if (nth < 1) nth = 1;
@@ -157,8 +175,7 @@ std::vector<int> seed_orders_uncached(int n, int trials, unsigned seed, int only
 
 void BzSide::apply_device_seed(unsigned key) {
     seed_pending = false;
-    seed_perm.clear();
-    seed_perm.shrink_to_fit();
+    seed_perm.reset();
     if (key == 0xffffffffu) return;
     const int w = (int)(key >> 15);
     if (w < inner) {
@@ -189,8 +206,7 @@ int BzSide::setup_host(const Problem& p, const BzOptions& opt, const char* t) {
         // the eliminations run on the GPU (setup_jobs); draw the column orders here
         seed_pending = true;
         seed_trials = opt.seed_trials;
-        const std::vector<int> ord = seed_orders(p.n, seed_trials, 0x9e3779b9u);
-        seed_perm.assign(ord.begin(), ord.end());
+        seed_perm = seed_order_bytes(p.n, seed_trials, 0x9e3779b9u);
     } else {
         std::vector<u64> w;
         const int seeded = random_is_seed(p, inner, opt.seed_trials, 0x9e3779b9u,
@@ -496,12 +512,20 @@ int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& job
         off = al(off + v.size() * sizeof(SeedDesc));
         const size_t off_keys = off;
         off = al(off + v.size() * 4);
+        // the column orders are shared by every side of the same length: one copy each
         std::vector<size_t> og(v.size()), oc(v.size()), op(v.size());
+        std::map<const std::vector<uint8_t>*, size_t> perm_off;
         for (size_t i = 0; i < v.size(); ++i) {
             const Problem& p = *v[i]->prob;
             og[i] = off; off = al(off + (size_t)p.code_gen.rows * W * 8);
             oc[i] = off; off = al(off + (size_t)std::max(1, p.check.rows) * W * 8);
-            op[i] = off; off = al(off + v[i]->seed_perm.size());
+            const std::vector<uint8_t>* pp = v[i]->seed_perm.get();
+            auto it = perm_off.find(pp);
+            if (it == perm_off.end()) {
+                it = perm_off.emplace(pp, off).first;
+                off = al(off + pp->size());
+            }
+            op[i] = it->second;
         }
         char* d = (char*)arena->alloc(off);
         if (!d) return kErrMemory;
@@ -519,7 +543,6 @@ int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& job
             u64* c = (u64*)(h + oc[i]);
             for (int r = 0; r < p.check.rows; ++r)
                 for (int w = 0; w < W; ++w) c[(size_t)r * W + w] = p.check.row(r)[w];
-            std::memcpy(h + op[i], v[i]->seed_perm.data(), v[i]->seed_perm.size());
             SeedDesc& D = hd[i];
             D.gen = (const unsigned long long*)(d + og[i]);
             D.check = (const unsigned long long*)(d + oc[i]);
@@ -534,6 +557,7 @@ int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& job
             hk[i] = 0xffffffffu;
             trials += v[i]->seed_trials;
         }
+        for (const auto& po : perm_off) std::memcpy(h + po.second, po.first->data(), po.first->size());
         if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
             launch_seed_trials(W, (const SeedDesc*)(d + off_desc), (int)v.size(), trials,
                                s->stream) != cudaSuccess ||

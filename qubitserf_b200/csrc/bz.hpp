@@ -62,6 +62,8 @@ int random_is_seed(const Problem& p, int init_best, int trials, unsigned seed, b
 // The column orders of those trials (trials x n, trial-major), drawn exactly as the
 // reference draws them; `only` >= 0 returns just that trial's order.
 std::vector<int> seed_orders(int n, int trials, unsigned seed, int only = -1);
+// The same orders as bytes (n <= 256), one shared copy per (n, trials, seed).
+std::shared_ptr<const std::vector<uint8_t>> seed_order_bytes(int n, int trials, unsigned seed);
 
 // One BZ subproblem stepped level by level.
 class BzSide {
@@ -96,7 +98,7 @@ public:
     bool seed_pending = false;
     int seed_trials = 0;
     int seed_trial = -1, seed_row = -1;
-    std::vector<uint8_t> seed_perm;   // trials x n, released after upload
+    std::shared_ptr<const std::vector<uint8_t>> seed_perm;   // trials x n, shared by length
     void apply_device_seed(unsigned key);
 };
 
