@@ -25,25 +25,58 @@ Mat from_dense(const u8* data, int rows, int cols) {
     for (int i = 0; i < rows; ++i) {
         u64* r = m.row(i);
         const u8* s = data + (size_t)i * cols;
-        for (int j = 0; j < cols; ++j)
-            if (s[j] & 1) r[j >> 6] |= 1ull << (j & 63);
+        for (int w = 0; w * 64 < cols; ++w) {
+            const int hi = std::min(64, cols - w * 64);
+            u64 word = 0;
+            for (int j = 0; j < hi; ++j) word |= (u64)(s[w * 64 + j] & 1u) << j;
+            r[w] = word;
+        }
     }
     return m;
 }
 
 // One elimination step on column `col`: returns true if a pivot was placed at `rank`.
-static inline bool eliminate_column(Mat& m, int rank, int col) {
-    const int wd = col >> 6;
-    const u64 bit = 1ull << (col & 63);
+// The clearing pass is branchless (every row XORs the pivot row under a mask made from its
+// bit in the column): which rows hold the bit is data, so a branch on it mispredicts about
+// half the time.  S = words per row (0: any).
+template <int S>
+static inline bool eliminate_column_s(Mat& m, int rank, int col) {
+    const int st = S > 0 ? S : m.stride;
+    const int wd = col >> 6, sh = col & 63;
+    u64* base = m.w.data();
     int sel = -1;
     for (int r = rank; r < m.rows; ++r)
-        if (m.row(r)[wd] & bit) { sel = r; break; }
+        if ((base[(size_t)r * st + wd] >> sh) & 1u) { sel = r; break; }
     if (sel < 0) return false;
     m.swap_rows(rank, sel);
-    const u64* p = m.row(rank);
-    for (int r = 0; r < m.rows; ++r)
-        if (r != rank && (m.row(r)[wd] & bit)) vec_xor(m.row(r), p, m.stride);
+    u64* prow = base + (size_t)rank * st;
+    if (S > 0) {
+        u64 p[S > 0 ? S : 1];
+        for (int k = 0; k < S; ++k) p[k] = prow[k];
+        for (int r = 0; r < m.rows; ++r) {
+            u64* row = base + (size_t)r * S;
+            const u64 mask = (r == rank) ? 0ull : (0ull - ((row[wd] >> sh) & 1u));
+            for (int k = 0; k < S; ++k) row[k] ^= p[k] & mask;
+        }
+    } else {
+        for (int r = 0; r < m.rows; ++r) {
+            if (r == rank) continue;
+            u64* row = base + (size_t)r * st;
+            const u64 mask = 0ull - ((row[wd] >> sh) & 1u);
+            for (int k = 0; k < st; ++k) row[k] ^= prow[k] & mask;
+        }
+    }
     return true;
+}
+
+static inline bool eliminate_column(Mat& m, int rank, int col) {
+    switch (m.stride) {
+        case 1: return eliminate_column_s<1>(m, rank, col);
+        case 2: return eliminate_column_s<2>(m, rank, col);
+        case 3: return eliminate_column_s<3>(m, rank, col);
+        case 4: return eliminate_column_s<4>(m, rank, col);
+        default: return eliminate_column_s<0>(m, rank, col);
+    }
 }
 
 // cpp/qsf/gf2.cpp:25-40
@@ -90,14 +123,27 @@ Mat nullspace(const Mat& in) {
     const int rank = (int)piv.size();
     std::vector<char> is_piv(m.cols, 0);
     for (int p : piv) is_piv[p] = 1;
+    // row of free column f: e_f plus e_{piv[r]} for every pivot row r with a 1 in column f,
+    // filled row by row from the free-column bits of each pivot row
     Mat ns(m.cols - rank, m.cols);
+    std::vector<int> out_of(m.cols, -1);
+    std::vector<u64> freemask(m.stride, 0ull);
     int out = 0;
     for (int f = 0; f < m.cols; ++f) {
         if (is_piv[f]) continue;
+        out_of[f] = out;
         ns.set(out, f, 1);
-        for (int r = 0; r < rank; ++r)
-            if (m.get(r, f)) ns.set(out, piv[r], 1);
+        freemask[f >> 6] |= 1ull << (f & 63);
         ++out;
+    }
+    for (int r = 0; r < rank; ++r) {
+        const u64* row = m.row(r);
+        const int p = piv[r];
+        for (int w = 0; w < m.stride; ++w)
+            for (u64 x = row[w] & freemask[w]; x; x &= x - 1) {
+                const int f = w * 64 + __builtin_ctzll(x);
+                ns.row(out_of[f])[p >> 6] |= 1ull << (p & 63);
+            }
     }
     return ns;
 }

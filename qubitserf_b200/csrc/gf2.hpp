@@ -29,6 +29,9 @@ inline int vec_weight(const u64* v, int stride) {
     for (int i = 0; i < stride; ++i) w += popc64(v[i]);
     return w;
 }
+inline void vec_or(u64* d, const u64* s, int stride) {
+    for (int i = 0; i < stride; ++i) d[i] |= s[i];
+}
 inline void vec_xor(u64* d, const u64* s, int stride) {
     for (int i = 0; i < stride; ++i) d[i] ^= s[i];
 }

@@ -21,15 +21,15 @@ std::vector<InfoSet> greedy_sets(const Mat& code_gen) {
     while (!active.empty()) {
         std::vector<int> piv = restricted_rref(work, active);
         seq.push_back({work, (int)piv.size(), piv});
-        std::vector<char> is_piv(n, 0), nonzero(n, 0);
+        std::vector<char> is_piv(n, 0);
         for (int c : piv) is_piv[c] = 1;
-        for (int r = 0; r < work.rows; ++r)
-            for (int c : active)
-                if (work.get(r, c)) nonzero[c] = 1;
+        // columns holding a 1 in some row: the OR of the rows
+        std::vector<u64> any(work.stride, 0ull);
+        for (int r = 0; r < work.rows; ++r) vec_or(any.data(), work.row(r), work.stride);
         std::vector<int> next;
         next.reserve(active.size());
         for (int c : active)
-            if (!is_piv[c] && nonzero[c]) next.push_back(c);
+            if (!is_piv[c] && ((any[c >> 6] >> (c & 63)) & 1u)) next.push_back(c);
         if (next.size() == active.size()) break;
         active.swap(next);
     }
@@ -39,57 +39,67 @@ std::vector<InfoSet> greedy_sets(const Mat& code_gen) {
 // Express column z over the independent class `cls`: (in_span, circuit) where circuit is
 // the ascending list of class columns whose XOR is z (cpp/distfind/css.cpp:316-351).
 // Origins are kept as bitsets over the columns, so the reference's sorted-list symmetric
-// difference becomes an XOR and the circuit is read out in ascending order.
+// difference becomes an XOR and the circuit is read out in ascending order.  A class is
+// independent, so both answers are unique whatever order its columns are inserted in:
+// each class keeps its reduced basis between queries (extended when a column is appended,
+// rebuilt after the augmenting path swaps columns) instead of rebuilding it per query.
 struct Expr {
     bool in_span;
     std::vector<int> circuit;
 };
 
+struct ClassBasis {
+    std::vector<u64> bv, bo;      // basis vectors (kw words) and origins (nw words)
+    std::vector<int> bpiv;        // pivot (lowest set bit) of each basis vector
+    int nb = 0;
+    bool valid = false;
+};
+
 struct Expresser {
     int kw = 0, nw = 0;
-    std::vector<u64> bv, bo;      // basis vectors (kw words) and origins (nw words)
-    std::vector<int> bpiv;
+    const std::vector<u64>* col = nullptr;
     std::vector<u64> v, o;
-    Expresser(int kw_, int n) : kw(kw_), nw(words_for(n)) {}
+    Expresser(int kw_, int n, const std::vector<u64>* c) : kw(kw_), nw(words_for(n)), col(c) {}
 
-    Expr operator()(const std::vector<int>& cls, const std::vector<u64>& col, int z,
-                    bool want_circuit) {
-        const size_t cap = cls.size() + 1;
-        if (bpiv.size() < cap) {
-            bv.resize(cap * kw);
-            bo.resize(cap * nw);
-            bpiv.resize(cap);
+    // v, o reduced against the basis: every pivot bit cleared, in insertion order
+    void reduce(const ClassBasis& B) {
+        for (int b = 0; b < B.nb; ++b) {
+            const int p = B.bpiv[b];
+            if ((v[p >> 6] >> (p & 63)) & 1u) {
+                for (int w = 0; w < kw; ++w) v[w] ^= B.bv[(size_t)b * kw + w];
+                for (int w = 0; w < nw; ++w) o[w] ^= B.bo[(size_t)b * nw + w];
+            }
         }
-        v.assign(kw, 0);
+    }
+    void load(int z) {
+        v.assign(col->begin() + (size_t)z * kw, col->begin() + (size_t)(z + 1) * kw);
         o.assign(nw, 0);
-        int nb = 0;
-        auto reduce = [&]() {
-            for (int b = 0; b < nb; ++b) {
-                const int p = bpiv[b];
-                if ((v[p >> 6] >> (p & 63)) & 1u) {
-                    for (int w = 0; w < kw; ++w) v[w] ^= bv[(size_t)b * kw + w];
-                    for (int w = 0; w < nw; ++w) o[w] ^= bo[(size_t)b * nw + w];
-                }
-            }
-        };
+    }
+    // append the reduced (v, o) as a basis vector when nonzero
+    void push(ClassBasis& B) {
+        int lb = -1;
+        for (int w = 0; w < kw; ++w)
+            if (v[w]) { lb = w * 64 + __builtin_ctzll(v[w]); break; }
+        if (lb < 0) return;
+        B.bv.insert(B.bv.end(), v.begin(), v.end());
+        B.bo.insert(B.bo.end(), o.begin(), o.end());
+        B.bpiv.push_back(lb);
+        ++B.nb;
+    }
+    void build(ClassBasis& B, const std::vector<int>& cls) {
+        B.bv.clear(); B.bo.clear(); B.bpiv.clear(); B.nb = 0;
         for (int idx : cls) {
-            for (int w = 0; w < kw; ++w) v[w] = col[(size_t)idx * kw + w];
-            std::fill(o.begin(), o.end(), 0);
+            load(idx);
             o[idx >> 6] |= 1ull << (idx & 63);
-            reduce();
-            int lb = -1;
-            for (int w = 0; w < kw; ++w)
-                if (v[w]) { lb = w * 64 + __builtin_ctzll(v[w]); break; }
-            if (lb >= 0) {
-                for (int w = 0; w < kw; ++w) bv[(size_t)nb * kw + w] = v[w];
-                for (int w = 0; w < nw; ++w) bo[(size_t)nb * nw + w] = o[w];
-                bpiv[nb] = lb;
-                ++nb;
-            }
+            reduce(B);
+            push(B);
         }
-        for (int w = 0; w < kw; ++w) v[w] = col[(size_t)z * kw + w];
-        std::fill(o.begin(), o.end(), 0);
-        reduce();
+        B.valid = true;
+    }
+    Expr query(ClassBasis& B, const std::vector<int>& cls, int z, bool want_circuit) {
+        if (!B.valid) build(B, cls);
+        load(z);
+        reduce(B);
         bool zero = true;
         for (int w = 0; w < kw; ++w)
             if (v[w]) { zero = false; break; }
@@ -99,31 +109,49 @@ struct Expresser {
                 for (u64 x = o[w]; x; x &= x - 1) e.circuit.push_back(w * 64 + __builtin_ctzll(x));
         return e;
     }
+    // z was just queried against B (not in its span) and appended to the class
+    void append_queried(ClassBasis& B, int z) {
+        o[z >> 6] ^= 1ull << (z & 63);
+        push(B);
+    }
 };
 
 // cpp/distfind/css.cpp:355-409
 bool matroid_partition(const Mat& code_gen, std::vector<std::vector<int>>& out) {
     const int n = code_gen.cols, K = code_gen.rows, kw = words_for(K);
+    // columns as bit vectors over the rows (transpose by the set bits of each row)
     std::vector<u64> col((size_t)n * kw, 0);
+    for (int i = 0; i < K; ++i) {
+        const u64* r = code_gen.row(i);
+        for (int w = 0; w < code_gen.stride; ++w)
+            for (u64 x = r[w]; x; x &= x - 1) {
+                const int j = w * 64 + __builtin_ctzll(x);
+                col[(size_t)j * kw + (i >> 6)] |= 1ull << (i & 63);
+            }
+    }
     std::vector<int> nonzero, zeros;
     for (int j = 0; j < n; ++j) {
-        u64* c = &col[(size_t)j * kw];
+        const u64* c = &col[(size_t)j * kw];
         bool nz = false;
-        for (int i = 0; i < K; ++i)
-            if (code_gen.get(i, j)) { c[i >> 6] |= 1ull << (i & 63); nz = true; }
+        for (int w = 0; w < kw; ++w) nz = nz || c[w] != 0;
         (nz ? nonzero : zeros).push_back(j);
     }
     std::vector<std::vector<int>> cls;
+    std::vector<ClassBasis> basis;
     std::vector<char> visited(n, 0);
-    Expresser express(kw, n);
+    Expresser express(kw, n, &col);
     std::function<bool(int, int)> place = [&](int z, int forbidden) -> bool {
         for (int c = 0; c < (int)cls.size(); ++c) {
             if (c == forbidden) continue;
-            if (!express(cls[c], col, z, false).in_span) { cls[c].push_back(z); return true; }
+            if (!express.query(basis[c], cls[c], z, false).in_span) {
+                cls[c].push_back(z);
+                express.append_queried(basis[c], z);
+                return true;
+            }
         }
         for (int c = 0; c < (int)cls.size(); ++c) {
             if (c == forbidden) continue;
-            Expr e = express(cls[c], col, z, true);
+            Expr e = express.query(basis[c], cls[c], z, true);
             if (!e.in_span) continue;
             for (int y : e.circuit) {
                 if (visited[y]) continue;
@@ -131,16 +159,21 @@ bool matroid_partition(const Mat& code_gen, std::vector<std::vector<int>>& out) 
                 std::vector<int>& v = cls[c];
                 v.erase(std::find(v.begin(), v.end(), y));
                 v.push_back(z);
+                basis[c].valid = false;
                 if (place(y, c)) return true;
                 v.erase(std::find(v.begin(), v.end(), z));
                 v.push_back(y);
+                basis[c].valid = false;
             }
         }
         return false;
     };
     for (int z : nonzero) {
         std::fill(visited.begin(), visited.end(), 0);
-        if (!place(z, -1)) cls.push_back({z});
+        if (!place(z, -1)) {
+            cls.push_back({z});
+            basis.emplace_back();
+        }
     }
     if (cls.empty()) cls.push_back({});
     for (int j : zeros) cls[0].push_back(j);
@@ -167,10 +200,11 @@ std::vector<InfoSet> gamma_sequence(const Mat& code_gen) {
     const int K = code_gen.rows, n = code_gen.cols;
     std::vector<InfoSet> greedy = greedy_sets(code_gen);
     if (K == 0) return greedy;
+    std::vector<u64> any(code_gen.stride, 0ull);   // columns holding a 1 in some row
+    for (int i = 0; i < K; ++i) vec_or(any.data(), code_gen.row(i), code_gen.stride);
     int nnz = 0;
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i < K; ++i)
-            if (code_gen.get(i, j)) { ++nnz; break; }
+    for (int w = 0; w < code_gen.stride; ++w) nnz += popc64(any[w]);
+    (void)n;
     const int max_full = nnz / K;
     const int greedy_full = count_full(greedy, K);
     if (greedy_full >= max_full || n > 200) return greedy;

@@ -20,12 +20,17 @@ struct Reducer {
     Mat rows;
     std::vector<int> piv;
     explicit Reducer(int cols) : rows(0, cols) {}
+    // Branchless: whether a basis row applies is data, so a branch on it mispredicts.
     bool reduce(u64* v) const {
+        const int st = rows.stride;
+        const u64* base = rows.w.data();
         for (int i = 0; i < rows.rows; ++i) {
             const int p = piv[i];
-            if ((v[p >> 6] >> (p & 63)) & 1u) vec_xor(v, rows.row(i), rows.stride);
+            const u64 mask = 0ull - ((v[p >> 6] >> (p & 63)) & 1u);
+            const u64* r = base + (size_t)i * st;
+            for (int k = 0; k < st; ++k) v[k] ^= r[k] & mask;
         }
-        return !vec_zero(v, rows.stride);
+        return !vec_zero(v, st);
     }
     void add(const u64* reduced) {
         rows.append_row(reduced);
@@ -93,13 +98,14 @@ namespace {
 // Rows of ko = nullspace(other) independent of rowspan(self) (cpp/distfind/css.cpp:175-186).
 Mat quotient_of(const Mat& self, const Mat& ko) {
     Reducer basis(self.cols);
+    std::vector<u64> t(std::max(1, self.stride));
     for (int i = 0; i < self.rows; ++i) {
-        std::vector<u64> t(self.row(i), self.row(i) + self.stride);
+        std::copy(self.row(i), self.row(i) + self.stride, t.begin());
         if (basis.reduce(t.data())) basis.add(t.data());
     }
     Mat out(0, self.cols);
     for (int i = 0; i < ko.rows; ++i) {
-        std::vector<u64> t(ko.row(i), ko.row(i) + ko.stride);
+        std::copy(ko.row(i), ko.row(i) + ko.stride, t.begin());
         if (!basis.reduce(t.data())) continue;
         basis.add(t.data());
         out.append_row(ko.row(i));
