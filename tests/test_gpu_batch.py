@@ -108,7 +108,7 @@ def test_one_shot_pipeline_equals_single_batch(native):
     prepared batch executed as a whole."""
     from qubitserf_b200 import workloads as W
     items = native.batch_items(W.batch_1024(300))
-    ans, st = native.Batch(items).run()                 # pipelined (3 chunks)
+    ans, st = native.Batch(items).run()                 # pipelined (2 chunks)
     b = native.Batch(items)
     h = b.prepare()
     ref, st2 = b.execute(h)                             # one batch
@@ -119,3 +119,25 @@ def test_one_shot_pipeline_equals_single_batch(native):
             (r.distance, r.lower_bound, r.proven, r.levels, r.z_weight, r.x_weight)
         assert a.witness_ok == 1
     assert st.codewords == st2.codewords
+
+
+def test_job_groups_do_not_change_answers(native):
+    """Execute steps the jobs as interleaved groups (QSFB_EXEC_GROUPS, each on its own
+    stream and host thread); one group and four groups give the same answers, levels and
+    codeword counts, and every group's witnesses verify."""
+    import os
+    from qubitserf_b200 import workloads as W
+    b = native.Batch(native.batch_items(W.batch_1024(400)))
+    h = b.prepare()
+    out = {}
+    try:
+        for g in ("1", "4"):
+            os.environ["QSFB_EXEC_GROUPS"] = g
+            a, st = b.execute(h)
+            out[g] = ([(x.distance, x.lower_bound, x.proven, x.levels, x.z_weight, x.x_weight,
+                        x.witness_ok) for x in a], st.codewords, st.certificates)
+    finally:
+        os.environ.pop("QSFB_EXEC_GROUPS", None)
+        b.free(h)
+    assert out["1"] == out["4"]
+    assert all(t[-1] == 1 for t in out["4"][0])
