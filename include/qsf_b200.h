@@ -220,7 +220,10 @@ void qsfb_batch_free(QsfbBatchHandle* handle);
  * at most max_active are in flight and their summed device footprint (rows + all subset
  * lists their levels will build) stays within mem_budget_bytes (0 = 64 GiB), runs one
  * fused round over all admitted queries' next levels, and completes each query as soon as
- * it is proven.  Answers equal qsfb_batch's for the same query, alone or in any mix. */
+ * it is proven.  Answers equal qsfb_batch's for the same query, alone or in any mix.
+ * intake_threads = 0: all host cores but two.  For steady latencies start the process with
+ * CUDA_MODULE_LOADING=EAGER (with lazy loading a kernel variant loads at its first launch,
+ * which a request then waits for) and warm the server up with a few queries. */
 typedef struct QsfbServer QsfbServer;
 typedef struct {
     double submit_s, ready_s, admit_s, done_s;   /* seconds since the server started */

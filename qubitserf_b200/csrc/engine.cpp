@@ -212,7 +212,7 @@ void* Arena::alloc(size_t bytes) {
     std::lock_guard<std::mutex> lk(mu_);
     bytes = align_up(std::max<size_t>(bytes, 16), 256);
     if (chunks_.empty() || used_ + bytes > chunks_.back().second) {
-        const size_t sz = round_bucket(std::max<size_t>(bytes, 64ull << 20));
+        const size_t sz = round_bucket(std::max<size_t>(bytes, min_chunk_));
         char* p = (char*)dev_->alloc(sz);
         if (!p) return nullptr;
         chunks_.push_back({p, sz});

@@ -124,7 +124,9 @@ struct ListBuf {
 // from it is released together when the arena is destroyed (one batch).
 class Arena {
 public:
-    explicit Arena(Device* d) : dev_(d) {}
+    // min_chunk: smallest device chunk taken from the caching allocator (a whole batch
+    // carves from 64 MiB chunks; a single serving request from much smaller ones)
+    explicit Arena(Device* d, size_t min_chunk = 64ull << 20) : dev_(d), min_chunk_(min_chunk) {}
     Arena(const Arena&) = delete;
     Arena& operator=(const Arena&) = delete;
     ~Arena();
@@ -133,6 +135,7 @@ public:
 
 private:
     Device* dev_;
+    size_t min_chunk_;
     std::mutex mu_;   // the rounds of several job groups may carve lists concurrently
     std::vector<std::pair<char*, size_t>> chunks_;
     size_t used_ = 0, total_ = 0;

@@ -152,6 +152,9 @@ struct QsfbServer {
 
     void intake_loop() {
         SessionLease lease(dev);
+        // staging reserved up front: growing pinned host memory later (cudaFreeHost +
+        // cudaMallocHost) would synchronise the device under the engine's rounds
+        if (lease.s) lease.s->ensure(1u << 20, 4u << 20);
         for (;;) {
             Request* r = nullptr;
             {
@@ -164,7 +167,9 @@ struct QsfbServer {
             build_jobs(r);
             std::vector<BzJob*> ptrs;
             for (auto& j : r->jobs) ptrs.push_back(j.get());
-            r->arena.reset(new Arena(dev));
+            // 1 MiB chunks: a request's rows, seeds and lists are small, and its footprint
+            // (which the admission budget counts) is the chunks it holds
+            r->arena.reset(new Arena(dev, 1ull << 20));
             int rc = lease.s ? setup_jobs(dev, lease.s, r->arena.get(), ptrs, 1, nullptr) : kErrDevice;
             size_t fp = r->arena->bytes();
             for (BzJob* j : ptrs)
@@ -216,6 +221,7 @@ struct QsfbServer {
 
     void engine_loop() {
         SessionLease lease(dev);
+        if (lease.s) lease.s->ensure(32u << 20, 32u << 20);   // see intake_loop
         std::vector<LevelReq> q;
         std::vector<int> side, owner;
         std::vector<LevelOut> outs;
@@ -306,7 +312,10 @@ int qsfb_server_start(int intake_threads, long long mem_budget_bytes, int max_ac
     S->budget = mem_budget_bytes > 0 ? (size_t)mem_budget_bytes : (size_t)64 << 30;
     S->max_active = max_active > 0 ? max_active : 4096;
     S->t0 = now_seconds();
-    int nt = intake_threads > 0 ? intake_threads : (int)std::thread::hardware_concurrency();
+    // default: all cores but two (the engine thread and the caller's submitting thread
+    // must not wait for a core behind the intake work)
+    int nt = intake_threads > 0 ? intake_threads
+                                : (int)std::thread::hardware_concurrency() - 2;
     nt = std::max(1, nt);
     for (int t = 0; t < nt; ++t) S->intake.emplace_back(&QsfbServer::intake_loop, S);
     S->engine = std::thread(&QsfbServer::engine_loop, S);
