@@ -5,7 +5,8 @@
 // registers, row i on lane i%32 slot i/32, and is put in restricted row-echelon form over
 // the trial's column order with the reference's pivot rule (first row at or below the rank
 // with a 1 in the column, swapped into position `rank`, then cleared from every other
-// row).  Per column: four ballots, one pivot broadcast by shuffle, one masked XOR per slot.
+// row).  Per column: one ballot per 32-row slot in use, one pivot broadcast by shuffle, one
+// masked XOR per slot in use.
 // The lightest logical nonzero row of every trial is folded into the side's 32-bit key
 // (weight:17 | trial:8 | row:7) with one atomicMin per warp.
 #include <cuda_runtime.h>
@@ -49,6 +50,7 @@ __global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __rest
     const SeedDesc& D = descs[lo];
     const int t = gt - D.trial_base;
     const int K = D.K, n = D.n;
+    const int S = (K + 31) >> 5;   // row slots in use (warp-uniform): the rest stay zero
 
     unsigned long long r[4][W];
 #pragma unroll
@@ -66,10 +68,13 @@ __global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __rest
         unsigned b[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
-            unsigned long long v = 0;
+            b[s] = 0u;
+            if (s < S) {
+                unsigned long long v = 0;
 #pragma unroll
-            for (int w = 0; w < W; ++w) if (w == wd) v = r[s][w];
-            b[s] = __ballot_sync(0xffffffffu, (v & bit) != 0ull);
+                for (int w = 0; w < W; ++w) if (w == wd) v = r[s][w];
+                b[s] = __ballot_sync(0xffffffffu, (v & bit) != 0ull);
+            }
         }
         int sel = -1;
 #pragma unroll
@@ -93,6 +98,7 @@ __global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __rest
         if (lane == rl) put_slot<W>(r, rs, pv);   // pivot row moves to `rank`
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
+            if (s >= S) continue;
             const int row = 32 * s + lane;
             unsigned long long v = 0;
 #pragma unroll
