@@ -3,13 +3,15 @@ roofline of the dominant pair-sweep kernel (the tcgen05 int8 sweep of full-rank 
 CUDA-core POPC sweep's integer-pipe roofline is reported beside it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--mode batch|plain] [--codes 1024]
+                    [--codes 1024] [--workload batch|collect|mitm|css128|...]
 
 A step certifies every code of the batch (512 classical [n in 48..128, k in n/4..n/2] +
 512 CSS [n in 40..128, ranks in n/5..n/3], seed 3; CSS codes solved with which='min').
 `value` is certificates per second from device time with the inputs resident; `e2e` is
 the same metric through the public C ABI from host matrices (host<->device copies inside
-the timed region).  Under torchrun every rank certifies its own copy of the batch
+the timed region).  Beside them: the plain per-code drop-in over the same batch, the
+reference's own plain per-code GPU path (its CUDA backend built for sm_100a) and its CPU
+path on the host cores.  Under torchrun every rank certifies its own copy of the batch
 (weak scaling, no collective on the data path); timing is the max over ranks.
 """
 from __future__ import annotations
@@ -164,6 +166,41 @@ def cpu_baseline_sample(codes, budget_s=20.0, start=0):
                       f"1024-code batch (classical/CSS alternating) in {dt:.1f} s"}
 
 
+def plain_reference_gpu(codes, ans, budget_s=60.0):
+    """The reference's own plain per-code GPU path: its distfind_* calls with backend "gpu"
+    on its CUDA backend (cpp/qsf/cuda/backend_cuda.cu, built for sm_100a from its sources
+    into oracle/_ref/libqubitserf_cuda.so), one code after another over the batch in index
+    order until the budget is spent.  Levels of fewer than 2^18 codewords run on its CPU
+    backend on all host threads, as the reference dispatches them.  Every result
+    (distance, lower bound, proven, levels) is compared with the batched engine's answer on
+    the same host."""
+    from oracle.refbind import REF_CUDA_LIB, RefCuda
+    if not REF_CUDA_LIB.exists():
+        return {"unavailable": "oracle/_ref/libqubitserf_cuda.so not built"}
+    eng = RefCuda()
+    if not eng.available():
+        return {"unavailable": "the reference's CUDA backend reports no device"}
+    eng.classical(codes[0].mats[0])   # context and module load outside the timed loop
+    t0 = time.perf_counter()
+    done, same = 0, 0
+    for cs, a in zip(codes, ans):
+        if cs.kind == "classical":
+            r = eng.classical(cs.mats[0])
+        else:
+            r = eng.css(cs.mats[0], cs.mats[1])
+        same += (r.distance, r.lower_bound, r.proven, r.levels) == \
+                (a.distance, a.lower_bound, a.proven, a.levels)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "certs/s", "codes": done, "seconds": dt,
+            "results_equal": same, "host_threads": os.cpu_count(),
+            "source": "reference distfind_* with backend gpu: its bz_enumerate kernel "
+                      "(backend_cuda.cu) built for sm_100a, levels under 2^18 codewords "
+                      "on its CPU backend"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,6 +209,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--codes", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain-reference", action="store_true",
+                    help="skip the reference's own per-code GPU path over the batch")
     ap.add_argument("--ref-budget", type=float, default=15.0,
                     help="seconds of reference CPU work per reference-arm step")
     ap.add_argument("--only-resident", action="store_true",
@@ -340,6 +379,7 @@ def main():
     if rank != 0:
         return
     cpu = None if args.no_cpu_baseline else cpu_baseline_sample(codes)
+    pref = None if args.no_plain_reference else plain_reference_gpu(codes, ans)
     line = {
         "metric": METRIC, "value": value, "unit": "certs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -347,6 +387,9 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i8",
         "data": "synthetic", "config": config,
         "plain_certs_per_s": plain, "batched_vs_plain": value / plain,
+        "plain_reference_gpu": pref,
+        "batched_vs_plain_reference": (value / pref["value"]) if pref and "value" in pref
+                                      else None,
         "gcodewords_per_s": achieved_cw / 1e9,
         "codewords_per_step": cw / args.steps, "rounds_per_step": rounds,
         "roofline": {

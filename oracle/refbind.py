@@ -4,10 +4,16 @@
   ``oracle/_ref/libqubitserf.so`` by ``oracle/Makefile``; its ``distfind_*`` ABI is the
   one in the reference's ``cpp/distfind/capi.h:12-111``, plus the two shim entry points of
   ``oracle/ref_shim.cpp``.
+* ``RefCuda`` -- the same sources with the reference's own CUDA backend
+  (``cpp/qsf/cuda/backend_cuda.cu``) compiled for sm_100a, as its CMake build does when a
+  CUDA toolkit is present (``CMakeLists.txt:86-90``): ``oracle/_ref/libqubitserf_cuda.so``,
+  called with ``backend="gpu"``.  It is the plain per-code GPU path that the batched
+  engine is compared with.
 * ``Oracle`` -- the C restatement ``oracle/libbzoracle.so`` (``oracle/bz_oracle.c``).
 
-Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg import this
-module, and only as the checker.  The product library never loads either file.
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s baseline legs import this
+module, and only as the checker or the timed comparator.  The product library never loads
+any of these files.
 """
 from __future__ import annotations
 
@@ -19,6 +25,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libqubitserf.so"
+REF_CUDA_LIB = HERE / "_ref" / "libqubitserf_cuda.so"
 ORACLE_LIB = HERE / "libbzoracle.so"
 
 WEIGHT_NONE = 1 << 30
@@ -65,7 +72,9 @@ def ref_available() -> bool:
 
 
 class Ref:
-    """The reference CPU library (``backend`` is always "cpu")."""
+    """The reference library on its CPU backend."""
+
+    backend = b"cpu"
 
     def __init__(self, path: Path = REF_LIB):
         self.lib = ctypes.CDLL(str(path), mode=os.RTLD_LOCAL)
@@ -108,7 +117,7 @@ class Ref:
     def classical(self, H, threads=0, method="bz"):
         a = u8(H)
         out = DistfindResult()
-        rc = self.lib.distfind_classical_distance(_p(a), a.shape[0], a.shape[1], method.encode(), b"cpu",
+        rc = self.lib.distfind_classical_distance(_p(a), a.shape[0], a.shape[1], method.encode(), self.backend,
                                                   threads, 0, ctypes.byref(out))
         assert rc == 0
         return out
@@ -118,7 +127,7 @@ class Ref:
         out = DistfindResult()
         rc = self.lib.distfind_css_distance(_p(ax), ax.shape[0], ax.shape[1], _p(az),
                                             az.shape[0], az.shape[1], method.encode(), which.encode(),
-                                            b"cpu", threads, 0, ctypes.byref(out))
+                                            self.backend, threads, 0, ctypes.byref(out))
         assert rc == 0
         return out
 
@@ -127,7 +136,7 @@ class Ref:
         out = DistfindResult()
         rc = self.lib.distfind_subsystem_distance(_p(ax), ax.shape[0], ax.shape[1], _p(az),
                                                   az.shape[0], az.shape[1], method.encode(),
-                                                  which.encode(), b"cpu", threads, 0,
+                                                  which.encode(), self.backend, threads, 0,
                                                   ctypes.byref(out))
         assert rc == 0
         return out
@@ -138,7 +147,7 @@ class Ref:
         out = DistfindOpResult()
         rc = self.lib.distfind_operator_weight(_p(ax), ax.shape[0], ax.shape[1], _p(az),
                                                az.shape[0], az.shape[1], _p(zz), _p(xx),
-                                               ax.shape[1], method.encode(), b"cpu", threads, 0,
+                                               ax.shape[1], method.encode(), self.backend, threads, 0,
                                                ctypes.byref(out))
         assert rc == 0
         return out
@@ -147,7 +156,7 @@ class Ref:
         a = u8(S)
         out = DistfindResult()
         rc = self.lib.distfind_stabilizer_distance(_p(a), a.shape[0], a.shape[1], method.encode(),
-                                                   which.encode(), b"cpu", threads, 0,
+                                                   which.encode(), self.backend, threads, 0,
                                                    ctypes.byref(out))
         return rc, out
 
@@ -155,7 +164,7 @@ class Ref:
         a = u8(G)
         out = DistfindResult()
         rc = self.lib.distfind_subsystem_stabilizer_distance(_p(a), a.shape[0], a.shape[1],
-                                                             method.encode(), which.encode(), b"cpu",
+                                                             method.encode(), which.encode(), self.backend,
                                                              threads, 0, ctypes.byref(out))
         return rc, out
 
@@ -164,7 +173,7 @@ class Ref:
         o = u8(op).reshape(-1)
         out = DistfindResult()
         rc = self.lib.distfind_stabilizer_operator_weight(_p(a), a.shape[0], a.shape[1], _p(o),
-                                                          o.shape[0], method.encode(), b"cpu", threads, 0,
+                                                          o.shape[0], method.encode(), self.backend, threads, 0,
                                                           ctypes.byref(out))
         return rc, out
 
@@ -232,6 +241,22 @@ class Ref:
             return rows[:cnt], int(L.codeaut_bz_combos(h))
         finally:
             L.codeaut_bz_free(h)
+
+class RefCuda(Ref):
+    """The reference library built with its CUDA backend, called with backend "gpu": its
+    levels of at least 2^18 codewords run on ``bz_enumerate`` (``backend_cuda.cu:133-205``),
+    smaller ones on its CPU backend (``backend_cuda.cu:518-521``)."""
+
+    backend = b"gpu"
+
+    def __init__(self, path: Path = REF_CUDA_LIB):
+        super().__init__(path)
+        self.lib.distfind_backend_available.argtypes = [ctypes.c_char_p]
+        self.lib.distfind_backend_available.restype = ctypes.c_int
+
+    def available(self) -> bool:
+        return self.lib.distfind_backend_available(b"gpu") == 1
+
 
 class OrcResult(ctypes.Structure):
     _fields_ = [("distance", ctypes.c_int), ("lower_bound", ctypes.c_int),
