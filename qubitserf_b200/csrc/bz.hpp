@@ -52,7 +52,7 @@ struct BzResult {
     std::vector<LevelRecord> trace;
 };
 
-// Upper bound from `trials` random column orders (reference cpp/distfind/bz.cpp:70-116):
+// Upper bound from `trials` random column orders (reference cpp/distfind/bz.cpp:24-70):
 // same generator, seeds and split of the trials over hardware_concurrency() streams, so
 // the bound equals the reference's on the same host.  parallel=false replays the streams
 // one after another (same result).  `word` receives a logical row achieving the bound.

@@ -1,12 +1,14 @@
 // Random-information-set upper bound on the device: the GF(2) elimination half of the
-// reference's random_is_seed (cpp/distfind/bz.cpp:70-116).  The host draws the column
-// orders exactly as the reference does (std::mt19937 + std::shuffle per stream); here one
-// warp takes one trial: the K x n code generator (K <= 128 rows, n <= 128 columns) sits in
-// registers, row i on lane i%32 slot i/32, and is put in restricted row-echelon form over
-// the trial's column order with the reference's pivot rule (first row at or below the rank
-// with a 1 in the column, swapped into position `rank`, then cleared from every other
-// row).  Per column: one ballot per 32-row slot in use, one pivot broadcast by shuffle, one
-// masked XOR per slot in use.
+// reference's random_is_seed (cpp/distfind/bz.cpp:24-70, the trial loop at :36-51).  The
+// host draws the column orders exactly as the reference does (std::mt19937 + std::shuffle
+// per stream); here one warp takes one trial: the K x n code generator (K <= 128 rows,
+// n <= 128 columns) sits in registers, row i on lane i%32 slot i/32, and is put in
+// restricted row-echelon form over the trial's column order with the reference's pivot rule
+// (first row at or below the rank with a 1 in the column, swapped into position `rank`,
+// then cleared from every other row).  The number of slots in use, S = ceil(K/32), is a
+// compile-time constant of the trial's body (one body per S, chosen per trial).  Per
+// column: the column index from a register by shuffle, one ballot per slot, one pivot
+// broadcast by shuffle, one masked XOR per slot.
 // The lightest logical nonzero row of every trial is folded into the side's 32-bit key
 // (weight:17 | trial:8 | row:7) with one atomicMin per warp.
 #include <cuda_runtime.h>
@@ -17,92 +19,84 @@
 namespace qsfb {
 namespace dev {
 
-template <int W>
-__device__ __forceinline__ void get_slot(const unsigned long long (&r)[4][W], int s,
+template <int W, int S>
+__device__ __forceinline__ void get_slot(const unsigned long long (&r)[S][W], int s,
                                          unsigned long long (&out)[W]) {
 #pragma unroll
-    for (int w = 0; w < W; ++w)
-        out[w] = s == 0 ? r[0][w] : s == 1 ? r[1][w] : s == 2 ? r[2][w] : r[3][w];
+    for (int w = 0; w < W; ++w) {
+        out[w] = r[0][w];
+#pragma unroll
+        for (int q = 1; q < S; ++q)
+            if (q == s) out[w] = r[q][w];
+    }
 }
 
-template <int W>
-__device__ __forceinline__ void put_slot(unsigned long long (&r)[4][W], int s,
+template <int W, int S>
+__device__ __forceinline__ void put_slot(unsigned long long (&r)[S][W], int s,
                                          const unsigned long long (&v)[W]) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < S; ++q)
         if (q == s) {
 #pragma unroll
             for (int w = 0; w < W; ++w) r[q][w] = v[w];
         }
 }
 
-template <int W>
-__global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __restrict__ descs,
-                                                          int ndesc, int total_trials) {
-    const int lane = threadIdx.x & 31;
-    const int gt = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (gt >= total_trials) return;
-    int lo = 0, hi = ndesc - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (descs[mid].trial_base <= gt) lo = mid; else hi = mid - 1;
-    }
-    const SeedDesc& D = descs[lo];
-    const int t = gt - D.trial_base;
+// One trial with the K rows in S slots of 32 (K <= 32 S): S and W fixed at compile time,
+// so every per-column step touches only the slots in use.
+template <int W, int S>
+__device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
     const int K = D.K, n = D.n;
-    const int S = (K + 31) >> 5;   // row slots in use (warp-uniform): the rest stay zero
-
-    unsigned long long r[4][W];
+    unsigned long long r[S][W];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < S; ++s) {
         const int row = 32 * s + lane;
 #pragma unroll
         for (int w = 0; w < W; ++w) r[s][w] = row < K ? __ldg(D.gen + (size_t)row * W + w) : 0ull;
     }
+    // the trial's column order (n <= 128 bytes): bytes 4 lane .. 4 lane + 3 on this lane
     const uint8_t* perm = D.perm + (size_t)t * n;
+    uint32_t pw = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int c = 4 * lane + j;
+        if (c < n) pw |= (uint32_t)__ldg(perm + c) << (8 * j);
+    }
     int rank = 0;
     for (int ci = 0; ci < n && rank < K; ++ci) {
-        const int col = __ldg(perm + ci);
+        const int col = (int)((__shfl_sync(0xffffffffu, pw, ci >> 2) >> (8 * (ci & 3))) & 0xffu);
         const int wd = col >> 6;
         const unsigned long long bit = 1ull << (col & 63);
-        unsigned b[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            b[s] = 0u;
-            if (s < S) {
-                unsigned long long v = 0;
-#pragma unroll
-                for (int w = 0; w < W; ++w) if (w == wd) v = r[s][w];
-                b[s] = __ballot_sync(0xffffffffu, (v & bit) != 0ull);
-            }
-        }
+        // the first row at or below `rank` with a 1 in the column
         int sel = -1;
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            unsigned m = b[s];
+        for (int s = S - 1; s >= 0; --s) {
+            unsigned long long v = r[s][0];
+#pragma unroll
+            for (int w = 1; w < W; ++w) if (w == wd) v = r[s][w];
+            unsigned m = __ballot_sync(0xffffffffu, (v & bit) != 0ull);
             const int first = 32 * s;
             if (rank >= first + 32) m = 0u;
-            else if (rank > first) m &= ~((1u << (rank - first)) - 1u);
-            if (sel < 0 && m) sel = first + __ffs(m) - 1;
+            else if (rank > first) m &= ~0u << (rank - first);
+            if (m) sel = first + __ffs(m) - 1;
         }
         if (sel < 0) continue;
         const int ps = sel >> 5, pl = sel & 31, rs = rank >> 5, rl = rank & 31;
         unsigned long long pv[W], ov[W], tmp[W];
-        get_slot<W>(r, ps, tmp);
+        get_slot<W, S>(r, ps, tmp);
 #pragma unroll
         for (int w = 0; w < W; ++w) pv[w] = __shfl_sync(0xffffffffu, tmp[w], pl);
-        get_slot<W>(r, rs, tmp);
+        get_slot<W, S>(r, rs, tmp);
 #pragma unroll
         for (int w = 0; w < W; ++w) ov[w] = __shfl_sync(0xffffffffu, tmp[w], rl);
-        if (lane == pl) put_slot<W>(r, ps, ov);   // old row `rank` moves to `sel`
-        if (lane == rl) put_slot<W>(r, rs, pv);   // pivot row moves to `rank`
+        if (lane == pl) put_slot<W, S>(r, ps, ov);   // old row `rank` moves to `sel`
+        if (lane == rl) put_slot<W, S>(r, rs, pv);   // pivot row moves to `rank`
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            if (s >= S) continue;
+        for (int s = 0; s < S; ++s) {
             const int row = 32 * s + lane;
-            unsigned long long v = 0;
+            unsigned long long v = r[s][0];
 #pragma unroll
-            for (int w = 0; w < W; ++w) if (w == wd) v = r[s][w];
+            for (int w = 1; w < W; ++w) if (w == wd) v = r[s][w];
             if (row != rank && (v & bit)) {
 #pragma unroll
                 for (int w = 0; w < W; ++w) r[s][w] ^= pv[w];
@@ -114,7 +108,7 @@ __global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __rest
     // lightest logical nonzero row of this trial
     unsigned key = 0xffffffffu;
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < S; ++s) {
         const int row = 32 * s + lane;
         if (row >= K) continue;
         int wt = 0;
@@ -138,6 +132,28 @@ __global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __rest
         key = o < key ? o : key;
     }
     if (lane == 0 && key != 0xffffffffu) atomicMin(D.key, key);
+}
+
+template <int W>
+__global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __restrict__ descs,
+                                                          int ndesc, int total_trials) {
+    const int lane = threadIdx.x & 31;
+    const int gt = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (gt >= total_trials) return;
+    int lo = 0, hi = ndesc - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].trial_base <= gt) lo = mid; else hi = mid - 1;
+    }
+    const SeedDesc& D = descs[lo];
+    const int t = gt - D.trial_base;
+    switch ((D.K + 31) >> 5) {   // row slots in use, uniform over the warp
+        case 0: return;
+        case 1: run_trial<W, 1>(D, t, lane); break;
+        case 2: run_trial<W, 2>(D, t, lane); break;
+        case 3: run_trial<W, 3>(D, t, lane); break;
+        default: run_trial<W, 4>(D, t, lane); break;
+    }
 }
 
 }  // namespace dev
