@@ -193,10 +193,12 @@ typedef struct {
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free.  Batches of 256 queries or more are pipelined in
- * chunks (two by default, QSFB_BATCH_CHUNKS to change; the host reduction and seeds of one
- * chunk run, on all host cores but four, while the device enumerates the previous one as
- * two job groups); the answers are those of one batch, and the stats sum the chunks
- * (rounds, codewords, phase times; device_bytes is the largest chunk's). */
+ * chunks (four by default, QSFB_BATCH_CHUNKS to change): the first, small chunk's rounds
+ * start at once as three job groups, and each later chunk, prepared meanwhile on all host
+ * cores but four, joins those groups at their next round boundary.  The answers are those
+ * of one batch; the stats give the merged rounds and sum the chunks' preparation phases
+ * (device_bytes: all chunks together).  QSFB_BATCH_TRACE prints each chunk's phase times
+ * to stderr. */
 int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
                QsfbBatchStats* stats);
 

@@ -558,15 +558,19 @@ int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& job
             trials += v[i]->seed_trials;
         }
         for (const auto& po : perm_off) std::memcpy(h + po.second, po.first->data(), po.first->size());
-        if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        // on the session's high-priority stream: in a pipelined batch or a server, the
+        // rounds of other codes fill the SMs meanwhile, and these codes wait for the result
+        const double tw0 = now_seconds();
+        if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s->urgent) != cudaSuccess ||
             launch_seed_trials(W, (const SeedDesc*)(d + off_desc), (int)v.size(), trials,
-                               s->stream) != cudaSuccess ||
+                               s->urgent) != cudaSuccess ||
             cudaMemcpyAsync(h + off_keys, d + off_keys, v.size() * 4, cudaMemcpyDeviceToHost,
-                            s->stream) != cudaSuccess ||
-            cudaStreamSynchronize(s->stream) != cudaSuccess) {
+                            s->urgent) != cudaSuccess ||
+            cudaStreamSynchronize(s->urgent) != cudaSuccess) {
             cudaGetLastError();
             return kErrDevice;
         }
+        if (stats) stats->device_seed_wait_s += now_seconds() - tw0;
         for (size_t i = 0; i < v.size(); ++i) v[i]->apply_device_seed(hk[i]);
         if (stats) stats->launches += 1;
     }
@@ -610,7 +614,7 @@ int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
 
 
 int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* rounds,
-               double* span_ms) {
+               double* span_ms, const JobFeed* feed) {
     int nround = 0;
     std::vector<LevelReq> q;
     std::vector<int> side, owner;
@@ -623,6 +627,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
     }
     int rc = kOk;
     for (;;) {
+        if (feed) (*feed)(jobs, false);
         bool any = false;
         q.clear(); side.clear(); owner.clear();
         for (size_t j = 0; j < jobs.size(); ++j) {
@@ -632,7 +637,10 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             jobs[j]->requests(q, side);
             for (size_t k = before; k < q.size(); ++k) owner.push_back((int)j);
         }
-        if (!any) break;
+        if (!any) {
+            if (feed && (*feed)(jobs, true)) continue;
+            break;
+        }
         ++nround;
         RunStats rs;
         outs.clear();

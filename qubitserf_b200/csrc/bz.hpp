@@ -153,8 +153,13 @@ int run_jobs(Device* dev, std::vector<BzJob*>& jobs, int host_threads, RunStats*
 // rounds repeatedly: host setup of every job + one upload into `arena`, then the rounds.
 int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
                int host_threads, RunStats* stats);
+// `feed` (optional) is called at the top of every round with idle = false and may append
+// jobs to `jobs` (they start from their first level in that round); when every job is done
+// it is called with idle = true, may block until it has more, and returns whether it
+// appended any (false ends the rounds).
+using JobFeed = std::function<bool(std::vector<BzJob*>&, bool idle)>;
 int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* rounds,
-               double* span_ms = nullptr);
+               double* span_ms = nullptr, const JobFeed* feed = nullptr);
 
 int bz_distance(Device* dev, const Problem& p, const BzOptions& opt, BzResult& r);
 int bz_min_interleaved(Device* dev, const Problem& pz, const Problem& px, const BzOptions& opt,

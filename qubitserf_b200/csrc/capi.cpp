@@ -6,6 +6,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 #include <cstdio>
 #include <cstdlib>
@@ -213,20 +215,66 @@ struct QsfbBatchHandle {
 
 namespace {
 
+// Chunks of a one-shot batch prepared while the first chunk's rounds run: a helper thread
+// publishes each prepared handle in order (nullptr if its preparation failed), and every
+// job group takes its round-robin share of each published chunk at its next round boundary,
+// so the chunks' rounds merge into one execution with one tail.
+struct ChunkFeed {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<QsfbBatchHandle*> ready;   // published chunks, in order
+    size_t total = 0;                      // chunks that will be published
+    void publish(QsfbBatchHandle* h) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            ready.push_back(h);
+        }
+        cv.notify_all();
+    }
+    // Group g of G: append its share of every chunk published since its last call
+    // (`taken` chunks so far).  Idle: wait until a chunk gives it a job or all are published.
+    bool take(std::vector<BzJob*>& jobs, size_t& taken, int g, int G, bool idle) {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            bool added = false;
+            for (; taken < ready.size(); ++taken) {
+                const QsfbBatchHandle* h = ready[taken];
+                if (!h) continue;
+                for (size_t j = (size_t)g; j < h->ptrs.size(); j += (size_t)G) {
+                    jobs.push_back(h->ptrs[j]);
+                    added = true;
+                }
+            }
+            if (added || !idle || ready.size() >= total) return added;
+            cv.wait(lk);
+        }
+    }
+};
+
 // The rounds of a prepared batch.  The jobs are independent, so they run as `groups`
 // interleaved job groups (QSFB_EXEC_GROUPS, default 3; jobs dealt round robin), each
 // stepping its own rounds on its own session and host thread: while one group's kernels
 // run, the others plan and apply on the host, which hides the host share of each round.
 // The span is the union over the groups, from one start event that every group's stream
 // waits on to the last group's end event.
+// With a feed, every group also takes its round-robin share of each chunk published
+// during the rounds (`total_jobs`, all chunks' jobs, sets the group count).
 int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_ms,
-                   int max_groups) {
+                   int max_groups, ChunkFeed* F = nullptr, size_t total_jobs = 0) {
     const char* ge = std::getenv("QSFB_EXEC_GROUPS");   // read per call (benchmarks switch it)
     const int groups_env = std::max(1, std::min(ge ? std::atoi(ge) : 3, 8));
-    const int G = std::max(1, std::min({groups_env, max_groups, (int)H->ptrs.size() / 64}));
-    if (G == 1) return run_rounds(H->lease->s, H->ptrs, rs, rounds, span_ms);
+    const size_t njobs = std::max(H->ptrs.size(), total_jobs);
+    const int G = std::max(1, std::min({groups_env, max_groups, (int)(njobs / 64)}));
+    std::vector<size_t> taken(G, 0);
+    std::vector<JobFeed> feeds;
+    for (int g = 0; g < G && F; ++g)
+        feeds.emplace_back([F, &taken, g, G](std::vector<BzJob*>& jobs, bool idle) {
+            return F->take(jobs, taken[g], g, G, idle);
+        });
     std::vector<std::vector<BzJob*>> part(G);
     for (size_t j = 0; j < H->ptrs.size(); ++j) part[j % G].push_back(H->ptrs[j]);
+    if (G == 1)
+        return run_rounds(H->lease->s, part[0], rs, rounds, span_ms, F ? &feeds[0] : nullptr);
     std::vector<std::unique_ptr<SessionLease>> extra;
     std::vector<Session*> sess{H->lease->s};
     for (int g = 1; g < G; ++g) {
@@ -252,7 +300,8 @@ int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_m
     std::vector<std::thread> th;
     for (int g = 0; g < G; ++g)
         th.emplace_back([&, g]() {
-            rcs[g] = run_rounds(sess[g], part[g], &st[g], &rr[g], nullptr);
+            rcs[g] = run_rounds(sess[g], part[g], &st[g], &rr[g], nullptr,
+                                F ? &feeds[g] : nullptr);
             if (cudaEventRecord(end[g], sess[g]->stream) != cudaSuccess) rcs[g] = kErrDevice;
         });
     for (std::thread& t : th) t.join();
@@ -286,17 +335,8 @@ int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_m
     return rc;
 }
 
-int batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats, int max_groups) {
-    if (!H || (!out && !H->map.empty())) return kErrNull;
-    const double t0 = now_seconds();
-    if (H->executed)
-        for (BzJob* j : H->ptrs) j->reset();
-    H->executed = true;
-    RunStats rs;
-    int rounds = 0;
-    double span = 0.0;
-    int rc = execute_groups(H, &rs, &rounds, &span, max_groups);
-    if (rc != kOk) return rc;
+// Witness rebuild, host verification and the per-query answers of an executed handle.
+void answers_of(QsfbBatchHandle* H, QsfbAnswer* out) {
     auto& jobs = H->jobs;
     // Results (witness rebuild + host verification) are independent per job: spread them
     // over the host cores.
@@ -339,26 +379,45 @@ int batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats, in
             a.z_weight = a.x_weight = -1;
         }
     }
+}
+
+// Execution figures of the rounds (whatever handles their jobs came from).
+void fill_exec_stats(const RunStats& rs, int rounds, double span, QsfbBatchStats* stats) {
+    stats->device_ms = rs.ms_gen + rs.ms_pairs;
+    stats->device_span_ms = span;
+    stats->pair_ms = rs.ms_pairs;
+    stats->tc_ms = rs.ms_tc;
+    stats->codewords = rs.codewords;
+    stats->popc_issued = rs.popc_issued;
+    stats->zero_codewords = rs.zero_codewords;
+    stats->tc_codewords = rs.tc_codewords;
+    stats->rounds = rounds;
+    stats->kernel_launches = rs.launches;
+    stats->gen_ms = rs.ms_gen;
+    stats->host_plan_seconds = rs.host_plan_s;
+    stats->host_apply_seconds = rs.host_apply_s;
+}
+
+int batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats, int max_groups) {
+    if (!H || (!out && !H->map.empty())) return kErrNull;
+    const double t0 = now_seconds();
+    if (H->executed)
+        for (BzJob* j : H->ptrs) j->reset();
+    H->executed = true;
+    RunStats rs;
+    int rounds = 0;
+    double span = 0.0;
+    int rc = execute_groups(H, &rs, &rounds, &span, max_groups);
+    if (rc != kOk) return rc;
+    answers_of(H, out);
     if (stats) {
+        fill_exec_stats(rs, rounds, span, stats);
         stats->seconds = now_seconds() - t0;
         stats->prepare_seconds = H->prepare_s;
         stats->host_setup_seconds = H->setup.host_setup_s;
         stats->device_seed_seconds = H->setup.device_seed_s;
-        stats->device_ms = rs.ms_gen + rs.ms_pairs;
-        stats->device_span_ms = span;
-        stats->pair_ms = rs.ms_pairs;
-        stats->tc_ms = rs.ms_tc;
-        stats->codewords = rs.codewords;
-        stats->popc_issued = rs.popc_issued;
-        stats->zero_codewords = rs.zero_codewords;
-        stats->tc_codewords = rs.tc_codewords;
-        stats->rounds = rounds;
-        stats->kernel_launches = rs.launches;
-        stats->certificates = (int)jobs.size();
+        stats->certificates = (int)H->jobs.size();
         stats->device_bytes = (long long)H->arena->bytes();
-        stats->gen_ms = rs.ms_gen;
-        stats->host_plan_seconds = rs.host_plan_s;
-        stats->host_apply_seconds = rs.host_apply_s;
     }
     return kOk;
 }
@@ -722,19 +781,30 @@ int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stat
 
 void qsfb_batch_free(QsfbBatchHandle* H) { delete H; }
 
-// One-shot batch.  A large batch is cut into chunks and pipelined: while the rounds of
-// chunk k run on the device (this thread), a helper thread prepares chunk k + 1 (host
-// reduction on all cores, seed eliminations and upload on its own stream).  The first
-// chunk is small so the device starts early.  Codes are independent, so the answers are
-// those of one batch; at most two chunks hold device memory at a time.
+// One-shot batch.  A large batch is cut into chunks: the first (small, so the device
+// starts early) is prepared on all host cores and its rounds start; a helper thread
+// prepares the others in order (host reduction, seed eliminations and upload on its own
+// stream) and publishes each to the running job groups, which take their share of its jobs
+// at their next round boundary: the chunks' rounds merge into one execution with one tail.
+// Codes are independent and a job's answer depends only on its own levels, so the answers
+// are those of one batch.  1024-code batch, end to end: one piece 17.9-18.4k certs/s, two
+// chunks run one after the other 18.5-19.4k, merged (2-8 chunks, 3-4 groups) 20.0-20.7k;
+// separate job groups for the later chunks 17-19k; widest codes first no change.
 int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
                QsfbBatchStats* stats) {
     const double t0 = now_seconds();
+    const bool trace = std::getenv("QSFB_BATCH_TRACE") != nullptr;
+    long long alloc0[4] = {0, 0, 0, 0};
+    int trc = kOk;
+    Device* tdev = trace ? device_or(&trc) : nullptr;
+    if (tdev) {
+        alloc0[0] = tdev->n_device_malloc; alloc0[1] = tdev->ns_device_malloc;
+        alloc0[2] = tdev->n_pinned_alloc; alloc0[3] = tdev->ns_pinned_alloc;
+    }
     constexpr int kPipeMin = 256;   // below this the batch runs in one piece
-    // QSFB_BATCH_CHUNKS: number of pipeline chunks (default 2; 1 = one piece), read per
-    // call.  1024-code batch, end to end: 2 chunks 17.4-17.8k certs/s, 3 chunks 17.3-17.4k.
+    // QSFB_BATCH_CHUNKS: number of pipeline chunks (default 4; 1 = one piece), read per call.
     const char* ce = std::getenv("QSFB_BATCH_CHUNKS");
-    const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : 2, 16));
+    const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : 4, 64));
     std::vector<int> cut{0};
     if (nq >= kPipeMin && chunks > 1) {
         const int first = std::max(32, nq / (2 * chunks));
@@ -747,68 +817,84 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     const int nchunks = (int)cut.size() - 1;
     std::vector<QsfbBatchHandle*> H(nchunks, nullptr);
     std::vector<int> prc(nchunks, kOk);
-    // Preparations that run beside an execution leave four host cores to its job groups'
-    // round planning (QSFB_OVERLAP_PREP_THREADS to set the count); overlapped executions
-    // step QSFB_OVERLAP_GROUPS job groups (default 2).  Measured on the 1024-code batch (16
-    // host cores): all cores + 1 group 15.5-16.3k certs/s end to end, 12 cores + 2 groups
-    // 17.1-17.8k.
+    std::vector<double> tp0(nchunks), tp1(nchunks);
+    // Preparations that run beside the rounds leave four host cores to the job groups'
+    // round planning (QSFB_OVERLAP_PREP_THREADS to set the count); the merged execution
+    // steps QSFB_OVERLAP_GROUPS job groups (default 3).
     const char* pe = std::getenv("QSFB_OVERLAP_PREP_THREADS");
     const char* ge = std::getenv("QSFB_OVERLAP_GROUPS");
     const int all = host_threads > 0 ? host_threads
                                      : std::max(1, (int)std::thread::hardware_concurrency());
     const int overlap_threads = pe ? std::max(1, std::atoi(pe)) : std::max(1, all - 4);
-    const int overlap_groups = ge ? std::max(1, std::atoi(ge)) : 2;
+    const int overlap_groups = ge ? std::max(1, std::atoi(ge)) : 3;
     auto prepare = [&](int c) {
+        tp0[c] = now_seconds();
         prc[c] = qsfb_batch_prepare(queries + cut[c], cut[c + 1] - cut[c],
                                     c == 0 ? host_threads : overlap_threads, &H[c]);
+        tp1[c] = now_seconds();
     };
-    QsfbBatchStats total;
-    std::memset(&total, 0, sizeof(total));
-    int rc = kOk;
+    auto release = [&]() {
+        for (QsfbBatchHandle*& h : H) { qsfb_batch_free(h); h = nullptr; }
+    };
+    if (nchunks == 1) {
+        prepare(0);
+        if (prc[0] != kOk) return prc[0];
+        const int rc = batch_execute(H[0], out, stats, 8);
+        release();
+        if (stats) stats->seconds = now_seconds() - t0;
+        return rc;
+    }
     prepare(0);
-    for (int c = 0; c < nchunks; ++c) {
-        std::thread next;
-        if (c + 1 < nchunks) next = std::thread(prepare, c + 1);
-        if (rc == kOk) rc = prc[c];
-        if (rc == kOk) {
-            QsfbBatchStats st;
-            std::memset(&st, 0, sizeof(st));
-            // one job group while the next chunk is being prepared beside it (the groups'
-            // host threads would compete with the preparation), grouped for the last chunk
-            rc = batch_execute(H[c], out ? out + cut[c] : nullptr, &st,
-                               c + 1 < nchunks ? overlap_groups : 8);
-            total.prepare_seconds += st.prepare_seconds;
-            total.host_setup_seconds += st.host_setup_seconds;
-            total.device_seed_seconds += st.device_seed_seconds;
-            total.device_ms += st.device_ms;
-            total.device_span_ms += st.device_span_ms;
-            total.pair_ms += st.pair_ms;
-            total.tc_ms += st.tc_ms;
-            total.codewords += st.codewords;
-            total.popc_issued += st.popc_issued;
-            total.zero_codewords += st.zero_codewords;
-            total.tc_codewords += st.tc_codewords;
-            total.rounds += st.rounds;
-            total.kernel_launches += st.kernel_launches;
-            total.certificates += st.certificates;
-            total.device_bytes = std::max(total.device_bytes, st.device_bytes);
-            total.gen_ms += st.gen_ms;
-            total.host_plan_seconds += st.host_plan_seconds;
-            total.host_apply_seconds += st.host_apply_seconds;
+    if (prc[0] != kOk) return prc[0];
+    ChunkFeed F;
+    F.total = (size_t)(nchunks - 1);
+    std::thread helper([&]() {
+        for (int c = 1; c < nchunks; ++c) {
+            prepare(c);
+            F.publish(prc[c] == kOk ? H[c] : nullptr);
         }
-        qsfb_batch_free(H[c]);
-        H[c] = nullptr;
-        if (next.joinable()) next.join();
-    }
-    for (QsfbBatchHandle* h : H) qsfb_batch_free(h);
-    if (rc == kOk) {
+    });
+    RunStats rs;
+    int rounds = 0;
+    double span = 0.0;
+    const double te0 = now_seconds();
+    H[0]->executed = true;
+    int rc = execute_groups(H[0], &rs, &rounds, &span, overlap_groups, &F, (size_t)nq);
+    const double te1 = now_seconds();
+    helper.join();
+    for (int c = 0; c < nchunks && rc == kOk; ++c)
+        if (prc[c] != kOk) rc = prc[c];
+    if (rc == kOk && out)
+        for (int c = 0; c < nchunks; ++c) answers_of(H[c], out + cut[c]);
+    if (tdev)
+        std::fprintf(stderr, "qsfb_batch: %lld device allocations (%.2f ms), %lld pinned "
+                     "staging allocations (%.2f ms)\n", tdev->n_device_malloc - alloc0[0],
+                     1e-6 * (double)(tdev->ns_device_malloc - alloc0[1]),
+                     tdev->n_pinned_alloc - alloc0[2],
+                     1e-6 * (double)(tdev->ns_pinned_alloc - alloc0[3]));
+    if (trace)   // one stderr line per chunk (ms from the call)
         for (int c = 0; c < nchunks; ++c)
-            if (prc[c] != kOk) { rc = prc[c]; break; }
-    }
-    if (stats) {
-        *stats = total;
+            std::fprintf(stderr, "qsfb_batch chunk %d: %d codes, prepare %.2f-%.2f ms (host "
+                         "reduction %.2f ms, device seeds %.2f ms of which %.2f waiting); "
+                         "rounds %.2f-%.2f ms\n", c,
+                         cut[c + 1] - cut[c], 1e3 * (tp0[c] - t0), 1e3 * (tp1[c] - t0),
+                         H[c] ? 1e3 * H[c]->setup.host_setup_s : 0.0,
+                         H[c] ? 1e3 * H[c]->setup.device_seed_s : 0.0,
+                         H[c] ? 1e3 * H[c]->setup.device_seed_wait_s : 0.0, 1e3 * (te0 - t0),
+                         1e3 * (te1 - t0));
+    if (stats && rc == kOk) {
+        std::memset(stats, 0, sizeof(*stats));
+        fill_exec_stats(rs, rounds, span, stats);
+        for (QsfbBatchHandle* h : H) {
+            stats->prepare_seconds += h->prepare_s;
+            stats->host_setup_seconds += h->setup.host_setup_s;
+            stats->device_seed_seconds += h->setup.device_seed_s;
+            stats->certificates += (int)h->jobs.size();
+            stats->device_bytes += (long long)h->arena->bytes();
+        }
         stats->seconds = now_seconds() - t0;
     }
+    release();
     return rc;
 }
 

@@ -114,7 +114,11 @@ void* Device::alloc(size_t bytes) {
     }
     cudaSetDevice(id);
     void* p = nullptr;
-    if (cudaMalloc(&p, b) != cudaSuccess) {
+    const double tm0 = now_seconds();
+    const cudaError_t me = cudaMalloc(&p, b);
+    n_device_malloc.fetch_add(1);
+    ns_device_malloc.fetch_add((long long)((now_seconds() - tm0) * 1e9));
+    if (me != cudaSuccess) {
         cudaGetLastError();
         // Drop the cache and retry once.
         std::multimap<size_t, void*> drop;
@@ -155,7 +159,14 @@ Session* Device::acquire() {
     cudaSetDevice(id);
     Session* s = new Session();
     s->dev = this;
+    int prio_least = 0, prio_greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) {
+        cudaGetLastError();
+        prio_greatest = 0;
+    }
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->urgent, cudaStreamNonBlocking, prio_greatest) !=
+            cudaSuccess ||
         cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess ||
         cudaEventCreate(&s->ev_tc0) != cudaSuccess || cudaEventCreate(&s->ev_tc1) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
@@ -186,9 +197,13 @@ int Session::ensure(size_t dbytes, size_t hbytes) {
         if (!d_stage.d) { d_stage.cap = 0; return kErrMemory; }
     }
     if (h_stage.cap < hbytes) {
+        const double tm0 = now_seconds();
         if (h_stage.h) cudaFreeHost(h_stage.h);
         h_stage.cap = round_bucket(hbytes);
-        if (cudaMallocHost(&h_stage.h, h_stage.cap) != cudaSuccess) {
+        const cudaError_t he = cudaMallocHost(&h_stage.h, h_stage.cap);
+        dev->n_pinned_alloc.fetch_add(1);
+        dev->ns_pinned_alloc.fetch_add((long long)((now_seconds() - tm0) * 1e9));
+        if (he != cudaSuccess) {
             cudaGetLastError();
             h_stage.h = nullptr;
             h_stage.cap = 0;

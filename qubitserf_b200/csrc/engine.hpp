@@ -11,6 +11,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -37,6 +38,8 @@ enum Status : int {
 
 struct Session;
 
+double now_seconds();   // steady clock, seconds
+
 class Device {
 public:
     // The process-wide device context; nullptr (with *rc = kErrDevice) without a GPU.
@@ -52,6 +55,10 @@ public:
     void release(void* p, size_t bytes);
     size_t bytes_in_use() const { return in_use_; }
     size_t bytes_cached() const { return cached_; }
+    // allocation calls that reach the driver (cache misses, pinned staging growth) and
+    // their wall time: both can stall other threads' work
+    std::atomic<long long> n_device_malloc{0}, ns_device_malloc{0};
+    std::atomic<long long> n_pinned_alloc{0}, ns_pinned_alloc{0};
 
     Session* acquire();
     void give_back(Session* s);
@@ -82,6 +89,10 @@ struct HostScratch {
 struct Session {
     Device* dev = nullptr;
     cudaStream_t stream = nullptr;
+    // the device's greatest stream priority: work that others wait on while rounds fill the
+    // SMs (the random-information-set seed eliminations of a preparation) goes here, so its
+    // blocks are scheduled first as SMs free up
+    cudaStream_t urgent = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_tc0 = nullptr, ev_tc1 = nullptr;   // around the tensor-core sweep
     // pair launches of a round are spread over these streams (forked after the list
@@ -200,6 +211,7 @@ struct RunStats {
     int launches = 0;
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)
+    double device_seed_wait_s = 0.0;   // of which: waiting for the copies and the kernel
     double host_plan_s = 0.0;     // run_levels host work before the launches
     double host_apply_s = 0.0;    // schedule updates after each round
 };
