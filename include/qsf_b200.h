@@ -290,6 +290,13 @@ int qsfb_flush_l2(void);
 const char* qsfb_device_name(void);
 int qsfb_device_sms(void);
 
+/* Allocation calls that reached the CUDA driver since the device was opened (cache misses of
+ * the device allocator; growth of sessions' pinned staging, which frees the old buffer
+ * with a device-wide synchronisation), with their wall time in nanoseconds:
+ * out[0] device allocations, out[1] their ns, out[2] pinned allocations, out[3] their ns.
+ * Returns 0, 1 (null) or 4 (no device). */
+int qsfb_alloc_counters(long long* out);
+
 /* ---------------------------------------------------------------- Part 3: codeaut collector
  * The Brouwer-Zimmermann low-weight collector of the reference's codeaut engine, with the
  * handle ABI of cpp/codeaut/capi.h:51-72 that its Python (python/qubitserf/codeaut/

@@ -148,6 +148,7 @@ SIGNATURES = [
     ("qsfb_tc_selftest", _i, [_i, _i, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("qsfb_device_name", _s, []),
     ("qsfb_device_sms", _i, []),
+    ("qsfb_alloc_counters", _i, [ctypes.POINTER(ctypes.c_longlong)]),
     ("codeaut_bz_collect", ctypes.c_void_p, [_u8p, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32]),
@@ -489,6 +490,14 @@ def microbench(which):
     v = ctypes.c_double()
     _check(lib().qsfb_microbench(int(which), ctypes.byref(v)), "qsfb_microbench")
     return v.value
+
+
+def alloc_counters():
+    """Driver-level allocations so far: (device allocations, their seconds, pinned staging
+    allocations, their seconds)."""
+    v = (ctypes.c_longlong * 4)()
+    _check(lib().qsfb_alloc_counters(v), "qsfb_alloc_counters")
+    return v[0], v[1] * 1e-9, v[2], v[3] * 1e-9
 
 
 def tc_selftest(ksteps, A, B, packed=False):

@@ -985,4 +985,16 @@ int qsfb_device_sms(void) {
     return d ? d->num_sms : 0;
 }
 
+int qsfb_alloc_counters(long long* out) {
+    if (!out) return kErrNull;
+    int rc = kOk;
+    Device* d = device_or(&rc);
+    if (!d) return rc;
+    out[0] = d->n_device_malloc;
+    out[1] = d->ns_device_malloc;
+    out[2] = d->n_pinned_alloc;
+    out[3] = d->ns_pinned_alloc;
+    return kOk;
+}
+
 }  // extern "C"

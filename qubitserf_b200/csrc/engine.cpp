@@ -73,6 +73,17 @@ int Device::init() {
     if (prop.major != 10 || prop.minor != 0) return kErrDevice;
     num_sms = prop.multiProcessorCount;
     name = prop.name;
+    // Pool-backed cache misses (QSFB_PLAIN_MALLOC=1: cudaMalloc instead).
+    if (!std::getenv("QSFB_PLAIN_MALLOC")) {
+        unsigned long long keep = ~0ull;
+        if (cudaDeviceGetDefaultMemPool(&pool_, id) != cudaSuccess ||
+            cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep) !=
+                cudaSuccess ||
+            cudaStreamCreateWithFlags(&alloc_stream_, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            pool_ = nullptr;
+        }
+    }
     const int ld = kBinomMaxK + 1;
     h_binom_.assign((size_t)(kBinomMaxN + 1) * ld, 0ull);
     for (int n = 0; n <= kBinomMaxN; ++n) {
@@ -114,21 +125,35 @@ void* Device::alloc(size_t bytes) {
     }
     cudaSetDevice(id);
     void* p = nullptr;
+    auto driver_alloc = [&]() -> bool {
+        if (!pool_) return cudaMalloc(&p, b) == cudaSuccess;
+        if (cudaMallocAsync(&p, b, alloc_stream_) != cudaSuccess) return false;
+        return cudaStreamSynchronize(alloc_stream_) == cudaSuccess;
+    };
     const double tm0 = now_seconds();
-    const cudaError_t me = cudaMalloc(&p, b);
+    const bool got = driver_alloc();
     n_device_malloc.fetch_add(1);
     ns_device_malloc.fetch_add((long long)((now_seconds() - tm0) * 1e9));
-    if (me != cudaSuccess) {
+    if (!got) {
         cudaGetLastError();
-        // Drop the cache and retry once.
+        // Drop the cache (after all work that may still use its blocks) and retry once.
         std::multimap<size_t, void*> drop;
         {
             std::lock_guard<std::mutex> lk(mu_);
             drop.swap(free_);
             cached_ = 0;
         }
-        for (auto& kv : drop) cudaFree(kv.second);
-        if (cudaMalloc(&p, b) != cudaSuccess) {
+        cudaDeviceSynchronize();
+        for (auto& kv : drop) {
+            if (pool_) cudaFreeAsync(kv.second, alloc_stream_);
+            else cudaFree(kv.second);
+        }
+        if (pool_) {
+            cudaStreamSynchronize(alloc_stream_);
+            cudaMemPoolTrimTo(pool_, 0);
+        }
+        cudaGetLastError();
+        if (!driver_alloc()) {
             cudaGetLastError();
             return nullptr;
         }
@@ -136,6 +161,16 @@ void* Device::alloc(size_t bytes) {
     std::lock_guard<std::mutex> lk(mu_);
     in_use_ += b;
     return p;
+}
+
+void Device::reserve(size_t bytes) {
+    if (!pool_ || bytes == 0) return;
+    cudaSetDevice(id);
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, bytes, alloc_stream_) == cudaSuccess)
+        cudaFreeAsync(p, alloc_stream_);   // the pool keeps the memory (release threshold)
+    cudaStreamSynchronize(alloc_stream_);
+    cudaGetLastError();
 }
 
 void Device::release(void* p, size_t bytes) {

@@ -53,6 +53,10 @@ public:
 
     void* alloc(size_t bytes);               // caching; nullptr on failure
     void release(void* p, size_t bytes);
+    // Grow the device memory pool behind alloc()'s cache misses by `bytes` of mapped memory
+    // that it keeps (a server calls it at start, so that a first allocation of a new size
+    // during serving does not map memory while requests wait).
+    void reserve(size_t bytes);
     size_t bytes_in_use() const { return in_use_; }
     size_t bytes_cached() const { return cached_; }
     // allocation calls that reach the driver (cache misses, pinned staging growth) and
@@ -71,6 +75,11 @@ private:
     int init();
     std::mutex mu_;
     std::multimap<size_t, void*> free_;
+    // Cache misses are served by the stream-ordered allocator from the device's default
+    // memory pool (release threshold: keep everything), on a stream of their own that is
+    // synchronised before the pointer is handed out, so any stream may use it at once.
+    cudaMemPool_t pool_ = nullptr;
+    cudaStream_t alloc_stream_ = nullptr;
     size_t in_use_ = 0, cached_ = 0;
     std::vector<Session*> idle_;
     std::vector<unsigned long long> h_binom_;

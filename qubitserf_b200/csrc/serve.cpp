@@ -310,6 +310,14 @@ int qsfb_server_start(int intake_threads, long long mem_budget_bytes, int max_ac
     auto* S = new QsfbServer();
     S->dev = dev;
     S->budget = mem_budget_bytes > 0 ? (size_t)mem_budget_bytes : (size_t)64 << 30;
+    // Mapped memory for the device allocator's first allocations of each size, so that a
+    // heavy request's first large list does not map memory on the engine thread (measured:
+    // one first 1 GiB-class allocation held a round, and the intake behind it, ~50 ms).
+    // QSFB_SERVER_RESERVE_MB (default 8192, at most the budget; 0 = none).
+    const char* re = std::getenv("QSFB_SERVER_RESERVE_MB");
+    const size_t reserve = std::min(S->budget, (size_t)(re ? std::max(0, std::atoi(re)) : 8192)
+                                                   << 20);
+    dev->reserve(reserve);
     S->max_active = max_active > 0 ? max_active : 4096;
     S->t0 = now_seconds();
     // default: all cores but two (the engine thread and the caller's submitting thread
