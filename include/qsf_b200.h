@@ -223,7 +223,10 @@ void qsfb_batch_free(QsfbBatchHandle* handle);
  * lists their levels will build) stays within mem_budget_bytes (0 = 64 GiB), runs one
  * fused round over all admitted queries' next levels, and completes each query as soon as
  * it is proven.  Answers equal qsfb_batch's for the same query, alone or in any mix.
- * intake_threads = 0: all host cores but two.  For steady latencies start the process with
+ * intake_threads = 0: all host cores but two.  start() grows the device memory pool behind
+ * the allocator by QSFB_SERVER_RESERVE_MB (default 8192, at most the budget), so that a
+ * request's first list of a new size is carved from mapped memory instead of mapping it
+ * while the round waits.  For steady latencies start the process with
  * CUDA_MODULE_LOADING=EAGER (with lazy loading a kernel variant loads at its first launch,
  * which a request then waits for) and warm the server up with a few queries. */
 typedef struct QsfbServer QsfbServer;

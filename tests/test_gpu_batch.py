@@ -104,21 +104,33 @@ def test_full_1024_batch_matches_reference(native):
 
 
 def test_one_shot_pipeline_equals_single_batch(native):
-    """qsfb_batch cuts batches of 256+ queries into pipelined chunks; the answers equal one
-    prepared batch executed as a whole."""
+    """qsfb_batch cuts batches of 256+ queries into chunks whose jobs join the running job
+    groups at round boundaries (each chunk at whatever round its preparation ends); with
+    any chunk and group count the answers, levels and codeword counts equal one prepared
+    batch executed as a whole."""
+    import os
     from qubitserf_b200 import workloads as W
     items = native.batch_items(W.batch_1024(300))
-    ans, st = native.Batch(items).run()                 # pipelined (2 chunks)
     b = native.Batch(items)
     h = b.prepare()
     ref, st2 = b.execute(h)                             # one batch
     b.free(h)
-    assert st.certificates == st2.certificates == len(items)
-    for a, r in zip(ans, ref):
-        assert (a.distance, a.lower_bound, a.proven, a.levels, a.z_weight, a.x_weight) == \
-            (r.distance, r.lower_bound, r.proven, r.levels, r.z_weight, r.x_weight)
-        assert a.witness_ok == 1
-    assert st.codewords == st2.codewords
+    want = [(r.distance, r.lower_bound, r.proven, r.levels, r.z_weight, r.x_weight)
+            for r in ref]
+    try:
+        for chunks, groups in [("4", "3"), ("2", "1"), ("8", "4"), ("3", "2")]:
+            os.environ["QSFB_BATCH_CHUNKS"] = chunks
+            os.environ["QSFB_OVERLAP_GROUPS"] = groups
+            ans, st = native.Batch(items).run()
+            got = [(a.distance, a.lower_bound, a.proven, a.levels, a.z_weight, a.x_weight)
+                   for a in ans]
+            assert got == want, (chunks, groups)
+            assert all(a.witness_ok == 1 for a in ans), (chunks, groups)
+            assert st.certificates == st2.certificates == len(items)
+            assert st.codewords == st2.codewords, (chunks, groups)
+    finally:
+        os.environ.pop("QSFB_BATCH_CHUNKS", None)
+        os.environ.pop("QSFB_OVERLAP_GROUPS", None)
 
 
 def test_job_groups_do_not_change_answers(native):
