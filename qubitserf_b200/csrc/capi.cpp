@@ -336,23 +336,31 @@ int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_m
 }
 
 // Witness rebuild, host verification and the per-query answers of an executed handle.
-void answers_of(QsfbBatchHandle* H, QsfbAnswer* out) {
-    auto& jobs = H->jobs;
-    // Results (witness rebuild + host verification) are independent per job: spread them
-    // over the host cores.
-    std::vector<BzResult> res(jobs.size());
-    {
-        std::atomic<size_t> next{0};
-        auto worker = [&]() {
-            for (size_t k; (k = next.fetch_add(1)) < jobs.size();) res[k] = jobs[k]->result();
-        };
-        const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
-                                                  (int)jobs.size() / 8 + 1));
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nth; ++t) pool.emplace_back(worker);
-        worker();
-        for (auto& th : pool) th.join();
+// Results (witness rebuild + host verification) of every job of the handles, independent
+// per job: one pool over the host cores for all of them.
+std::vector<std::vector<BzResult>> results_of(const std::vector<QsfbBatchHandle*>& Hs) {
+    std::vector<std::vector<BzResult>> res(Hs.size());
+    std::vector<std::pair<size_t, size_t>> work;
+    for (size_t h = 0; h < Hs.size(); ++h) {
+        res[h].resize(Hs[h]->jobs.size());
+        for (size_t k = 0; k < Hs[h]->jobs.size(); ++k) work.emplace_back(h, k);
     }
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for (size_t w; (w = next.fetch_add(1)) < work.size();)
+            res[work[w].first][work[w].second] = Hs[work[w].first]->jobs[work[w].second]->result();
+    };
+    const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
+                                              (int)work.size() / 8 + 1));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return res;
+}
+
+// The per-query answers of an executed handle from its jobs' results.
+void answers_of(QsfbBatchHandle* H, const std::vector<BzResult>& res, QsfbAnswer* out) {
     for (size_t i = 0; i < H->map.size(); ++i) {
         QsfbAnswer& a = out[i];
         std::memset(&a, 0, sizeof(a));
@@ -409,7 +417,7 @@ int batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats, in
     double span = 0.0;
     int rc = execute_groups(H, &rs, &rounds, &span, max_groups);
     if (rc != kOk) return rc;
-    answers_of(H, out);
+    answers_of(H, results_of({H})[0], out);
     if (stats) {
         fill_exec_stats(rs, rounds, span, stats);
         stats->seconds = now_seconds() - t0;
@@ -833,8 +841,15 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
                                     c == 0 ? host_threads : overlap_threads, &H[c]);
         tp1[c] = now_seconds();
     };
+    // the chunks' handles are torn down in parallel (jobs' host state, device lists back to
+    // the allocator's cache, sessions back to the pool)
     auto release = [&]() {
-        for (QsfbBatchHandle*& h : H) { qsfb_batch_free(h); h = nullptr; }
+        std::vector<std::thread> th;
+        for (size_t c = 1; c < H.size(); ++c)
+            if (H[c]) th.emplace_back(qsfb_batch_free, H[c]);
+        qsfb_batch_free(H[0]);
+        for (auto& t : th) t.join();
+        for (QsfbBatchHandle*& h : H) h = nullptr;
     };
     if (nchunks == 1) {
         prepare(0);
@@ -864,8 +879,11 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     helper.join();
     for (int c = 0; c < nchunks && rc == kOk; ++c)
         if (prc[c] != kOk) rc = prc[c];
-    if (rc == kOk && out)
-        for (int c = 0; c < nchunks; ++c) answers_of(H[c], out + cut[c]);
+    if (rc == kOk && out) {
+        const std::vector<std::vector<BzResult>> res = results_of(H);
+        for (int c = 0; c < nchunks; ++c) answers_of(H[c], res[c], out + cut[c]);
+    }
+    const double ta1 = now_seconds();
     if (tdev)
         std::fprintf(stderr, "qsfb_batch: %lld device allocations (%.2f ms), %lld pinned "
                      "staging allocations (%.2f ms)\n", tdev->n_device_malloc - alloc0[0],
@@ -895,6 +913,9 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
         stats->seconds = now_seconds() - t0;
     }
     release();
+    if (trace)
+        std::fprintf(stderr, "qsfb_batch: answers %.2f ms, release %.2f ms, call %.2f ms\n",
+                     1e3 * (ta1 - te1), 1e3 * (now_seconds() - ta1), 1e3 * (now_seconds() - t0));
     return rc;
 }
 
