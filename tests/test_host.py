@@ -188,6 +188,9 @@ def test_dispatch_rules_without_device(native, golden):
             assert rc == 4
         with pytest.raises(RuntimeError):
             native.classical_distance_raw(H, "bz", "auto", 0, False)
+        counters = (ctypes.c_longlong * 4)()
+        assert lib.qsfb_alloc_counters(counters) == 4
+    assert lib.qsfb_alloc_counters(None) == 1
     assert lib.distfind_backend_available(b"cpu") == 0
     assert lib.distfind_backend_available(b"metal") == 0
 
