@@ -304,12 +304,15 @@ def main():
             launches += st.kernel_launches
             rounds = st.rounds
     # per-kernel statistics (the rooflines) from one more, untimed execution as a single job
-    # group: with several groups their kernels overlap and summed event times count twice
+    # group with each round's pair launches on one stream: with several groups, or pair
+    # launches forked over streams, kernels overlap and their event times include others'
     os.environ["QSFB_EXEC_GROUPS"] = "1"
+    os.environ["QSFB_SERIAL_PAIRS"] = "1"
     try:
         _, st1 = batch.execute(handle)
     finally:
         os.environ.pop("QSFB_EXEC_GROUPS", None)
+        os.environ.pop("QSFB_SERIAL_PAIRS", None)
     k = args.steps   # every step certifies the same batch: per-step figures times the steps
     pair_ms, tc_ms, tc_cw = st1.pair_ms * k, st1.tc_ms * k, st1.tc_codewords * k
     cw, popc_issued, zero_cw = st1.codewords * k, st1.popc_issued * k, st1.zero_codewords * k

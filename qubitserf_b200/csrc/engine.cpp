@@ -913,7 +913,10 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     cudaEventCreate(&evm);
     cudaEventRecord(evm, st);
     // fork: the pair launches (independent levels; they share only the atomic witness keys)
-    // go round-robin over the auxiliary streams, the tensor-core sweep first
+    // go round-robin over the auxiliary streams, the tensor-core sweep first.
+    // QSFB_SERIAL_PAIRS (read per call): all on one stream, so that each kernel's events
+    // time it alone (benchmarks' per-kernel statistics).
+    const bool serial_pairs = std::getenv("QSFB_SERIAL_PAIRS") != nullptr;
     cudaEventRecord(s->ev_fork, st);
     for (int k = 0; k < Session::kAux; ++k) cudaStreamWaitEvent(s->aux[k], s->ev_fork, 0);
     unsigned long long all_jobs = 0;
@@ -924,7 +927,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         const size_t gi = (groups.back().tc ? (gi0 == 0 ? groups.size() - 1 : gi0 - 1) : gi0);
         const Group& Gp = groups[gi];
         const LevelDesc* gd = (const LevelDesc*)(d + off_lvl) + Gp.first;
-        cudaStream_t gs = s->aux[next_aux];
+        cudaStream_t gs = s->aux[serial_pairs ? 0 : next_aux];
         next_aux = (next_aux + 1) % Session::kAux;
         if (Gp.tc) cudaEventRecord(s->ev_tc0, gs);
         const cudaError_t e =
