@@ -580,8 +580,7 @@ int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& job
     return kOk;
 }
 
-int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
-               int host_threads, RunStats* stats) {
+int setup_jobs_host(std::vector<BzJob*>& jobs, int host_threads, RunStats* stats) {
     const double th0 = now_seconds();
     int nth = host_threads > 0 ? host_threads : (int)std::thread::hardware_concurrency();
     nth = std::max(1, std::min<int>(nth, (int)jobs.size()));
@@ -604,12 +603,23 @@ int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
     }
     if (err.load() != kOk) return err.load();
     if (stats) stats->host_setup_s += now_seconds() - th0;
+    return kOk;
+}
+
+int setup_jobs_device(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
+                      RunStats* stats) {
     int rc = device_seeds(dev, s, arena, jobs, stats);
     if (rc != kOk) return rc;
     std::vector<SideDev*> sides;
     for (BzJob* j : jobs)
         for (SideDev* sd : j->device_sides()) sides.push_back(sd);
     return upload_sides(dev, s, arena, sides);
+}
+
+int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
+               int host_threads, RunStats* stats) {
+    const int rc = setup_jobs_host(jobs, host_threads, stats);
+    return rc != kOk ? rc : setup_jobs_device(dev, s, arena, jobs, stats);
 }
 
 

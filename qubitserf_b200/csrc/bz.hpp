@@ -153,6 +153,11 @@ int run_jobs(Device* dev, std::vector<BzJob*>& jobs, int host_threads, RunStats*
 // rounds repeatedly: host setup of every job + one upload into `arena`, then the rounds.
 int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
                int host_threads, RunStats* stats);
+// setup_jobs in two phases: the host setup of every job (no device work), then the seed
+// eliminations and the upload (a pipeline runs the next batch's host phase meanwhile).
+int setup_jobs_host(std::vector<BzJob*>& jobs, int host_threads, RunStats* stats);
+int setup_jobs_device(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
+                      RunStats* stats);
 // `feed` (optional) is called at the top of every round with idle = false and may append
 // jobs to `jobs` (they start from their first level in that round); when every job is done
 // it is called with idle = true, may block until it has more, and returns whether it

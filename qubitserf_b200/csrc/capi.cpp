@@ -707,7 +707,10 @@ int qsfb_last_counts(int* side, int* w, int* g, unsigned long long* count, int c
     return n;
 }
 
-int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
+namespace {
+
+// Host phase of qsfb_batch_prepare: the handle, its jobs and their host setup.
+int batch_prepare_host(const QsfbQuery* queries, int nq, int host_threads,
                        QsfbBatchHandle** handle) {
     if ((!queries && nq > 0) || !handle) return kErrNull;
     *handle = nullptr;
@@ -775,11 +778,33 @@ int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
     H->lease.reset(new SessionLease(dev));
     if (!H->lease->s) { delete H; return kErrDevice; }
     H->arena.reset(new Arena(dev));
-    rc = setup_jobs(dev, H->lease->s, H->arena.get(), H->ptrs, host_threads, &H->setup);
+    rc = setup_jobs_host(H->ptrs, host_threads, &H->setup);
     if (rc != kOk) { delete H; return rc; }
     H->prepare_s = now_seconds() - tp0;
     *handle = H;
     return kOk;
+}
+
+// Device phase: seed eliminations and upload.  On failure the handle is freed and nulled.
+int batch_prepare_device(QsfbBatchHandle*& H) {
+    const double t0 = now_seconds();
+    const int rc = setup_jobs_device(H->dev, H->lease->s, H->arena.get(), H->ptrs, &H->setup);
+    if (rc != kOk) {
+        delete H;
+        H = nullptr;
+        return rc;
+    }
+    H->prepare_s += now_seconds() - t0;
+    return kOk;
+}
+
+}  // namespace
+
+int qsfb_batch_prepare(const QsfbQuery* queries, int nq, int host_threads,
+                       QsfbBatchHandle** handle) {
+    const int rc = batch_prepare_host(queries, nq, host_threads, handle);
+    if (rc != kOk) return rc;
+    return batch_prepare_device(*handle);
 }
 
 int qsfb_batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats) {
@@ -791,8 +816,9 @@ void qsfb_batch_free(QsfbBatchHandle* H) { delete H; }
 
 // One-shot batch.  A large batch is cut into chunks: the first (small, so the device
 // starts early) is prepared on all host cores and its rounds start; a helper thread
-// prepares the others in order (host reduction, seed eliminations and upload on its own
-// stream) and publishes each to the running job groups, which take their share of its jobs
+// prepares the others in order (host reduction; seed eliminations and upload on its own
+// stream, beside the next chunk's host reduction) and publishes each to the running job
+// groups, which take their share of its jobs
 // at their next round boundary: the chunks' rounds merge into one execution with one tail.
 // Codes are independent and a job's answer depends only on its own levels, so the answers
 // are those of one batch.  1024-code batch, end to end: one piece 17.9-18.4k certs/s, two
@@ -863,10 +889,23 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     if (prc[0] != kOk) return prc[0];
     ChunkFeed F;
     F.total = (size_t)(nchunks - 1);
+    // The helper prepares chunks 1.. in order, in two phases: while chunk c's seed
+    // eliminations and upload run (the host mostly waiting for the device), chunk c + 1's
+    // host reduction runs beside them.
+    auto prepare_host = [&](int c) {
+        tp0[c] = now_seconds();
+        prc[c] = batch_prepare_host(queries + cut[c], cut[c + 1] - cut[c], overlap_threads,
+                                    &H[c]);
+    };
     std::thread helper([&]() {
+        prepare_host(1);
         for (int c = 1; c < nchunks; ++c) {
-            prepare(c);
+            std::thread next;
+            if (c + 1 < nchunks) next = std::thread(prepare_host, c + 1);
+            if (prc[c] == kOk) prc[c] = batch_prepare_device(H[c]);
+            tp1[c] = now_seconds();
             F.publish(prc[c] == kOk ? H[c] : nullptr);
+            if (next.joinable()) next.join();
         }
     });
     RunStats rs;
