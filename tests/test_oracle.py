@@ -111,6 +111,31 @@ def test_oracle_random_batch_codes_match_reference(orc, ref):
             assert orc.css(*cs.mats).distance == ref.css(*cs.mats).distance, i
 
 
+def test_reference_cuda_build_equals_cpu_build_without_device(ref, golden):
+    """oracle/_ref/libqubitserf_cuda.so (the reference's sources with its CUDA backend, the
+    plain per-code GPU comparator) is a working build of the same library: without a device
+    its CUDA backend reports unavailable, backend "gpu" runs the reference CPU backend, and
+    every field equals the CPU build's."""
+    from oracle.refbind import REF_CUDA_LIB, RefCuda
+    if ref is None or not REF_CUDA_LIB.exists():
+        pytest.skip("reference libraries not built here")
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the GPU tests compare the CUDA path")
+    rc = RefCuda()
+    assert not rc.available()
+    for name in ["hamming4", "steane", "toric3", "surface3", "batch_512"]:
+        res = golden.results[name]
+        mats = golden.mats(name)
+        if res["kind"] == "classical":
+            a, b = rc.classical(mats[0]), ref.classical(mats[0])
+        else:
+            a, b = rc.css(*mats), ref.css(*mats)
+        assert (a.distance, a.lower_bound, a.proven, a.levels) == \
+            (b.distance, b.lower_bound, b.proven, b.levels), name
+        assert a.distance == res["distance"], name
+
+
 def test_oracle_problem_ranks_match_reference(orc, ref, golden):
     if ref is None:
         pytest.skip("reference library not built here")
