@@ -493,8 +493,7 @@ cudaError_t launch_seed_trials(int W, const SeedDesc* d_descs, int ndesc, int to
 
 // Run every pending seed trial of every job in one launch per row width, then fold the
 // per-side keys into the bounds.
-int device_seeds(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
-                 RunStats* stats) {
+int device_seeds(Session* s, Arena* arena, std::vector<BzJob*>& jobs, RunStats* stats) {
     std::vector<BzSide*> pend[3];   // by row words W = 1, 2
     for (BzJob* j : jobs)
         for (int i = 0; i < (j->pair ? 2 : 1); ++i)
@@ -608,7 +607,7 @@ int setup_jobs_host(std::vector<BzJob*>& jobs, int host_threads, RunStats* stats
 
 int setup_jobs_device(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
                       RunStats* stats) {
-    int rc = device_seeds(dev, s, arena, jobs, stats);
+    int rc = device_seeds(s, arena, jobs, stats);
     if (rc != kOk) return rc;
     std::vector<SideDev*> sides;
     for (BzJob* j : jobs)
