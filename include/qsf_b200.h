@@ -121,7 +121,9 @@ typedef struct {
  * systematic.  *out_best = min(current_best, lightest logical codeword < current_best);
  * out_counts[g] = evaluated combinations of set g (== C(K,d)); the arg-min is returned as
  * (*out_g, *out_rank) with rank in the lexicographic order of cpp/qsf/combinatorics.hpp:52-61
- * (-1 if nothing beat current_best). */
+ * (-1 if nothing beat current_best).  Sizes are checked before any device work: d <= 64,
+ * K <= 4096, num_gamma <= 255 and C(K, d) < 2^62, else 5; a level whose subset lists would
+ * exceed 2^36 entries, else 6. */
 int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const uint64_t* gamma,
                         int kcheck, const uint64_t* check, int current_best, int* out_best,
                         unsigned long long* out_counts, int* out_g, unsigned long long* out_rank);
@@ -260,9 +262,11 @@ int qsfb_server_stop(QsfbServer* server);
  * NULL).  Results equal qsfb_enumerate_plan's.  All scratch sits in one fixed 32 MiB device
  * array inside the library (held on every GPU the library runs on until exit), shared by
  * every call: calls that overlap on the GPU race, so serialise them.  The first call on a
- * device sets the array up; make it before any stream capture.  Limits: K <= 128,
- * num_gamma <= 8, kcheck <= 256, stride <= 16 and the level's subset lists within the
- * array; beyond them it returns 8 without touching the device.  stream: a cudaStream_t
+ * device sets the array up (its address, and a binomial table copied on `stream`); make it
+ * before any stream capture.  The address stays cached while the library is loaded, so
+ * after a cudaDeviceReset the library must be reloaded.  Limits: K <= 128, num_gamma <= 8,
+ * kcheck <= 256, stride <= 16, d <= 64, C(K, d) < 2^62, and the level's subset lists within
+ * the array; beyond them it returns 8 without touching the device.  stream: a cudaStream_t
  * (NULL = default stream); returns after the level has finished on that stream. */
 int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int num_gamma,
                                 const uint64_t* d_gamma, int kcheck, const uint64_t* d_check,

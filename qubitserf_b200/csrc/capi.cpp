@@ -601,7 +601,10 @@ int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const ui
                         unsigned long long* out_rank) {
     if (!gamma || !out_best || (kcheck > 0 && !check)) return kErrNull;
     if (stride != words_for(n) || K < 1 || d < 1 || d > K || num_gamma < 1) return kErrShape;
-    int rc = kOk;
+    // sizes first: a level whose lists cannot exist is rejected before any device work
+    int rc = level_size_rc(K, d);
+    if (rc != kOk) return rc;
+    if (num_gamma > 255) return kErrUnsupported;   // the witness key holds the set in 8 bits
     Device* dev = device_or(&rc);
     if (!dev) return rc;
     // The reference weighs every bit of the `stride` words (cpp/qsf/bits.hpp:29-33), so a

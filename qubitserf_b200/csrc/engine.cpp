@@ -440,6 +440,33 @@ struct Plan {
 
 unsigned long long level_pairs(const Device* dev, int K, int w) { return dev->binom(K, w); }
 
+unsigned long long host_binom(int n, int k) {
+    if (k < 0 || n < 0 || k > n) return 0ull;
+    k = std::min(k, n - k);   // C(n, i) grows with i up to n/2: the running value never shrinks
+    unsigned __int128 r = 1;
+    for (int i = 0; i < k; ++i) {
+        r = r * (unsigned)(n - i) / (unsigned)(i + 1);   // exact: C(n, i) * (n - i) = C(n, i + 1) * (i + 1)
+        if (r >> 64) return kSat;
+    }
+    return (unsigned long long)r;
+}
+
+void level_split(unsigned long long pairs, int w, int* a, int* b) {
+    *a = pairs <= (1ull << 14) ? w : (w + 1) / 2;
+    *b = w - *a;
+}
+
+int level_size_rc(int K, int w) {
+    if (w < 1 || w > K || w > kBinomMaxK || K > kBinomMaxN) return kErrUnsupported;
+    const unsigned long long pairs = host_binom(K, w);
+    if (pairs == kSat || pairs >= (1ull << 62)) return kErrUnsupported;
+    int a, b;
+    level_split(pairs, w, &a, &b);
+    if (host_binom(K, a) > kMaxListEntries || host_binom(K, b) > kMaxListEntries)
+        return kErrMemory;
+    return kOk;
+}
+
 int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelOut>& outs,
                RunStats* stats) {
     Device* dev = s->dev;
@@ -456,12 +483,11 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         const LevelReq& q = reqs[r];
         SideDev* S = q.side;
         const int K = S->K, w = q.w;
-        if (w < 1 || w > K || w > kBinomMaxK) return kErrUnsupported;
+        const int size_rc = level_size_rc(K, w);
+        if (size_rc != kOk) return size_rc;
         const unsigned long long pairs = dev->binom(K, w);
-        if (pairs == kSat || pairs >= (1ull << 62)) return kErrUnsupported;
         int a, b;
-        if (pairs <= (1ull << 14)) { a = w; b = 0; }
-        else { a = (w + 1) / 2; b = w - a; }
+        level_split(pairs, w, &a, &b);
         // tensor-core term range of this level (the same for every set): terms whose
         // rectangles keep at least half of every tile busy; nx grows and ny shrinks with p
         int p1 = -1, p2 = -1;

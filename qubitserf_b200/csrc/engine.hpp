@@ -232,4 +232,21 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
 // Enumeration counts are the per-set C(K,w); used by tests of the job decomposition.
 unsigned long long level_pairs(const Device* dev, int K, int w);
 
+// Subset lists above this many entries are never built: at 4 bytes per probe word plus the
+// 64-byte +-1 row they would exceed any device's memory, and every product of a list
+// count with a per-entry byte size stays far from 2^64 below it.
+constexpr unsigned long long kMaxListEntries = 1ull << 36;
+
+// C(n, k) computed on the host without a table, saturating to ~0ull at 2^64.
+unsigned long long host_binom(int n, int k);
+
+// The prefix/suffix split of a level's w-subsets: a = w (single list) when C(K, w) is
+// small, else a = ceil(w/2), b = w - a.
+void level_split(unsigned long long pairs, int w, int* a, int* b);
+
+// Size guard of one level of a K-row set, without a device: kOk, kErrUnsupported (w or K
+// beyond the binomial table, C(K, w) saturated or >= 2^62) or kErrMemory (a subset list
+// beyond kMaxListEntries).  Every path that sizes buffers from binomials calls it first.
+int level_size_rc(int K, int w);
+
 }  // namespace qsfb

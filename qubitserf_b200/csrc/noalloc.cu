@@ -34,6 +34,7 @@ cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long lo
 cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          unsigned long long jobs, unsigned long long* ctr,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
+void level_split(unsigned long long pairs, int w, int* a, int* b);
 }  // namespace qsfb
 
 namespace {
@@ -138,7 +139,10 @@ unsigned long long host_binom(int n, int k) {
 }
 
 // Set-up once per device (device current): look up the scratch address, fill the table.
-int device_slot(DevSlot** out) {
+// The table goes up on the caller's stream, followed by a wait on that stream only, so the
+// set-up does not synchronise the whole device.  The address is cached for the life of the
+// loaded library: after a cudaDeviceReset the library must be reloaded.
+int device_slot(cudaStream_t st, DevSlot** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
@@ -152,9 +156,10 @@ int device_slot(DevSlot** out) {
             cudaGetLastError();
             return 4;
         }
-        const BinomTable& table = binom_table();
-        if (cudaMemcpy((unsigned char*)p + kOffBinom, table.v, sizeof(table.v),
-                       cudaMemcpyHostToDevice) != cudaSuccess ||
+        const BinomTable& table = binom_table();   // static storage: outlives the async copy
+        if (cudaMemcpyAsync((unsigned char*)p + kOffBinom, table.v, sizeof(table.v),
+                            cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess ||
             cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
             cudaGetLastError();
             return 4;
@@ -181,9 +186,13 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
     cudaStream_t st = (cudaStream_t)stream;
 
     // ---- plan (the rules of the allocating path: prefix/suffix split, probe filter)
+    // Every size below is bounded before it is multiplied: a saturated binomial (C >= 2^64
+    // reads as ~0ull) or a list count beyond the scratch array is rejected first, so no
+    // product or sum can wrap.
     const unsigned long long pairs = host_binom(K, d);
-    const int a = pairs <= (1ull << 14) ? d : (d + 1) / 2;
-    const int b = d - a;
+    if (pairs == ~0ull || pairs >= (1ull << 62)) return kErrScratch;
+    int a, b;
+    level_split(pairs, d, &a, &b);
     const int W32 = 2 * stride;              // a u64 row is 2*stride little-endian u32 words
     const int HP = W32 >= 3 ? 4 : W32;
     const int bound = current_best >= kWeightNone ? 4094 : current_best - 1;
@@ -191,13 +200,16 @@ extern "C" int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int 
     const int filt = choose_filter(HP, 32 * W32, T - 1, false).filt;
     const int SW = (kcheck + 31) / 32;
     const unsigned long long na = host_binom(K, a), nb = host_binom(K, b);
+    constexpr size_t kListRoom = kScratchBytes - kOffLists;
+    const unsigned long long entry_bytes = (unsigned long long)HP * 4 + 1;   // probe words + pivot count
+    if (na > kListRoom / entry_bytes || nb > kListRoom / entry_bytes) return kErrScratch;
     const size_t list_a = (size_t)na * HP * 4, list_b = (size_t)nb * HP * 4;
     auto up = [](size_t x) { return (x + 255) / 256 * 256; };
-    const size_t per_set = up(list_a) + up(na) + up(list_b) + up(nb);
-    if (kOffLists + per_set * num_gamma > kScratchBytes) return kErrScratch;
+    const size_t per_set = up(list_a) + up(na) + up(list_b) + up(nb);   // < 4 x (32 MiB + 256)
+    if (per_set > kListRoom / (size_t)num_gamma) return kErrScratch;
 
     DevSlot* slot = nullptr;
-    if (device_slot(&slot) != 0) return 4;
+    if (device_slot(st, &slot) != 0) return 4;
     unsigned char* base = slot->ptr;
 
     // ---- descriptors (host, fixed arrays) -> one copy into the scratch descriptor region

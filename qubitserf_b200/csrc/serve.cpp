@@ -67,8 +67,12 @@ size_t list_footprint(Device* dev, const BzSide& S) {
         std::vector<std::pair<int, int>> seen;
         for (int w = 1; w <= wmax; ++w) {
             if ((w + 1) - (S.K - S.ranks[g]) <= 0) continue;   // set inactive at this level
+            // a level the engine cannot size: charge a footprint no budget admits beside
+            // others (still far from overflowing a sum over requests)
+            if (level_size_rc(S.K, w) != kOk) return (size_t)1 << 50;
             const unsigned long long pairs = dev->binom(S.K, w);
-            const int a = pairs <= (1ull << 14) ? w : (w + 1) / 2, b = w - a;
+            int a, b;
+            level_split(pairs, w, &a, &b);
             for (auto sz : {std::make_pair(a, 0), std::make_pair(b, 1)}) {
                 if (std::find(seen.begin(), seen.end(), sz) != seen.end()) continue;
                 seen.push_back(sz);

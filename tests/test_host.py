@@ -195,6 +195,37 @@ def test_dispatch_rules_without_device(native, golden):
     assert lib.distfind_backend_available(b"metal") == 0
 
 
+@pytest.mark.parametrize("K,stride,d", [
+    (128, 2, 32),    # C(128, 16) lists: binomials saturate at 2^64
+    (128, 2, 40),
+    (128, 2, 64),
+    (100, 2, 50),
+    (128, 2, 9),     # lists fit 64-bit sizes but not the 32 MiB array
+])
+def test_noalloc_size_guard_rejects_before_device(native, K, stride, d):
+    """The allocation-free level rejects every level its scratch array cannot hold with rc 8
+    before any device call, including levels whose binomials saturate (C(K, a) >= 2^64):
+    the pointers passed here are placeholders that must never be dereferenced."""
+    lib = native.lib()
+    fake = ctypes.c_void_p(256)
+    rc = lib.qsfb_enumerate_plan_noalloc(64 * stride, stride, K, d, 1, fake, 0, None,
+                                         1 << 30, fake, None, None, None, None)
+    assert rc == 8
+
+
+def test_plan_size_guard_rejects_before_device(native):
+    """The allocating raw-plan level checks its sizes before it looks for a device: w beyond
+    the 64 columns of the binomial table and C(K, w) >= 2^62 give rc 5, subset lists beyond
+    2^36 entries rc 6 (C(64, 60) is small, but its prefix list C(64, 30) is not)."""
+    rng = np.random.default_rng(3)
+    for K, d, want in [(100, 65, 5), (128, 40, 5), (4097, 2, 5), (64, 60, 6)]:
+        stride = 2
+        gamma = rng.integers(0, 2**63, (1, K, stride), dtype=np.uint64)
+        check = np.zeros((0, stride), np.uint64)
+        with pytest.raises(RuntimeError, match=f"rc={want}:"):
+            native.enumerate_plan(64 * stride, K, d, gamma, check, 1 << 30)
+
+
 def test_api_argument_validation():
     from qubitserf_b200 import api
     Hx = np.ones((1, 4), np.uint8)

@@ -28,18 +28,22 @@ def _device_buffers(torch, gamma, check, ng):
     return g, c, best, counts, og, orank
 
 
-def _noalloc(native, torch, n, K, d, gamma, check, cur):
+def _noalloc(native, torch, n, K, d, gamma, check, cur, optional=True):
+    """One call; optional=False passes NULL for the per-set counts and the arg-min."""
     stride = (n + 63) // 64
     ng = gamma.size // (K * stride)
     kcheck = check.size // stride
     g, c, best, counts, og, orank = _device_buffers(torch, gamma, check, ng)
     stream = torch.cuda.current_stream().cuda_stream
+    opt = (counts.data_ptr(), og.data_ptr(), orank.data_ptr()) if optional else (None,) * 3
     rc = native.lib().qsfb_enumerate_plan_noalloc(
         n, stride, K, d, ng, g.data_ptr(), kcheck, c.data_ptr(), cur, best.data_ptr(),
-        counts.data_ptr(), og.data_ptr(), orank.data_ptr(), stream)
+        *opt, stream)
     torch.cuda.synchronize()
     if rc != 0:
         return rc, None
+    if not optional:
+        return 0, int(best.item())
     rank = int(orank.cpu().numpy().view(np.uint64)[0])
     return 0, (int(best.item()), [int(x) for x in counts.cpu().numpy().view(np.uint64)],
                int(og.item()), rank)
@@ -64,6 +68,8 @@ def test_noalloc_matches_allocating_entry_point(native, K, stride, d, ng, kcheck
         rc, got = _noalloc(native, torch, n, K, d, gamma, check, cur)
         assert rc == 0
         assert got == want, (got, want)
+    rc, got = _noalloc(native, torch, n, K, d, gamma, check, cur, optional=False)
+    assert (rc, got) == (0, want[0])
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(native):
@@ -76,3 +82,6 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(native):
     gamma = rng.integers(0, 2**63, (1, 128, 2), dtype=np.uint64)   # lists beyond 32 MiB
     rc, _ = _noalloc(native, torch, 128, 128, 9, gamma, check, WEIGHT_NONE)
     assert rc == 8
+    for d in (40, 64):   # C(128, d/2) saturates the 64-bit binomials: still rejected
+        rc, _ = _noalloc(native, torch, 128, 128, d, gamma, check, WEIGHT_NONE)
+        assert rc == 8
