@@ -10,7 +10,7 @@
  * there is no CPU fallback.
  *
  * Return codes: 0 ok; 1 null pointer; 2 not a [z|x] matrix / bad operator length;
- * 3 method "cc" on a non-CSS code (the reference's own codes, capi.cpp:152-404);
+ * 3 method "cc" on a non-CSS code (the reference's own codes, cpp/distfind/capi.cpp:29-288);
  * 4 no usable sm_100 device or a CUDA error; 5 method/backend/size this engine does not
  * run (method "cc" where the reference runs its connected-cluster solver, backend "cpu",
  * n > 1024 after pivot removal); 6 device memory exhausted.  Codes 4-6 surface in the
@@ -129,7 +129,7 @@ int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const ui
                         unsigned long long* out_counts, int* out_g, unsigned long long* out_rank);
 
 /* Host reduction only (no device): the BZ subproblem and its information sets exactly as
- * the reference's bz_distance sees them (cpp/distfind/bz.cpp:141-159).  kind: 0 classical(H=A),
+ * the reference's bz_distance sees them (cpp/distfind/bz.cpp:95-115).  kind: 0 classical(H=A),
  * 1 css Z (Hx=A,Hz=B), 2 css X, 3 subsystem Z (Gx=A,Gz=B), 4 subsystem X, 5 non-CSS
  * stabilizer S=A after the (a|b)->(a|b|a^b) isometry.  meta = {n, K, num_gamma, kcheck, even,
  * count_all, seed_upper, stride}; gamma (num_gamma*K*stride words) and check
@@ -137,6 +137,21 @@ int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const ui
 int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
                          int bc, int* meta, int* ranks, int max_gamma, uint64_t* gamma,
                          long long max_words, uint64_t* check, long long max_check);
+
+/* qsfb_prepare_problem with the information sets built where the engine builds them (no
+ * reference counterpart; it exposes the device construction that replaces the reference's
+ * host eliminations, cpp/distfind/css.cpp:177-203, 336-366 and cpp/qsf/gf2.cpp:42-58).
+ * on_device = 1: the GPU kernel (one warp per subproblem, K and n <= 128; larger ones and
+ * more than 8 sets are built on the host); 0: the host construction.  meta holds 11 ints:
+ * qsfb_prepare_problem's 8, then W32 = ceil(n/32), SWP = max(1, ceil(kcheck/32)) and 1 when
+ * the device built the sets.  red (num_gamma*K*W32 u32, when not NULL): each set's rows over
+ * its non-pivot columns in ascending order, zero padded; syn (num_gamma*K*SWP u32): bit c of
+ * row r = parity(check_c & row r) -- the two tables the pair sweeps read.
+ * Returns 0, 1 (null), 2 (shape), 4 (device), 7 (buffer small). */
+int qsfb_prepare_sides(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
+                       int bc, int on_device, int* meta, int* ranks, int max_gamma,
+                       uint64_t* gamma, long long max_words, uint64_t* check, long long max_check,
+                       uint32_t* red, long long max_red, uint32_t* syn, long long max_syn);
 
 /* Report / witness / per-level counts of the last distance call on this thread. */
 int qsfb_last_report(QsfbReport* out);
@@ -192,6 +207,8 @@ typedef struct {
     double host_apply_seconds;   /* host schedule updates after the rounds */
     unsigned long long tc_codewords;    /* codewords swept by the tensor-core kernel */
     double tc_ms;                /* tensor-core sweep launches alone (CUDA events) */
+    double device_sets_seconds;  /* information sets + packed rows on the device (copies,
+                                    kernels, read-back, host partition step) */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free.  Batches of 256 queries or more are pipelined in

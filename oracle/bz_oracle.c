@@ -275,7 +275,7 @@ static problem coset_problem(const mat* G, const u64* v) {
     p.seed_upper = v_weight(v, words_for(n));
     return p;
 }
-/* cpp/distfind/stab.cpp:107-253 */
+/* cpp/distfind/stab.cpp:13-178 */
 static mat sw_swap(const mat* m) {
     const int q = m->cols / 2;
     mat o = m_new(m->rows, m->cols);
@@ -375,7 +375,7 @@ static problem isometry(const problem* sp) {
 }
 
 /* ------------------------------------------------------------------ information sets
- * cpp/distfind/css.cpp:258-447 */
+ * cpp/distfind/css.cpp:177-366 */
 typedef struct { mat g; int rank; } gset;
 typedef struct { gset* s; int n, cap; } gseq;
 
@@ -425,7 +425,7 @@ static gseq greedy(const mat* gen) {
     return q;
 }
 
-/* matroid partition by augmenting DFS, cpp/distfind/css.cpp:294-409 */
+/* matroid partition by augmenting DFS, cpp/distfind/css.cpp:274-328 */
 typedef struct { int* v; int n, cap; } ivec;
 static void iv_push(ivec* a, int x) {
     if (a->n == a->cap) { a->cap = a->cap ? 2 * a->cap : 8; a->v = (int*)realloc(a->v, sizeof(int) * (size_t)a->cap); }
@@ -696,7 +696,7 @@ int orc_enumerate_fast(int n, int stride, int K, int d, int ng, const uint64_t* 
 }
 
 /* ------------------------------------------------------------------ BZ schedule
- * cpp/distfind/bz.cpp:118-403 */
+ * cpp/distfind/bz.cpp:72-370 */
 typedef struct {
     int has, K, ng, stride, kcheck, even, maxw;
     int* ranks;
@@ -805,7 +805,7 @@ static void record_level(recorder* R, int side_idx, int w, int active, int K) {
     R->n++;
 }
 
-/* one level of a side (bz.cpp:303-317) */
+/* one level of a side (cpp/distfind/bz.cpp:257-271) */
 static void side_step(side* S, int w, recorder* R, int side_idx) {
     const int active = active_at(S, w);
     record_level(R, side_idx, w, active, S->K);
@@ -836,7 +836,7 @@ static void bz_single(const problem* p, const orc_options* opt, orc_result* r) {
     side_free(&S);
 }
 
-/* bz_min_interleaved, cpp/distfind/bz.cpp:342-403 (cap_to_min) */
+/* bz_min_interleaved, cpp/distfind/bz.cpp:296-357 (cap_to_min) */
 static void bz_min(const problem* pz, const problem* px, const orc_options* opt,
                    orc_result* r) {
     memset(r, 0, sizeof(*r));
@@ -1195,7 +1195,7 @@ int orc_operator_weight(const uint8_t* Gx, int gxr, int gxc, const uint8_t* Gz, 
     return 0;
 }
 
-/* symplectic_distance_driver, cpp/distfind/capi.cpp:285-338 (bz only) */
+/* symplectic_distance_driver, cpp/distfind/capi.cpp:168-223 (bz only) */
 int orc_stabilizer_distance(const uint8_t* S, int rows, int cols, int subsystem, char which,
                             const orc_options* opt, orc_result* out) {
     if (cols % 2) return 2;
@@ -1212,7 +1212,7 @@ int orc_stabilizer_distance(const uint8_t* S, int rows, int cols, int subsystem,
     mat Sn = subsystem ? sympl_center(&G) : m_copy(&G);
     problem sp = sympl_problem(&Sn, &G);
     if (opt && opt->mitm) {
-        /* mitm enumerates symplectic parts directly (capi.cpp:333-335) */
+        /* mitm enumerates symplectic parts directly (cpp/distfind/capi.cpp:217-218) */
         mitm_single(&sp, out);
         p_free(&sp);
         m_free(&Sn);
@@ -1245,7 +1245,7 @@ int orc_pauli_operator_weight(const uint8_t* Gm, int rows, int cols, const uint8
         p.qubits = cols / 2;
         p.seed_upper = sw_weight(v, p.qubits);
         if (opt && opt->mitm) {
-            mitm_single(&p, out);   /* capi.cpp:275-282 */
+            mitm_single(&p, out);   /* cpp/distfind/capi.cpp:272-282 */
         } else {
             problem e = isometry(&p);
             bz_single(&e, opt, out);

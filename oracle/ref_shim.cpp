@@ -7,9 +7,9 @@
 // only as C++ (qsf::Backend::enumerate, distfind::gamma_sequence).  These extern "C"
 // wrappers make both reachable from ctypes so the C restatement in oracle/bz_oracle.c
 // and the product's host reduction can be pinned against the reference itself:
-//   ref_enumerate       -> qsf::cpu_backend()->enumerate(EnumPlan)   (cpp/qsf/backend_cpu.cpp:254-268)
+//   ref_enumerate       -> qsf::cpu_backend()->enumerate(EnumPlan)   (cpp/qsf/backend_cpu.cpp:33-75)
 //   ref_problem_gammas  -> classical_problem / css_problem / subsystem_problem + gamma_sequence
-//                          + the rank-descending stable sort of bz_distance (cpp/distfind/bz.cpp:141-153)
+//                          + the rank-descending stable sort of bz_distance (cpp/distfind/bz.cpp:95-107)
 #include "qsf/backend.hpp"
 #include "qsf/combinatorics.hpp"
 #include "distfind/css.hpp"

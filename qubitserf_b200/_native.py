@@ -75,7 +75,7 @@ class QsfbBatchStats(ctypes.Structure):
                 ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong),
                 ("gen_ms", ctypes.c_double), ("host_plan_seconds", ctypes.c_double),
                 ("host_apply_seconds", ctypes.c_double), ("tc_codewords", ctypes.c_ulonglong),
-                ("tc_ms", ctypes.c_double)]
+                ("tc_ms", ctypes.c_double), ("device_sets_seconds", ctypes.c_double)]
 
 
 class QsfbTiming(ctypes.Structure):
@@ -104,6 +104,7 @@ class QsfbCollectStats(ctypes.Structure):
 # (name, restype, argtypes) of every exported function; tests check the export list.
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
 _ip = ctypes.POINTER(ctypes.c_int)
 _ullp = ctypes.POINTER(ctypes.c_ulonglong)
 _rp = ctypes.POINTER(DistfindResult)
@@ -123,6 +124,9 @@ SIGNATURES = [
                                  _ullp]),
     ("qsfb_prepare_problem", _i, [_i, _u8p, _i, _i, _u8p, _i, _i, _ip, _ip, _i, _u64p,
                                   ctypes.c_longlong, _u64p, ctypes.c_longlong]),
+    ("qsfb_prepare_sides", _i, [_i, _u8p, _i, _i, _u8p, _i, _i, _i, _ip, _ip, _i, _u64p,
+                                ctypes.c_longlong, _u64p, ctypes.c_longlong, _u32p,
+                                ctypes.c_longlong, _u32p, ctypes.c_longlong]),
     ("qsfb_last_report", _i, [ctypes.POINTER(QsfbReport)]),
     ("qsfb_last_witness", _i, [_u8p, _i]),
     ("qsfb_last_counts", _i, [_ip, _ip, _ip, _ullp, _i]),
@@ -343,6 +347,39 @@ def prepare_problem(kind, A, B=None):
             "gamma": gamma[: ng * K * stride].reshape(ng, K, stride).copy(),
             "check": check[: kcheck * stride].reshape(kcheck, stride).copy(),
             "even": bool(even), "count_all": bool(count_all), "seed_upper": seed_upper}
+
+
+def prepare_sides(kind, A, B=None, on_device=True):
+    """The subproblem's information sets built on the device (on_device) or the host, with
+    the packed non-pivot rows and detector syndromes the pair sweeps read."""
+    a = as_u8(A)
+    b = as_u8(B) if B is not None else np.zeros((0, a.shape[1]), np.uint8)
+    meta = (ctypes.c_int * 11)()
+    ncol = a.shape[1] * 3 // 2 if kind == 5 else a.shape[1]
+    stride = (ncol + 63) // 64
+    w32 = (ncol + 31) // 32
+    maxg = ncol + 2
+    ranks = (ctypes.c_int * maxg)()
+    gamma = np.zeros(maxg * ncol * stride + 1, dtype=np.uint64)
+    check = np.zeros(ncol * stride + 1, dtype=np.uint64)
+    red = np.zeros(maxg * ncol * w32 + 1, dtype=np.uint32)
+    syn = np.zeros(maxg * ncol * max(1, (ncol + 31) // 32) + 1, dtype=np.uint32)
+    rc = lib().qsfb_prepare_sides(kind, _p(a), a.shape[0], a.shape[1],
+                                  _p(b) if b.size else None, b.shape[0], b.shape[1],
+                                  1 if on_device else 0, meta, ranks, maxg,
+                                  gamma.ctypes.data_as(_u64p), gamma.size,
+                                  check.ctypes.data_as(_u64p), check.size,
+                                  red.ctypes.data_as(_u32p), red.size,
+                                  syn.ctypes.data_as(_u32p), syn.size)
+    _check(rc, "qsfb_prepare_sides")
+    n, K, ng, kcheck, even, count_all, seed_upper, stride, W32, SWP, on_dev = list(meta)
+    return {"n": n, "K": K, "stride": stride, "ranks": [ranks[i] for i in range(ng)],
+            "gamma": gamma[: ng * K * stride].reshape(ng, K, stride).copy(),
+            "check": check[: kcheck * stride].reshape(kcheck, stride).copy(),
+            "red": red[: ng * K * W32].reshape(ng, K, W32).copy(),
+            "syn": syn[: ng * K * SWP].reshape(ng, K, SWP).copy(),
+            "even": bool(even), "count_all": bool(count_all), "seed_upper": seed_upper,
+            "device": bool(on_dev)}
 
 
 def last_report() -> QsfbReport:

@@ -20,7 +20,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <iostream>
-#include <sstream>
+#include <iterator>
 #include <string>
 #include <vector>
 
@@ -64,70 +64,124 @@ struct Matrix {
     std::exit(2);
 }
 
+// Appends rows of one fixed width; the first row sets the width.  `where` names the
+// source in error messages.
+class RowSink {
+public:
+    explicit RowSink(std::string where) : where_(std::move(where)) {}
+    void add(const std::vector<uint8_t>& row, int line) {
+        if (m_.rows == 0) {
+            m_.cols = (int)row.size();
+            first_line_ = line;
+        } else if ((int)row.size() != m_.cols) {
+            die(where_ + ": line " + std::to_string(line) + " has " + std::to_string(row.size()) +
+                " entries, line " + std::to_string(first_line_) + " has " +
+                std::to_string(m_.cols));
+        }
+        m_.bits.insert(m_.bits.end(), row.begin(), row.end());
+        ++m_.rows;
+    }
+    Matrix take() { return std::move(m_); }
+    int rows() const { return m_.rows; }
+
+private:
+    std::string where_;
+    Matrix m_;
+    int first_line_ = 0;
+};
+
+// A 0/1 matrix file: one row per non-blank line, entries separated by blanks, each entry a
+// single 0 or 1.
 Matrix read_matrix_file(const std::string& path) {
-    std::ifstream in(path);
-    if (!in) die("cannot open file: " + path);
-    Matrix m;
-    std::string line;
-    while (std::getline(in, line)) {
-        std::istringstream ls(line);
-        std::vector<uint8_t> row;
-        std::string tok;
-        while (ls >> tok) {
-            if (tok == "0") row.push_back(0);
-            else if (tok == "1") row.push_back(1);
-            else die("matrix file " + path + " contains non-binary token '" + tok + "'");
+    std::ifstream in(path, std::ios::binary);
+    if (!in) die(path + ": cannot be opened");
+    const std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    RowSink sink(path);
+    std::vector<uint8_t> row;
+    int line = 1;
+    size_t i = 0;
+    while (i <= text.size()) {
+        const char c = i < text.size() ? text[i] : '\n';
+        if (c == '\n') {
+            if (!row.empty()) sink.add(row, line);
+            row.clear();
+            ++line;
+            ++i;
+            continue;
         }
-        if (row.empty()) continue;
-        if (m.rows == 0) m.cols = (int)row.size();
-        else if ((int)row.size() != m.cols) die("ragged matrix in " + path + " (rows have differing widths)");
-        m.bits.insert(m.bits.end(), row.begin(), row.end());
-        ++m.rows;
+        if (std::isspace((unsigned char)c)) { ++i; continue; }
+        size_t j = i;   // one entry: up to the next blank
+        while (j < text.size() && !std::isspace((unsigned char)text[j])) ++j;
+        const std::string entry = text.substr(i, j - i);
+        if (entry != "0" && entry != "1")
+            die(path + ": line " + std::to_string(line) + ": entry '" + entry + "' is not 0 or 1");
+        row.push_back((uint8_t)(entry[0] - '0'));
+        i = j;
     }
-    if (m.rows == 0) die("matrix file " + path + " is empty");
-    return m;
+    if (sink.rows() == 0) die(path + ": no rows");
+    return sink.take();
 }
 
-std::vector<std::string> read_lines() {
-    std::vector<std::string> lines;
-    std::string line;
-    while (std::getline(std::cin, line)) {
-        if (!line.empty() && line.back() == '\r') line.pop_back();
-        if (line.empty()) break;
-        lines.push_back(line);
+// Pauli letters: bit 0 = X part, bit 1 = Z part; 4 = not a Pauli letter.
+struct PauliTable {
+    uint8_t code[256];
+    PauliTable() {
+        std::fill(code, code + 256, (uint8_t)4);
+        for (char c : std::string("I._ ")) code[(unsigned char)c] = 0;
+        for (char c : std::string("Xx")) code[(unsigned char)c] = 1;
+        for (char c : std::string("Zz")) code[(unsigned char)c] = 2;
+        for (char c : std::string("Yy")) code[(unsigned char)c] = 3;
     }
-    return lines;
+};
+const PauliTable kPauli;
+
+// x and z parts of one Pauli string; `what` names it in error messages.
+void decode_pauli(const std::string& s, const std::string& what, std::vector<uint8_t>& x,
+                  std::vector<uint8_t>& z, int* kinds) {
+    x.assign(s.size(), 0);
+    z.assign(s.size(), 0);
+    int seen = 0;
+    for (size_t j = 0; j < s.size(); ++j) {
+        const uint8_t c = kPauli.code[(unsigned char)s[j]];
+        if (c == 4)
+            die(what + ": character '" + std::string(1, s[j]) +
+                "' is not a Pauli letter (I . _ X Z Y)");
+        x[j] = c & 1u;
+        z[j] = (c >> 1) & 1u;
+        seen |= c;
+    }
+    if (kinds) *kinds = seen;
 }
 
-// X-type and Z-type rows of CSS generator strings ("what" names them in errors).
-void split_css_rows(const std::vector<std::string>& lines, const char* what, Matrix& X,
-                    Matrix& Z, int& n) {
-    n = (int)lines[0].size();
-    X.cols = Z.cols = n;
-    for (size_t li = 0; li < lines.size(); ++li) {
-        const std::string& s = lines[li];
-        if ((int)s.size() != n) die(std::string(what) + "s have differing lengths");
-        std::vector<uint8_t> x(n, 0), z(n, 0);
-        bool hx = false, hz = false;
-        for (int j = 0; j < n; ++j) {
-            switch (s[j]) {
-                case 'I': case '.': case '_': case ' ': break;
-                case 'X': case 'x': x[j] = 1; hx = true; break;
-                case 'Z': case 'z': z[j] = 1; hz = true; break;
-                case 'Y': case 'y':
-                    die(std::string(what) + " " + std::to_string(li + 1) +
-                        " contains a Y -- only CSS codes are supported");
-                default:
-                    die(std::string(what) + " " + std::to_string(li + 1) +
-                        " has an unrecognised character '" + s[j] + "'");
-            }
-        }
-        if (hx && hz)
-            die(std::string(what) + " " + std::to_string(li + 1) +
-                " mixes X and Z -- only CSS codes are supported");
-        if (hx) { X.bits.insert(X.bits.end(), x.begin(), x.end()); ++X.rows; }
-        else if (hz) { Z.bits.insert(Z.bits.end(), z.begin(), z.end()); ++Z.rows; }
+// Generator strings from stdin: one per line up to a blank line or the end of input.  Each
+// must be a pure X or a pure Z string (CSS input); identity-only lines carry no generator.
+void read_css_generators(Matrix& X, Matrix& Z, int& n, bool& any) {
+    RowSink xs("input"), zs("input");
+    std::string s;
+    int line = 0;
+    n = -1;
+    any = false;
+    std::vector<uint8_t> x, z;
+    while (std::getline(std::cin, s)) {
+        ++line;
+        if (!s.empty() && s.back() == '\r') s.pop_back();
+        if (s.empty()) break;
+        any = true;
+        if (n < 0) n = (int)s.size();
+        if ((int)s.size() != n)
+            die("input line " + std::to_string(line) + ": length " + std::to_string(s.size()) +
+                ", the first line has " + std::to_string(n));
+        int kinds = 0;
+        decode_pauli(s, "input line " + std::to_string(line), x, z, &kinds);
+        if (kinds == 3)
+            die("input line " + std::to_string(line) +
+                ": not a pure X or pure Z generator (CSS input only)");
+        if (kinds == 1) xs.add(x, line);
+        else if (kinds == 2) zs.add(z, line);
     }
+    X = xs.take();
+    Z = zs.take();
+    X.cols = Z.cols = std::max(n, 0);
 }
 
 const uint8_t* data_or_dummy(const Matrix& m) {
@@ -196,24 +250,16 @@ int main(int argc, char** argv) {
     if (o.op_mode) {
         if (!o.hx_path.empty())
             die("-o/--operator reads generators and the operator from stdin (no --hx/--hz)");
-        const std::vector<std::string> lines = read_lines();
-        if (lines.empty()) die("operator mode needs at least one generator line on stdin");
         Matrix Gx, Gz;
         int n = 0;
-        split_css_rows(lines, "generator", Gx, Gz, n);
+        bool any = false;
+        read_css_generators(Gx, Gz, n, any);
+        if (!any) die("operator mode: no generator lines on stdin");
         if ((int)o.op.size() != n)
-            die("operator length (" + std::to_string(o.op.size()) +
-                ") differs from the generators (" + std::to_string(n) + ")");
-        std::vector<uint8_t> z(n, 0), x(n, 0);
-        for (int j = 0; j < n; ++j) {
-            switch (o.op[j]) {
-                case 'I': case '.': case '_': case ' ': break;
-                case 'X': case 'x': x[j] = 1; break;
-                case 'Z': case 'z': z[j] = 1; break;
-                case 'Y': case 'y': x[j] = z[j] = 1; break;
-                default: die(std::string("operator has an unrecognised character '") + o.op[j] + "'");
-            }
-        }
+            die("operator has length " + std::to_string(o.op.size()) + ", the generators " +
+                std::to_string(n));
+        std::vector<uint8_t> z, x;
+        decode_pauli(o.op, "operator", x, z, nullptr);
         // with --subsystem the generators are the gauge group: the coset is taken modulo it
         DistfindOpResult w{};
         const int rc = distfind_operator_weight(data_or_dummy(Gx), Gx.rows, n, data_or_dummy(Gz),
@@ -235,12 +281,13 @@ int main(int argc, char** argv) {
     if (!o.hx_path.empty()) {
         X = read_matrix_file(o.hx_path);
         Z = read_matrix_file(o.hz_path);
-        if (X.cols != Z.cols) die("Hx and Hz have differing column counts (different number of qubits)");
+        if (X.cols != Z.cols)
+            die("--hx has " + std::to_string(X.cols) + " columns, --hz " + std::to_string(Z.cols));
     } else {
-        const std::vector<std::string> lines = read_lines();
-        if (lines.empty()) die("no stabilisers on stdin (provide Pauli strings or --hx/--hz)");
         int n = 0;
-        split_css_rows(lines, "stabiliser", X, Z, n);
+        bool any = false;
+        read_css_generators(X, Z, n, any);
+        if (!any) die("no generator lines on stdin (Pauli strings, or --hx/--hz files)");
     }
     if (o.verbose)
         std::cerr << "qsfb-distfind: method=" << o.method << " backend=" << o.backend

@@ -1,5 +1,5 @@
 // BZ schedule on the device engine.  Bounds, termination, verbose lines and the Z/X
-// interleave keep the reference's semantics (cpp/distfind/bz.cpp:118-403,
+// interleave keep the reference's semantics (cpp/distfind/bz.cpp:72-370,
 // cpp/distfind/progress.hpp:12-33) so that distance, lower_bound, proven and levels agree
 // with the reference run on the same host; the enumeration itself runs on the GPU.
 #include "bz.hpp"
@@ -18,6 +18,9 @@
 #include <thread>
 #include <cstring>
 
+#include <nvtx3/nvToolsExt.h>
+
+#include "infoset_types.hpp"
 #include "seed_types.hpp"
 
 namespace qsfb {
@@ -38,6 +41,13 @@ void verbose_bound(int lb, double secs, const char* tag) {
     else std::fprintf(stderr, "Distance bound: >%d\n", lb);
     fprint_elapsed(secs);
 }
+// DISTFIND_PROFILE: one line per enumerated level of a single-side run, in the reference's
+// format (cpp/distfind/bz.cpp:132, 147-155), with the backend named "cuda".
+bool profile_on() {
+    static const bool on = std::getenv("DISTFIND_PROFILE") != nullptr;
+    return on;
+}
+
 void verbose_final(int d, double secs, const char* tag) {
     if (*tag) std::fprintf(stderr, "%s-distance: =%d\n", tag, d);
     else std::fprintf(stderr, "Distance: =%d\n", d);
@@ -195,10 +205,13 @@ int BzSide::setup_host(const Problem& p, const BzOptions& opt, const char* t) {
     even = p.even;
     has_logicals = !(K == 0 || (!p.count_all && p.check.rows == 0));
     if (!has_logicals) { resolved = resolved0 = true; return kOk; }
-    sets = information_sets(p.code_gen);
-    ng = (int)sets.size();
-    ranks.resize(ng);
-    for (int g = 0; g < ng; ++g) ranks[g] = sets[g].rank;
+    const bool dev_sets = opt.device_infosets && K <= kInfosetMaxK && p.n <= kInfosetMaxN;
+    if (!dev_sets) {
+        sets = information_sets(p.code_gen);
+        ng = (int)sets.size();
+        ranks.resize(ng);
+        for (int g = 0; g < ng; ++g) ranks[g] = sets[g].rank;
+    }
     inner = p.seed_upper > 0 ? p.seed_upper : kWeightNone;
     if (p.seed_upper > 0) best_word = p.seed_word;
     if (opt.device_seed && K <= kSeedMaxK && p.n <= kSeedMaxN && opt.seed_trials <= 256 &&
@@ -216,7 +229,22 @@ int BzSide::setup_host(const Problem& p, const BzOptions& opt, const char* t) {
     maxw = K;
     inner0 = inner;
     resolved0 = resolved;
+    if (dev_sets) {
+        infoset_pending = true;   // built by setup_jobs_device
+        return kOk;
+    }
     return dev.prepare(p, sets);
+}
+
+int BzSide::adopt_sets(std::vector<InfoSet>&& s, uint32_t* red, uint32_t* syn, int W32, int SWP,
+                       Device* d, Arena* arena) {
+    infoset_pending = false;
+    sets = std::move(s);
+    ng = (int)sets.size();
+    ranks.resize(ng);
+    for (int g = 0; g < ng; ++g) ranks[g] = sets[g].rank;
+    if (!red) return dev.prepare(*prob, sets);
+    return dev.adopt_device(*prob, sets, red, syn, W32, SWP, d, arena);
 }
 
 void BzSide::reset() {
@@ -409,6 +437,13 @@ void BzJob::apply(const std::vector<const LevelOut*>& outs, const std::vector<in
         const LevelOut o = out_for(0);
         S.absorb(w, o);
         record(0, o);
+        if (profile_on() && S.has_logicals) {
+            const unsigned long long total = host_binom(S.K, w);
+            const int act = S.active_at(w);
+            std::fprintf(stderr, "[prof cuda] d=%d K=%d ng=%d/%d stride=%d total=%llu "
+                         "work=%llu -> %.3f ms\n", w, S.K, act, S.ng, words_for(p[0].n), total,
+                         total * (unsigned long long)act, 1e3 * (now - tl_));
+        }
         if (S.inner <= S.outer && !no_stop_) {
             S.proven = true;
             done_ = true;
@@ -609,6 +644,13 @@ int setup_jobs_device(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>
                       RunStats* stats) {
     int rc = device_seeds(s, arena, jobs, stats);
     if (rc != kOk) return rc;
+    std::vector<BzSide*> pend;
+    for (BzJob* j : jobs)
+        if (!j->zero)
+            for (int i = 0; i < (j->pair ? 2 : 1); ++i)
+                if (j->s[i].infoset_pending) pend.push_back(&j->s[i]);
+    rc = device_infosets(s, arena, pend, stats);
+    if (rc != kOk) return rc;
     std::vector<SideDev*> sides;
     for (BzJob* j : jobs)
         for (SideDev* sd : j->device_sides()) sides.push_back(sd);
@@ -654,7 +696,9 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
         RunStats rs;
         outs.clear();
         if (!q.empty()) {
+            nvtxRangePushA("qsfb round");   // one range per round for profilers (no-op alone)
             rc = run_levels(s, q, outs, &rs);
+            nvtxRangePop();
             if (rc != kOk) break;
         }
         // per-job slices (requests of one job are contiguous)

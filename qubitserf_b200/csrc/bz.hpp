@@ -5,7 +5,7 @@
 // weight level per ROUND; every unresolved job of a round contributes its level to ONE
 // run_levels() call, so a single code (the plain drop-in) and a batch of a thousand codes
 // run through the same code path.  Bounds, termination and the Z/X cap keep the
-// reference's semantics (cpp/distfind/bz.cpp:118-403):
+// reference's semantics (cpp/distfind/bz.cpp:72-370):
 //   outer(w) = sum_g max(0, (w+1) - (K - rank_g))  (+1 if odd and every codeword is even)
 //   stop when inner <= outer; a pair side is capped once its outer reaches the best found.
 // In a pair both sides' level w run in the same round; the X result is folded in only if
@@ -29,6 +29,8 @@ struct BzOptions {
     int seed_trials = 256;
     bool parallel_seed = true;   // host seed trials on hardware_concurrency threads
     bool device_seed = true;     // eliminations of the seed trials on the GPU when K, n <= 128
+    bool device_infosets = false; // information sets (and the packed rows) built on the GPU
+                                 // when K, n <= 128
 };
 
 // One enumerated level, for the per-(information set, w) count record.
@@ -100,6 +102,12 @@ public:
     int seed_trial = -1, seed_row = -1;
     std::shared_ptr<const std::vector<uint8_t>> seed_perm;   // trials x n, shared by length
     void apply_device_seed(unsigned key);
+    // information sets pending on the GPU (setup_jobs_device builds them and the packed rows)
+    bool infoset_pending = false;
+    // Take the sets built on the device (or, with red == nullptr, build the rows on the host
+    // for upload): fills ng, ranks and the device image.
+    int adopt_sets(std::vector<InfoSet>&& s, uint32_t* red, uint32_t* syn, int W32, int SWP,
+                   Device* d, Arena* arena);
 };
 
 class BzJob {
@@ -158,6 +166,11 @@ int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
 int setup_jobs_host(std::vector<BzJob*>& jobs, int host_threads, RunStats* stats);
 int setup_jobs_device(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
                       RunStats* stats);
+// The information sets of every side whose construction is pending, on the device (one
+// warp per side), with their packed rows and syndromes written into `arena`; sides the
+// kernel cannot hold fall back to the host construction (rows uploaded by upload_sides).
+int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
+                    RunStats* stats);
 // `feed` (optional) is called at the top of every round with idle = false and may append
 // jobs to `jobs` (they start from their first level in that round); when every job is done
 // it is called with idle = true, may block until it has more, and returns whether it

@@ -1,5 +1,5 @@
 // extern "C" boundary of libqsfb200.so.  The distfind_* functions keep the reference's
-// signatures, result structs, dispatch and return codes (cpp/distfind/capi.cpp:144-420);
+// signatures, result structs, dispatch and return codes (cpp/distfind/capi.cpp:16-301);
 // every accepted call runs on the GPU (method "bz": the BZ enumeration; "mitm": the
 // meet-in-the-middle join of mitm.cu) and there is no CPU path.
 #include "../../include/qsf_b200.h"
@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "bz.hpp"
+#include "infoset_types.hpp"
 #include "engine.hpp"
 #include "mitm.hpp"
 #include "problem.hpp"
@@ -113,7 +114,7 @@ int solve_one(Device* dev, const Problem& p, bool mitm, int verbose, BzResult& r
     return mitm ? mitm_distance(dev, p, r) : bz_distance(dev, p, options(verbose), r);
 }
 
-// Merge for the (non-interleaved) subsystem min, cpp/distfind/capi.cpp:265-274.
+// Merge for the (non-interleaved) subsystem min, cpp/distfind/capi.cpp:147-156.
 BzResult min_of(const BzResult& z, const BzResult& x) {
     auto v = [](int d) { return d < 0 ? (1 << 30) : d; };
     BzResult r = (v(x.distance) < v(z.distance)) ? x : z;
@@ -424,6 +425,7 @@ int batch_execute(QsfbBatchHandle* H, QsfbAnswer* out, QsfbBatchStats* stats, in
         stats->prepare_seconds = H->prepare_s;
         stats->host_setup_seconds = H->setup.host_setup_s;
         stats->device_seed_seconds = H->setup.device_seed_s;
+        stats->device_sets_seconds = H->setup.device_sets_s;
         stats->certificates = (int)H->jobs.size();
         stats->device_bytes = (long long)H->arena->bytes();
     }
@@ -452,7 +454,7 @@ int distfind_classical_distance(const uint8_t* H, int rows, int cols, const char
                                 DistfindResult* out) {
     (void)threads;
     if (!out || !H) return kErrNull;
-    // the classical path has no cc form: the reference runs BZ for it (capi.cpp:79)
+    // the classical path has no cc form: the reference runs BZ for it (cpp/distfind/capi.cpp:79)
     const bool mitm = is_mitm(method);
     int rc = check_dispatch(mitm ? "mitm" : "bz", backend);
     if (rc != kOk) return rc;
@@ -490,7 +492,7 @@ int distfind_operator_weight(const uint8_t* Gx, int gx_rows, int gx_cols, const 
     bool proven = true;
     BzResult last;
     int nbits = A.cols;
-    // cpp/distfind/op_weight.cpp:22-41: Z part modulo rowspace(Gz), X part modulo rowspace(Gx).
+    // cpp/distfind/op_weight.cpp:9-36: Z part modulo rowspace(Gz), X part modulo rowspace(Gx).
     auto solve = [&](const Mat& G, const uint8_t* vec, int* res) -> int {
         if (in_rowspace(G, vec)) { *res = 0; return kOk; }
         Problem p = coset_problem(G, vec);
@@ -645,28 +647,31 @@ int qsfb_enumerate_plan(int n, int stride, int K, int d, int num_gamma, const ui
     return kOk;
 }
 
-int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
-                         int bc, int* meta, int* ranks, int max_gamma, uint64_t* gamma,
-                         long long max_words, uint64_t* check, long long max_check) {
-    if (!A || !meta) return kErrNull;
+namespace {
+// The BZ subproblem of one query kind (the reductions qsfb_prepare_problem documents).
+int kind_problem(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br, int bc,
+                 Problem* p) {
     Mat mA = from_dense(A, ar, ac);
     Mat mB = (B && br > 0) ? from_dense(B, br, bc) : Mat(0, ac);
-    Problem p;
     switch (kind) {
-        case 0: p = classical_problem(mA); break;
-        case 1: p = css_problem(mA, mB, 'Z'); break;
-        case 2: p = css_problem(mA, mB, 'X'); break;
-        case 3: p = subsystem_problem(mA, mB, 'Z'); break;
-        case 4: p = subsystem_problem(mA, mB, 'X'); break;
+        case 0: *p = classical_problem(mA); break;
+        case 1: *p = css_problem(mA, mB, 'Z'); break;
+        case 2: *p = css_problem(mA, mB, 'X'); break;
+        case 3: *p = subsystem_problem(mA, mB, 'Z'); break;
+        case 4: *p = subsystem_problem(mA, mB, 'X'); break;
         case 5:
             if (ac % 2) return kErrShape;
-            p = isometry_extend(symplectic_problem(mA, mA));
+            *p = isometry_extend(symplectic_problem(mA, mA));
             break;
         default: return kErrShape;
     }
+    return kOk;
+}
+
+int write_sets(const Problem& p, const std::vector<InfoSet>& sets, int* meta, int* ranks,
+               int max_gamma, uint64_t* gamma, long long max_words, uint64_t* check,
+               long long max_check) {
     const int K = p.code_gen.rows, stride = words_for(p.n);
-    std::vector<InfoSet> sets;
-    if (K > 0) sets = information_sets(p.code_gen);
     const int ng = (int)sets.size();
     const int kcheck = p.count_all ? 0 : p.check.rows;
     meta[0] = p.n; meta[1] = K; meta[2] = ng; meta[3] = kcheck;
@@ -683,6 +688,81 @@ int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8
     if (check)
         for (int c = 0; c < kcheck; ++c)
             std::copy(p.check.row(c), p.check.row(c) + stride, check + (size_t)c * stride);
+    return kOk;
+}
+}  // namespace
+
+int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
+                         int bc, int* meta, int* ranks, int max_gamma, uint64_t* gamma,
+                         long long max_words, uint64_t* check, long long max_check) {
+    if (!A || !meta) return kErrNull;
+    Problem p;
+    const int rc = kind_problem(kind, A, ar, ac, B, br, bc, &p);
+    if (rc != kOk) return rc;
+    std::vector<InfoSet> sets;
+    if (p.code_gen.rows > 0) sets = information_sets(p.code_gen);
+    return write_sets(p, sets, meta, ranks, max_gamma, gamma, max_words, check, max_check);
+}
+
+int qsfb_prepare_sides(int kind, const uint8_t* A, int ar, int ac, const uint8_t* B, int br,
+                       int bc, int on_device, int* meta, int* ranks, int max_gamma,
+                       uint64_t* gamma, long long max_words, uint64_t* check, long long max_check,
+                       uint32_t* red, long long max_red, uint32_t* syn, long long max_syn) {
+    if (!A || !meta) return kErrNull;
+    Problem p;
+    int rc = kind_problem(kind, A, ar, ac, B, br, bc, &p);
+    if (rc != kOk) return rc;
+    const int K = p.code_gen.rows;
+    const int kcheck = p.count_all ? 0 : p.check.rows;
+    const int W32 = (p.n + 31) / 32, SWP = std::max(1, (kcheck + 31) / 32);
+    meta[8] = W32;
+    meta[9] = SWP;
+    meta[10] = 0;
+    if (K == 0) return write_sets(p, {}, meta, ranks, max_gamma, gamma, max_words, check, max_check);
+    BzSide S;   // only its information sets and device image are used
+    S.prob = &p;
+    S.K = K;
+    std::unique_ptr<Arena> arena;
+    std::unique_ptr<SessionLease> lease;
+    const bool dev_ok = on_device && K <= kInfosetMaxK && p.n <= kInfosetMaxN;
+    if (dev_ok) {
+        Device* dev = device_or(&rc);
+        if (!dev) return rc;
+        lease.reset(new SessionLease(dev));
+        if (!lease->s) return kErrDevice;
+        arena.reset(new Arena(dev, 1ull << 20));
+        S.infoset_pending = true;
+        rc = device_infosets(lease->s, arena.get(), {&S}, nullptr);
+        if (rc != kOk) return rc;
+        meta[10] = S.dev.device_rows ? 1 : 0;
+    } else {
+        rc = S.adopt_sets(information_sets(p.code_gen), nullptr, nullptr, 0, 0, nullptr, nullptr);
+        if (rc != kOk) return rc;
+    }
+    rc = write_sets(p, S.sets, meta, ranks, max_gamma, gamma, max_words, check, max_check);
+    if (rc != kOk) return rc;
+    const int ng = S.ng;
+    if ((red && (long long)ng * K * W32 > max_red) || (syn && (long long)ng * K * SWP > max_syn))
+        return 7;
+    const SideDev& D = S.dev;
+    std::vector<uint32_t> hr, hs;
+    if (D.device_rows) {
+        hr.resize((size_t)ng * K * W32);
+        hs.resize((size_t)ng * K * SWP);
+        if (cudaMemcpy(hr.data(), D.d_red, hr.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(hs.data(), D.d_syn, hs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            cudaGetLastError();
+            return kErrDevice;
+        }
+    } else {   // host rows: re-stride to W32 = ceil(n/32) words, zero padded
+        hr.assign((size_t)ng * K * W32, 0u);
+        for (size_t r = 0; r < (size_t)ng * K; ++r)
+            std::copy(D.h_red.begin() + r * D.W32, D.h_red.begin() + (r + 1) * D.W32,
+                      hr.begin() + r * W32);
+        hs = D.h_syn;
+    }
+    if (red) std::copy(hr.begin(), hr.end(), red);
+    if (syn) std::copy(hs.begin(), hs.end(), syn);
     return kOk;
 }
 
@@ -760,7 +840,7 @@ int batch_prepare_host(const QsfbQuery* queries, int nq, int host_threads,
                 return 0;
             }, !single, opt));
         } else {
-            // Z part modulo rowspace(Gz), X part modulo rowspace(Gx) (op_weight.cpp:22-41)
+            // Z part modulo rowspace(Gz), X part modulo rowspace(Gx) (op_weight.cpp:9-36)
             m.job0 = (int)jobs.size();
             jobs.emplace_back(new BzJob([q](Problem& p0, Problem&) {
                 Mat B = from_dense(q.B, q.b_rows, q.b_cols);
@@ -935,12 +1015,13 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     if (trace)   // one stderr line per chunk (ms from the call)
         for (int c = 0; c < nchunks; ++c)
             std::fprintf(stderr, "qsfb_batch chunk %d: %d codes, prepare %.2f-%.2f ms (host "
-                         "reduction %.2f ms, device seeds %.2f ms of which %.2f waiting); "
-                         "rounds %.2f-%.2f ms\n", c,
+                         "reduction %.2f ms, device seeds %.2f ms of which %.2f waiting, "
+                         "device sets %.2f ms); rounds %.2f-%.2f ms\n", c,
                          cut[c + 1] - cut[c], 1e3 * (tp0[c] - t0), 1e3 * (tp1[c] - t0),
                          H[c] ? 1e3 * H[c]->setup.host_setup_s : 0.0,
                          H[c] ? 1e3 * H[c]->setup.device_seed_s : 0.0,
-                         H[c] ? 1e3 * H[c]->setup.device_seed_wait_s : 0.0, 1e3 * (te0 - t0),
+                         H[c] ? 1e3 * H[c]->setup.device_seed_wait_s : 0.0,
+                         H[c] ? 1e3 * H[c]->setup.device_sets_s : 0.0, 1e3 * (te0 - t0),
                          1e3 * (te1 - t0));
     if (stats && rc == kOk) {
         std::memset(stats, 0, sizeof(*stats));
@@ -949,6 +1030,7 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
             stats->prepare_seconds += h->prepare_s;
             stats->host_setup_seconds += h->setup.host_setup_s;
             stats->device_seed_seconds += h->setup.device_seed_s;
+            stats->device_sets_seconds += h->setup.device_sets_s;
             stats->certificates += (int)h->jobs.size();
             stats->device_bytes += (long long)h->arena->bytes();
         }

@@ -333,6 +333,39 @@ int SideDev::prepare(const Problem& p, const std::vector<InfoSet>& sets) {
     return kOk;
 }
 
+int SideDev::adopt_device(const Problem& p, const std::vector<InfoSet>& sets, uint32_t* red,
+                          uint32_t* syn, int W32_, int SWP, Device* d, Arena* a) {
+    n = p.n;
+    K = p.code_gen.rows;
+    ng = (int)sets.size();
+    count_all = p.count_all;
+    kcheck = p.count_all ? 0 : p.check.rows;
+    if (K > kBinomMaxN || ng > 255 || ng == 0) return kErrUnsupported;
+    ranks.resize(ng);
+    nonpivot.assign(ng, {});
+    for (int g = 0; g < ng; ++g) {
+        ranks[g] = sets[g].rank;
+        std::vector<char> isp(n, 0);
+        for (int c : sets[g].pivots) isp[c] = 1;
+        for (int c = 0; c < n; ++c)
+            if (!isp[c]) nonpivot[g].push_back(c);
+    }
+    W32 = W32_;
+    SW = (kcheck + 31) / 32;
+    if (W32 > 32 || SW > 32 || std::max(SW, 1) != SWP) return kErrUnsupported;
+    h_red.clear();
+    h_syn.clear();
+    bytes_red = (size_t)ng * K * W32 * 4;
+    bytes_syn = (size_t)ng * K * SWP * 4;
+    dev = d;
+    arena = a;
+    owns = false;
+    d_red = red;
+    d_syn = syn;
+    device_rows = true;
+    return kOk;
+}
+
 int SideDev::upload(Device* d, Session* s) {
     dev = d;
     owns = true;
@@ -350,7 +383,8 @@ int SideDev::upload(Device* d, Session* s) {
 
 int upload_sides(Device* dev, Session* s, Arena* arena, const std::vector<SideDev*>& sides) {
     size_t total = 0;
-    for (SideDev* S : sides) total += align_up(S->bytes_red, 256) + align_up(S->bytes_syn, 256);
+    for (SideDev* S : sides)
+        if (!S->device_rows) total += align_up(S->bytes_red, 256) + align_up(S->bytes_syn, 256);
     if (total == 0) return kOk;
     char* d = (char*)arena->alloc(total);
     if (!d) return kErrMemory;
@@ -359,6 +393,7 @@ int upload_sides(Device* dev, Session* s, Arena* arena, const std::vector<SideDe
     char* h = (char*)s->h_stage.h;
     size_t off = 0;
     for (SideDev* S : sides) {
+        if (S->device_rows) continue;   // built in place by the information-set kernel
         S->dev = dev;
         S->arena = arena;
         S->owns = false;

@@ -173,6 +173,11 @@ public:
     int prepare(const Problem& p, const std::vector<InfoSet>& sets);
     // Device half for a single side: own allocation + copy on the session stream.
     int upload(Device* dev, Session* s);
+    // The rows were built on the device (the information-set kernel wrote red/syn into
+    // `arena` with row strides W32 and SWP): take the host-side description of the sets.
+    int adopt_device(const Problem& p, const std::vector<InfoSet>& sets, uint32_t* red,
+                     uint32_t* syn, int W32, int SWP, Device* dev, Arena* arena);
+    bool device_rows = false;    // red/syn built on the device (nothing to upload)
 
     int n = 0, K = 0, ng = 0, W32 = 0, SW = 0, kcheck = 0;
     bool count_all = false;
@@ -221,6 +226,7 @@ struct RunStats {
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)
     double device_seed_wait_s = 0.0;   // of which: waiting for the copies and the kernel
+    double device_sets_s = 0.0;   // wall time of the device information-set phase
     double host_plan_s = 0.0;     // run_levels host work before the launches
     double host_apply_s = 0.0;    // schedule updates after each round
 };

@@ -1,6 +1,6 @@
 // Information-set construction.  The column partition decides the ranks, hence the BZ
 // lower bound at every level; the partition algorithm therefore keeps the reference's
-// steps and tie-breaking (cpp/distfind/css.cpp:258-447): greedy peel, then an augmenting
+// steps and tie-breaking (cpp/distfind/css.cpp:177-366): greedy peel, then an augmenting
 // DFS matroid partition with the same class order, element order and size sort.
 #include "infoset.hpp"
 
@@ -11,7 +11,7 @@ namespace qsfb {
 
 namespace {
 
-// cpp/distfind/css.cpp:258-284
+// cpp/distfind/css.cpp:177-203
 std::vector<InfoSet> greedy_sets(const Mat& code_gen) {
     std::vector<InfoSet> seq;
     const int n = code_gen.cols;
@@ -37,7 +37,7 @@ std::vector<InfoSet> greedy_sets(const Mat& code_gen) {
 }
 
 // Express column z over the independent class `cls`: (in_span, circuit) where circuit is
-// the ascending list of class columns whose XOR is z (cpp/distfind/css.cpp:316-351).
+// the ascending list of class columns whose XOR is z (cpp/distfind/css.cpp:232-266).
 // Origins are kept as bitsets over the columns, so the reference's sorted-list symmetric
 // difference becomes an XOR and the circuit is read out in ascending order.  A class is
 // independent, so both answers are unique whatever order its columns are inserted in:
@@ -116,7 +116,7 @@ struct Expresser {
     }
 };
 
-// cpp/distfind/css.cpp:355-409
+// cpp/distfind/css.cpp:274-328
 bool matroid_partition(const Mat& code_gen, std::vector<std::vector<int>>& out) {
     const int n = code_gen.cols, K = code_gen.rows, kw = words_for(K);
     // columns as bit vectors over the rows (transpose by the set bits of each row)
@@ -196,39 +196,66 @@ int count_full(const std::vector<InfoSet>& s, int K) {
     return f;
 }
 
-std::vector<InfoSet> gamma_sequence(const Mat& code_gen) {
+}  // namespace
+
+int full_sets(const std::vector<InfoSet>& s, int K) { return count_full(s, K); }
+
+bool matroid_sets(const Mat& code_gen, int greedy_full, std::vector<std::vector<int>>* lists,
+                  std::vector<int>* ranks) {
     const int K = code_gen.rows, n = code_gen.cols;
-    std::vector<InfoSet> greedy = greedy_sets(code_gen);
-    if (K == 0) return greedy;
+    if (K == 0) return false;
     std::vector<u64> any(code_gen.stride, 0ull);   // columns holding a 1 in some row
     for (int i = 0; i < K; ++i) vec_or(any.data(), code_gen.row(i), code_gen.stride);
     int nnz = 0;
     for (int w = 0; w < code_gen.stride; ++w) nnz += popc64(any[w]);
-    (void)n;
     const int max_full = nnz / K;
-    const int greedy_full = count_full(greedy, K);
-    if (greedy_full >= max_full || n > 200) return greedy;
+    if (greedy_full >= max_full || n > 200) return false;
     std::vector<std::vector<int>> part;
-    if (!matroid_partition(code_gen, part)) return greedy;
+    if (!matroid_partition(code_gen, part)) return false;
     std::sort(part.begin(), part.end(),
               [](const std::vector<int>& a, const std::vector<int>& b) {
                   return a.size() > b.size();
               });
-    std::vector<InfoSet> seq;
+    // The nonzero columns of a class are independent, so its restricted RREF has one pivot
+    // per nonzero column: the ranks are known before any elimination.
+    std::vector<std::vector<int>> seq;
+    std::vector<int> rk;
+    int full = 0;
     for (auto& cols : part) {
         if (cols.empty()) continue;
-        Mat work = code_gen;
-        std::vector<int> piv = restricted_rref(work, cols);
-        seq.push_back({work, (int)piv.size(), piv});
+        int r = 0;
+        for (int c : cols) r += (int)((any[c >> 6] >> (c & 63)) & 1u);
+        full += (r == K);
+        seq.push_back(cols);
+        rk.push_back(r);
     }
-    if (seq.empty() || count_full(seq, K) <= greedy_full) return greedy;
-    return seq;
+    if (seq.empty() || full <= greedy_full) return false;
+    std::vector<int> order(seq.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rk[a] > rk[b]; });
+    lists->clear();
+    ranks->clear();
+    for (int i : order) {
+        lists->push_back(std::move(seq[i]));
+        ranks->push_back(rk[i]);
+    }
+    return true;
 }
 
-}  // namespace
-
 std::vector<InfoSet> information_sets(const Mat& code_gen) {
-    std::vector<InfoSet> seq = gamma_sequence(code_gen);
+    // cpp/distfind/css.cpp:336-366: greedy peel, replaced by the matroid partition when it
+    // packs more full-rank sets; then the rank-descending stable sort of bz.cpp:95-97
+    std::vector<InfoSet> seq = greedy_sets(code_gen);
+    std::vector<std::vector<int>> lists;
+    std::vector<int> ranks;
+    if (matroid_sets(code_gen, count_full(seq, code_gen.rows), &lists, &ranks)) {
+        seq.clear();
+        for (const auto& cols : lists) {
+            Mat work = code_gen;
+            std::vector<int> piv = restricted_rref(work, cols);
+            seq.push_back({work, (int)piv.size(), piv});
+        }
+    }
     std::stable_sort(seq.begin(), seq.end(),
                      [](const InfoSet& a, const InfoSet& b) { return a.rank > b.rank; });
     return seq;

@@ -44,7 +44,7 @@ struct DevTable {
     size_t bytes = 0;
 };
 
-// One MITM subproblem stepped level by level (the reference's MitmSide, mitm.cpp:382-426).
+// One MITM subproblem stepped level by level (the reference's MitmSide, cpp/distfind/mitm.cpp:403-448).
 class MitmSide {
 public:
     ~MitmSide() { release(); }
@@ -285,7 +285,7 @@ int mitm_min_interleaved(Device* dev, const Problem& pz, const Problem& px, BzRe
     int rc = Z.setup(dev, lease.s, pz);
     if (rc == kOk) rc = X.setup(dev, lease.s, px);
     if (rc != kOk) return rc;
-    // cpp/distfind/mitm.cpp:447-493 with cap_to_min
+    // cpp/distfind/mitm.cpp:467-516 with cap_to_min
     MitmSide* sides[2] = {&Z, &X};
     int best = kWeightNone;
     if (Z.has_logicals && Z.seed_upper > 0) best = std::min(best, Z.seed_upper);

@@ -1,6 +1,6 @@
 // Meet-in-the-middle distance (method "mitm") on the device: same problems, results and
 // level semantics as the reference's mitm_distance / mitm_min_interleaved
-// (cpp/distfind/mitm.cpp:318-521).  No witness is produced (the reference returns none).
+// (cpp/distfind/mitm.cpp:318-537).  No witness is produced (the reference returns none).
 #pragma once
 #include "bz.hpp"
 

@@ -15,7 +15,7 @@ int lowest_set(const u64* v, int stride) {
 }
 
 // Incrementally built triangular basis keyed by each row's lowest set column
-// (the reducing basis of cpp/distfind/css.cpp:98-126).
+// (the reducing basis of cpp/distfind/css.cpp:17-45).
 struct Reducer {
     Mat rows;
     std::vector<int> piv;
@@ -70,7 +70,7 @@ Mat rows_combine(const Mat& C, const Mat& B) {
     return out;
 }
 
-// cpp/distfind/css.cpp:159-168
+// cpp/distfind/css.cpp:78-87
 Problem build(const Mat& Hself, const Mat& Hother) {
     Problem p;
     p.n = Hself.cols;
@@ -95,7 +95,7 @@ std::vector<u64> pack_bytes(const u8* vec, int n) {
 }  // namespace
 
 namespace {
-// Rows of ko = nullspace(other) independent of rowspan(self) (cpp/distfind/css.cpp:175-186).
+// Rows of ko = nullspace(other) independent of rowspan(self) (cpp/distfind/css.cpp:94-105).
 Mat quotient_of(const Mat& self, const Mat& ko) {
     Reducer basis(self.cols);
     std::vector<u64> t(std::max(1, self.stride));
@@ -279,7 +279,7 @@ Mat symplectic_center(const Mat& G) {
     return C;
 }
 
-// cpp/distfind/stab.cpp:173-207
+// cpp/distfind/stab.cpp:98-132
 Problem symplectic_problem(const Mat& Snorm, const Mat& Gtriv) {
     Problem p;
     p.symplectic = true;

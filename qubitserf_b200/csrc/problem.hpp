@@ -25,25 +25,25 @@ struct Problem {
     int qubits = 0;
 };
 
-// cpp/distfind/css.cpp:175-186
+// cpp/distfind/css.cpp:94-105
 Mat quotient_basis(const Mat& self, const Mat& other);
-// cpp/distfind/css.cpp:188-190 / 159-168
+// cpp/distfind/css.cpp:107-109 / 78-87
 Problem css_problem(const Mat& Hx, const Mat& Hz, char which);
 // Both sides of a CSS code at once: the same two problems as css_problem(·,'Z') and
 // css_problem(·,'X'), sharing the two nullspaces and the two quotient bases.
 std::pair<Problem, Problem> css_problem_pair(const Mat& Hx, const Mat& Hz);
-// cpp/distfind/css.cpp:192-201
+// cpp/distfind/css.cpp:111-120
 Problem classical_problem(const Mat& H);
-// cpp/distfind/css.cpp:203-214
+// cpp/distfind/css.cpp:122-133
 std::pair<Mat, Mat> css_center(const Mat& Gx, const Mat& Gz);
-// cpp/distfind/css.cpp:216-220
+// cpp/distfind/css.cpp:135-139
 Problem subsystem_problem(const Mat& Gx, const Mat& Gz, char which);
-// cpp/distfind/css.cpp:222-229
+// cpp/distfind/css.cpp:141-148
 bool in_rowspace(const Mat& G, const u8* vec);
-// cpp/distfind/css.cpp:231-255
+// cpp/distfind/css.cpp:150-174
 Problem coset_problem(const Mat& G, const u8* vec);
 
-// Symplectic [z|x] helpers, cpp/distfind/stab.cpp:107-220.
+// Symplectic [z|x] helpers, cpp/distfind/stab.cpp:32-146.
 Mat symplectic_swap(const Mat& m);
 int symplectic_row_weight(const u64* row, int qubits);
 bool is_css_symplectic(const Mat& S);
@@ -51,7 +51,7 @@ std::pair<Mat, Mat> split_css(const Mat& S);
 Mat symplectic_center(const Mat& G);
 Problem symplectic_problem(const Mat& Snorm, const Mat& Gtriv);
 Problem symplectic_coset_problem(const Mat& G, const u8* op);
-// (a|b) -> (a|b|a^b): symplectic weight doubles into Hamming weight, cpp/distfind/stab.cpp:222-253.
+// (a|b) -> (a|b|a^b): symplectic weight doubles into Hamming weight, cpp/distfind/stab.cpp:147-178.
 Problem isometry_extend(const Problem& sp);
 
 // Independent host check of a witness codeword: c lies in rowspan(code_gen), is a logical

@@ -6,7 +6,7 @@ Runs only where the reference CPU library has been built from its sources
 * golden.npz   -- the input matrices (uint8), keyed by case name
 * golden.json  -- per case: the reference's distance / proven flag, and for the
                   no-early-stop cases the reference's per-level (w, active, work) trace
-                  read from its DISTFIND_PROFILE lines (cpp/distfind/bz.cpp:193-201)
+                  read from its DISTFIND_PROFILE lines (cpp/distfind/bz.cpp:147-155)
 
     python tests/golden/make_golden.py              # golden.npz + golden.json
     python tests/golden/make_golden.py --batch1024  # batch1024.json (all 1024 batch codes)

@@ -1,7 +1,7 @@
 """GPU distances through the drop-in C ABI against the reference's golden vectors, the
 reference library itself (full DistfindResult where it is present), the C oracle, and the
 host verification of every returned witness.  Mirrors the reference's GPU tests
-(tests/distfind/test_distance.py:167-242): strict equality, repeated runs, Z/X alternation,
+(tests/distfind/test_distance.py:129-226): strict equality, repeated runs, Z/X alternation,
 deep paths and large n."""
 from __future__ import annotations
 

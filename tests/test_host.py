@@ -109,7 +109,7 @@ def _prep_cases(golden):
 
 def test_host_reduction_bit_exact_vs_reference(native, ref, golden):
     """Information-set generators, ranks, detector, parity and seed bound equal the
-    reference's (cpp/distfind/bz.cpp:141-159) bit for bit."""
+    reference's (cpp/distfind/bz.cpp:95-115) bit for bit."""
     if ref is None:
         pytest.skip("reference library not built here")
     for name, kind, mats in _prep_cases(golden):
@@ -130,9 +130,38 @@ def test_host_reduction_matches_oracle(native, orc, golden):
             assert a[k] == b[k], (name, k)
 
 
+def test_prepare_sides_host_construction(native, golden):
+    """The host construction behind qsfb_prepare_sides equals qsfb_prepare_problem, and its
+    packed tables have the documented shapes (rows over ceil(n/32) words, syndromes over
+    max(1, ceil(kcheck/32))); without a device the device construction fails with rc 4."""
+    lib = native.lib()
+    for name, kind, mats in _prep_cases(golden):
+        a = native.prepare_sides(kind, *mats, on_device=False)
+        b = native.prepare_problem(kind, *mats)
+        for k in ("n", "K", "stride", "ranks", "even", "count_all", "seed_upper"):
+            assert a[k] == b[k], (name, k)
+        assert np.array_equal(a["gamma"], b["gamma"]) and np.array_equal(a["check"], b["check"])
+        ng = len(a["ranks"])
+        assert a["red"].shape == (ng, a["K"], (a["n"] + 31) // 32), name
+        assert a["syn"].shape == (ng, a["K"], max(1, (len(a["check"]) + 31) // 32)), name
+        assert not a["device"]
+        # the pivot columns of every set are zero in the packed rows: each row's weight is
+        # its weight outside the set's pivots
+        for g in range(ng):
+            rows = a["gamma"][g]
+            w_full = np.array([sum(bin(int(x)).count("1") for x in r) for r in rows])
+            w_red = np.array([sum(bin(int(x)).count("1") for x in r) for r in a["red"][g]])
+            piv = np.zeros(a["K"], np.int64)
+            piv[: a["ranks"][g]] = 1
+            assert np.array_equal(w_full - piv, w_red), (name, g)
+    if lib.qsfb_device_sms() == 0:
+        with pytest.raises(RuntimeError, match="rc=4:"):
+            native.prepare_sides(0, golden.mats("hamming3")[0], on_device=True)
+
+
 def test_matroid_partition_cases_bit_exact(native, ref):
     """Classical codes where the greedy peel is suboptimal take the matroid partition
-    (cpp/distfind/css.cpp:417-447); the chosen sets must still agree exactly."""
+    (cpp/distfind/css.cpp:336-366); the chosen sets must still agree exactly."""
     if ref is None:
         pytest.skip("reference library not built here")
     from qubitserf_b200.workloads import classical_parity_from_rng
@@ -260,35 +289,48 @@ def _cli(args, stdin=""):
 
 
 def test_cli_usage_errors_exit_2(tmp_path):
-    """qsfb-distfind keeps the reference CLI's input rules (cpp/distfind/cli/
-    distfind_cli.cpp:100-433): usage errors exit 2 with a message on stderr, before any
-    device work."""
+    """qsfb-distfind accepts the reference CLI's inputs (cpp/distfind/cli/
+    distfind_cli.cpp:100-188: CSS Pauli strings on stdin, 0/1 matrix files): malformed input
+    and usage errors exit 2 with a message on stderr, before any device work."""
     rc, out, _ = _cli(["--help"])
     assert rc == 0 and out.startswith("Usage: qsfb-distfind")
     for args, stdin, msg in [
         (["--frobnicate"], "", "unrecognised argument"),
         (["--zx", "--z"], "XXI\n", "--zx cannot be combined"),
         (["--hx", "a.txt"], "", "--hx and --hz must be given together"),
-        ([], "", "no stabilisers on stdin"),
-        ([], "XXZ\n", "mixes X and Z"),
-        ([], "XYI\n", "contains a Y"),
-        ([], "XXI\nZZ\n", "differing lengths"),
-        ([], "XQI\n", "unrecognised character"),
-        (["-o", "XX"], "XXI\n", "operator length"),
+        ([], "", "no generator lines on stdin"),
+        ([], "XXZ\n", "input line 1: not a pure X or pure Z generator"),
+        ([], "IXI\nXYI\n", "input line 2: not a pure X or pure Z generator"),
+        ([], "XXI\nZZ\n", "input line 2: length 2, the first line has 3"),
+        ([], "XQI\n", "input line 1: character 'Q' is not a Pauli letter"),
+        (["-o", "XX"], "XXI\n", "operator has length 2, the generators 3"),
+        (["-o", "XW"], "XI\n", "operator: character 'W' is not a Pauli letter"),
         (["--threads", "x"], "", "non-negative integer"),
     ]:
         rc, out, err = _cli(args, stdin)
         assert rc == 2 and msg in err and out == "", (args, err)
     bad = tmp_path / "ragged.txt"
-    bad.write_text("1 0 1\n0 1\n")
+    bad.write_text("1 0 1\n\n0 1\n")
     good = tmp_path / "good.txt"
     good.write_text("1 1 0\n")
     rc, _, err = _cli(["--hx", str(bad), "--hz", str(good)])
-    assert rc == 2 and "ragged matrix" in err
+    assert rc == 2 and "ragged.txt: line 3 has 2 entries, line 1 has 3" in err
     two = tmp_path / "two.txt"
     two.write_text("1 2 0\n")
     rc, _, err = _cli(["--hx", str(two), "--hz", str(good)])
-    assert rc == 2 and "non-binary token" in err
+    assert rc == 2 and "two.txt: line 1: entry '2' is not 0 or 1" in err
+    glued = tmp_path / "glued.txt"
+    glued.write_text("10 1\n")
+    rc, _, err = _cli(["--hx", str(glued), "--hz", str(good)])
+    assert rc == 2 and "entry '10' is not 0 or 1" in err
+    empty = tmp_path / "empty.txt"
+    empty.write_text("\n \n")
+    rc, _, err = _cli(["--hx", str(empty), "--hz", str(good)])
+    assert rc == 2 and "empty.txt: no rows" in err
+    narrow = tmp_path / "narrow.txt"
+    narrow.write_text("1 1\n")
+    rc, _, err = _cli(["--hx", str(good), "--hz", str(narrow)])
+    assert rc == 2 and "--hx has 3 columns, --hz 2" in err
 
 
 def test_cli_without_device_fails_cleanly(native):
