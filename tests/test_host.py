@@ -5,6 +5,7 @@ from __future__ import annotations
 
 import ctypes
 import hashlib
+import os
 import re
 import subprocess
 import sys
@@ -338,3 +339,39 @@ def test_cli_without_device_fails_cleanly(native):
         pytest.skip("a device is present")
     rc, out, err = _cli([], "XXXXIII\nZZZZIII\n")
     assert rc == 1 and out == "" and "rc=4" in err
+
+
+def test_reference_python_binds_the_drop_in(native):
+    """The reference's unmodified Python package (copied beside its libraries under
+    oracle/_ref) loads this library through QUBITSERF_LIB and binds every distfind_*
+    signature; without a device, backend "gpu" is refused by its own check, "cpu" comes
+    back as rc 5 and "auto" as rc 4, both RuntimeError (python/qubitserf/distfind/
+    _native.py:132-133, api.py:66-72)."""
+    ref_py = ROOT / "oracle" / "_ref" / "python"
+    if not (ref_py / "qubitserf" / "distfind" / "api.py").exists():
+        pytest.skip("the reference Python package was not copied under oracle/_ref")
+    script = (
+        "import sys, json, numpy as np\n"
+        "sys.path.insert(0, sys.argv[1])\n"
+        "from qubitserf import distfind as df\n"
+        "from qubitserf.distfind import _native as N\n"
+        "H = np.array([[1,1,0,1,1,0,0],[1,0,1,1,0,1,0],[0,1,1,1,0,0,1]], np.uint8)\n"
+        "out = {'version': df.version(), 'backends': df.available_backends()}\n"
+        "for b in ('gpu', 'cpu', 'auto'):\n"
+        "    try:\n"
+        "        df.classical_distance(H, backend=b); out[b] = 'ok'\n"
+        "    except RuntimeError as e:\n"
+        "        out[b] = str(e)\n"
+        "print(json.dumps(out))\n")
+    env = dict(os.environ, QUBITSERF_LIB=str(native.LIB_PATH))
+    p = subprocess.run([sys.executable, "-c", script, str(ref_py)], env=env,
+                       capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    out = __import__("json").loads(p.stdout.strip().splitlines()[-1])
+    assert out["version"] == "0.1.0"
+    if native.lib().qsfb_device_sms() == 0:
+        assert out["backends"] == ["cpu"]
+        assert "no GPU backend" in out["gpu"]
+        assert "rc=5" in out["cpu"] and "rc=4" in out["auto"]
+    else:
+        assert "gpu" in out["backends"] and out["gpu"] == "ok" and "rc=5" in out["cpu"]
