@@ -217,6 +217,9 @@ def main():
     ap.add_argument("--ref-full", action="store_true",
                     help="reference arm: certify the whole batch once (a one-off timing; "
                          "minutes of host work)")
+    ap.add_argument("--shard", action="store_true",
+                    help="under torchrun: the ranks split the batch round robin (strong "
+                         "scaling) instead of each certifying its own copy (weak scaling)")
     ap.add_argument("--only-resident", action="store_true",
                     help="time only the resident-input rounds (profiling runs)")
     ap.add_argument("--workload", default="batch",
@@ -244,10 +247,17 @@ def main():
         args.codes = 1
         wname = {"css128": "css_n128_rank40x40_seed1_min", "classical128": "classical_n128_k40_seed2",
                  "classical96": "classical_n96_k32_seed0"}[args.workload]
+    all_codes = codes
+    sharded = args.shard and world > 1
+    if sharded:   # strong scaling: rank r certifies codes r, r + world, ...
+        from qubitserf_b200 import dist as D
+        codes = D.shard(all_codes, rank, world)
+    # certificates of one step over all ranks: every rank's copy, or the batch once
+    units = len(all_codes) if sharded else len(all_codes) * world
     config = {"workload": wname, "codes": args.codes,
-              "classical": sum(c.kind == "classical" for c in codes),
-              "css": sum(c.kind == "css" for c in codes), "n_range": [40, 128],
-              "parallelism": f"replicas{world}",
+              "classical": sum(c.kind == "classical" for c in all_codes),
+              "css": sum(c.kind == "css" for c in all_codes), "n_range": [40, 128],
+              "parallelism": f"shard{world}" if sharded else f"replicas{world}",
               "l2": "256 MiB L2 flush before every timed step",
               "timed": "qsfb_batch_execute rounds (3 interleaved job groups), CUDA-event span "
                        "over all groups (host gaps included)"}
@@ -336,7 +346,7 @@ def main():
     cw, popc_issued, zero_cw = st1.codewords * k, st1.popc_issued * k, st1.zero_codewords * k
     batch.free(handle)
     span_s = max_over_ranks(pg, sum(spans) / 1000.0)
-    value = args.codes * args.steps * world / span_s
+    value = units * args.steps / span_s
     dists = [a.distance for a in ans]
     assert all(a.witness_ok for a in ans), "a witness failed host verification"
     # algorithmic POPC of the full evaluation: per level work x 2W (W = 64-bit words)
@@ -371,7 +381,7 @@ def main():
         e2e_t.append(time.perf_counter() - t)
     assert [a.distance for a in ans2] == dists
     e2e_s = max_over_ranks(pg, sum(e2e_t))
-    e2e = args.codes * args.steps * world / e2e_s
+    e2e = units * args.steps / e2e_s
     host_setup = st2.host_setup_seconds
 
     # --- the plain per-code drop-in path over the same batch (one pass, wall clock)
@@ -379,7 +389,7 @@ def main():
     pdev, pcw, ppopc, plaunch, pd = run_plain(_native, codes)
     plain_s = time.perf_counter() - t
     assert pd == dists, "plain and batched distances differ"
-    plain = args.codes / plain_s
+    plain = len(codes) / plain_s
     popc_per_cw = ppopc / max(pcw, 1)
 
     clocks = clk.summary()
@@ -397,16 +407,27 @@ def main():
     # CUDA-core sweep: the rest of the codewords over the rest of the pair-kernel time
     cc_s = max(pair_s - tc_ms / 1000.0, 1e-12)
     cc_cw_rate = (cw - tc_cw) / cc_s
+    # every code's answer in batch order on rank 0 (shards gathered; one gloo gather)
+    full_dists = dists
+    if sharded:
+        parts = D.gather_to_root(pg, dists, world)
+        full_dists = D.unshard(parts) if rank == 0 else None
     if rank != 0:
         return
-    cpu = None if args.no_cpu_baseline else cpu_baseline_sample(codes)
+    golden_ok = None
+    gold = ROOT / "tests" / "golden" / "batch1024.json"
+    if args.workload == "batch" and args.codes == 1024 and gold.exists():
+        want = [r[0] for r in json.loads(gold.read_text())["codes"]]
+        golden_ok = want == full_dists
+    cpu = None if args.no_cpu_baseline else cpu_baseline_sample(all_codes)
     pref = None if args.no_plain_reference else plain_reference_gpu(codes, ans)
     line = {
         "metric": METRIC, "value": value, "unit": "certs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": span_s / args.steps * 1000.0,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i8",
-        "data": "synthetic", "config": config,
+        "higher_is_better": True, "scaling": "strong" if sharded else "weak",
+        "vs_baseline": None, "dtype": "i8", "data": "synthetic", "config": config,
+        "distances_equal_reference_golden": golden_ok,
         "plain_certs_per_s": plain, "batched_vs_plain": value / plain,
         "plain_reference_gpu": pref,
         "batched_vs_plain_reference": (value / pref["value"]) if pref and "value" in pref
@@ -456,8 +477,8 @@ def main():
                         "merged rounds' device span"},
         "gpu_launches": launches,
         "clocks": clocks,
-        "distance_checksum": int(np.sum(np.array(dists, dtype=np.int64) *
-                                        np.arange(1, len(dists) + 1))),
+        "distance_checksum": int(np.sum(np.array(full_dists, dtype=np.int64) *
+                                        np.arange(1, len(full_dists) + 1))),
     }
     print(json.dumps(line), flush=True)
 

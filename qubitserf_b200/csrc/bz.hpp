@@ -12,6 +12,7 @@
 // the sequential Z-then-X order would have stepped X (capped levels are discarded), which
 // leaves every reported number identical to the sequential schedule.
 #pragma once
+#include <cstdlib>
 #include <functional>
 #include <memory>
 #include <string>
@@ -29,8 +30,9 @@ struct BzOptions {
     int seed_trials = 256;
     bool parallel_seed = true;   // host seed trials on hardware_concurrency threads
     bool device_seed = true;     // eliminations of the seed trials on the GPU when K, n <= 128
-    bool device_infosets = false; // information sets (and the packed rows) built on the GPU
-                                 // when K, n <= 128
+    // information sets (and the packed rows) built on the GPU when K, n <= 128;
+    // QSFB_HOST_INFOSETS=1 builds them on the host instead (same results)
+    bool device_infosets = std::getenv("QSFB_HOST_INFOSETS") == nullptr;
 };
 
 // One enumerated level, for the per-(information set, w) count record.

@@ -54,3 +54,21 @@ def barrier(pg):
 def shard(items, rank: int, world: int):
     """Round-robin share of `items` for strong scaling (heavy codes spread over ranks)."""
     return items[rank::world]
+
+
+def unshard(parts):
+    """Inverse of shard(): parts[r] is rank r's share; returns the items in their order."""
+    world = len(parts)
+    out = [None] * sum(len(p) for p in parts)
+    for r, part in enumerate(parts):
+        out[r::world] = part
+    return out
+
+
+def gather_to_root(pg, obj, world: int):
+    """Every rank's `obj`, in rank order, on rank 0 (None elsewhere); one gloo gather."""
+    if pg is None:
+        return [obj]
+    out = [None] * world if pg.get_rank() == 0 else None
+    pg.gather_object(obj, out, dst=0)
+    return out

@@ -26,7 +26,9 @@ def _worker(rank, world, port, q):
     s = dist.sum_over_ranks(pg, 1.0)
     dist.barrier(pg)
     mine = dist.shard(list(range(37)), r, w)
-    q.put((rank, m, s, mine))
+    parts = dist.gather_to_root(pg, [10 * i for i in mine], w)
+    whole = dist.unshard(parts) if r == 0 else None
+    q.put((rank, m, s, mine, whole))
     pg.destroy_process_group()
 
 
@@ -46,6 +48,8 @@ def test_two_gloo_ranks():
     assert [o[2] for o in out] == [2.0, 2.0]
     covered = sorted(out[0][3] + out[1][3])
     assert covered == list(range(37))
+    # rank 0 rebuilds every code's answer in batch order from the two shards
+    assert out[0][4] == [10 * i for i in range(37)] and out[1][4] is None
 
 
 def test_single_process_defaults(monkeypatch):
