@@ -142,9 +142,9 @@ int qsfb_prepare_problem(int kind, const uint8_t* A, int ar, int ac, const uint8
  * reference counterpart; it exposes the device construction that replaces the reference's
  * host eliminations, cpp/distfind/css.cpp:177-203, 336-366 and cpp/qsf/gf2.cpp:42-58).
  * on_device = 1: the GPU kernel (one warp per subproblem, K and n <= 128; larger ones and
- * more than 8 sets are built on the host); 0: the host construction.  meta holds 11 ints:
- * qsfb_prepare_problem's 8, then W32 = ceil(n/32), SWP = max(1, ceil(kcheck/32)) and 1 when
- * the device built the sets.  red (num_gamma*K*W32 u32, when not NULL): each set's rows over
+ * more than 16 sets are built on the host); 0: the host construction.  meta holds 12 ints:
+ * qsfb_prepare_problem's 8, then W32 = ceil(n/32), SWP = max(1, ceil(kcheck/32)), 1 when
+ * the device built the sets, and 1 when it built them from matroid-partition classes.  red (num_gamma*K*W32 u32, when not NULL): each set's rows over
  * its non-pivot columns in ascending order, zero padded; syn (num_gamma*K*SWP u32): bit c of
  * row r = parity(check_c & row r) -- the two tables the pair sweeps read.
  * Returns 0, 1 (null), 2 (shape), 4 (device), 7 (buffer small). */

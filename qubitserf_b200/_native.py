@@ -354,7 +354,7 @@ def prepare_sides(kind, A, B=None, on_device=True):
     the packed non-pivot rows and detector syndromes the pair sweeps read."""
     a = as_u8(A)
     b = as_u8(B) if B is not None else np.zeros((0, a.shape[1]), np.uint8)
-    meta = (ctypes.c_int * 11)()
+    meta = (ctypes.c_int * 12)()
     ncol = a.shape[1] * 3 // 2 if kind == 5 else a.shape[1]
     stride = (ncol + 63) // 64
     w32 = (ncol + 31) // 32
@@ -372,14 +372,14 @@ def prepare_sides(kind, A, B=None, on_device=True):
                                   red.ctypes.data_as(_u32p), red.size,
                                   syn.ctypes.data_as(_u32p), syn.size)
     _check(rc, "qsfb_prepare_sides")
-    n, K, ng, kcheck, even, count_all, seed_upper, stride, W32, SWP, on_dev = list(meta)
+    n, K, ng, kcheck, even, count_all, seed_upper, stride, W32, SWP, on_dev, classes = list(meta)
     return {"n": n, "K": K, "stride": stride, "ranks": [ranks[i] for i in range(ng)],
             "gamma": gamma[: ng * K * stride].reshape(ng, K, stride).copy(),
             "check": check[: kcheck * stride].reshape(kcheck, stride).copy(),
             "red": red[: ng * K * W32].reshape(ng, K, W32).copy(),
             "syn": syn[: ng * K * SWP].reshape(ng, K, SWP).copy(),
             "even": bool(even), "count_all": bool(count_all), "seed_upper": seed_upper,
-            "device": bool(on_dev)}
+            "device": bool(on_dev), "classes": bool(classes)}
 
 
 def last_report() -> QsfbReport:

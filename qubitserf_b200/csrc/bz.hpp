@@ -106,6 +106,7 @@ public:
     void apply_device_seed(unsigned key);
     // information sets pending on the GPU (setup_jobs_device builds them and the packed rows)
     bool infoset_pending = false;
+    bool sets_from_classes = false;   // built on the device from matroid-partition classes
     // Take the sets built on the device (or, with red == nullptr, build the rows on the host
     // for upload): fills ng, ranks and the device image.
     int adopt_sets(std::vector<InfoSet>&& s, uint32_t* red, uint32_t* syn, int W32, int SWP,

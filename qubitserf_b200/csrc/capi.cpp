@@ -718,6 +718,7 @@ int qsfb_prepare_sides(int kind, const uint8_t* A, int ar, int ac, const uint8_t
     meta[8] = W32;
     meta[9] = SWP;
     meta[10] = 0;
+    meta[11] = 0;
     if (K == 0) return write_sets(p, {}, meta, ranks, max_gamma, gamma, max_words, check, max_check);
     BzSide S;   // only its information sets and device image are used
     S.prob = &p;
@@ -735,6 +736,7 @@ int qsfb_prepare_sides(int kind, const uint8_t* A, int ar, int ac, const uint8_t
         rc = device_infosets(lease->s, arena.get(), {&S}, nullptr);
         if (rc != kOk) return rc;
         meta[10] = S.dev.device_rows ? 1 : 0;
+        meta[11] = S.sets_from_classes ? 1 : 0;
     } else {
         rc = S.adopt_sets(information_sets(p.code_gen), nullptr, nullptr, 0, 0, nullptr, nullptr);
         if (rc != kOk) return rc;

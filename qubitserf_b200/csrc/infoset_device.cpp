@@ -11,8 +11,11 @@
 // kInfosetMaxSets sets) is built on the host instead and uploaded with the others.
 #include <algorithm>
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
+#include <vector>
 
 #include "bz.hpp"
 #include "infoset_types.hpp"
@@ -74,7 +77,10 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
     if (cap >= (1ull << 31)) return kErrUnsupported;   // heap offsets are 32-bit
     char* d = (char*)arena->alloc(off);
     if (!d) return kErrMemory;
-    int rc = s->ensure(0, off);
+    // pinned staging for what crosses before the kernels and the meta read-back only: the
+    // heap comes back into pageable memory, so the staging does not grow with it (growing
+    // pinned memory costs tens of ms and synchronises the device)
+    int rc = s->ensure(0, staged);
     if (rc != kOk) return rc;
     char* h = (char*)s->h_stage.h;
     InfosetDesc* hd = (InfosetDesc*)(h + off_desc);
@@ -129,13 +135,14 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
     }
     const unsigned long long used = *(const unsigned long long*)(h + off_ctr);
     if (used > cap) return kErrDevice;
-    if (used > 0 &&
-        (cudaMemcpyAsync(h + off_heap, d_heap, used * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-         cudaStreamSynchronize(st) != cudaSuccess)) {
+    thread_local std::vector<u64> heap_host;
+    if (heap_host.size() < used) heap_host.resize(used);
+    if (used > 0 && cudaMemcpy(heap_host.data(), d_heap, used * 8, cudaMemcpyDeviceToHost) !=
+                        cudaSuccess) {
         cudaGetLastError();
         return kErrDevice;
     }
-    const u64* heap = (const u64*)(h + off_heap);
+    const u64* heap = heap_host.data();
     for (size_t i = 0; i < n; ++i) {
         Item& it = *items[i];
         const InfosetMeta& M = *((const InfosetMeta*)(h + off_meta) + i);
@@ -173,6 +180,7 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
 int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
                     RunStats* stats) {
     if (sides.empty()) return kOk;
+    static const bool trace = std::getenv("QSFB_BATCH_TRACE") != nullptr;
     const double t0 = now_seconds();
     std::vector<Item> items(sides.size());
     size_t rows_bytes = 0;
@@ -202,6 +210,7 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
     for (Item& it : items) pass.push_back(&it);
     int rc = run_pass(s, arena, pass, false);
     if (rc != kOk) return rc;
+    const double t1 = now_seconds();
 
     // the matroid-partition step, on the host, for the sides whose greedy peel may be beaten
     std::vector<Item*> cand;
@@ -233,17 +242,29 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
     pass.clear();
     for (Item* it : cand)
         if (it->state == kClasses) pass.push_back(it);
+    const double t2 = now_seconds();
+    const size_t nclasses = pass.size();
     rc = run_pass(s, arena, pass, true);
     if (rc != kOk) return rc;
+    const double t3 = now_seconds();
+    int nhost = 0;
 
     for (Item& it : items) {
         BzSide& S = *it.side;
+        nhost += it.state != kDone;
+        S.sets_from_classes = it.state == kDone && !it.lists.empty();
         rc = it.state == kDone
                  ? S.adopt_sets(std::move(it.sets), it.red, it.syn, it.W32, it.SWP, s->dev, arena)
                  : S.adopt_sets(information_sets(it.p->code_gen), nullptr, nullptr, 0, 0, s->dev,
                                 arena);
         if (rc != kOk) return rc;
     }
+    if (trace)
+        std::fprintf(stderr, "qsfb device sets: %zu sides: greedy pass %.2f ms, partition "
+                     "search %.2f ms (%zu candidates, %zu replaced), class pass %.2f ms, "
+                     "adopt %.2f ms (%d built on the host)\n", items.size(), 1e3 * (t1 - t0),
+                     1e3 * (t2 - t1), cand.size(), nclasses, 1e3 * (t3 - t2),
+                     1e3 * (now_seconds() - t3), nhost);
     if (stats) {
         stats->device_sets_s += now_seconds() - t0;
         stats->launches += 2;

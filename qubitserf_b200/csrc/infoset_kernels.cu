@@ -140,18 +140,23 @@ __device__ __forceinline__ void emit_set(const InfosetDesc& D, const Rows<W, S>&
             if (row < K) red[(size_t)row * D.W32 + ow] = acc[s];
         }
     }
-    // detector syndromes, 32 checks per output word
+    // detector syndromes, 32 checks per output word; the 32 check rows of a word are loaded
+    // by the 32 lanes (one each) and broadcast by shuffle, so no lane waits on a chain of
+    // dependent global loads
     uint32_t* syn = D.syn + (size_t)g * K * D.SWP;
     for (int ow = 0; ow < D.SWP; ++ow) {
         uint32_t acc[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) acc[s] = 0u;
-        for (int j = 0; j < 32; ++j) {
-            const int c = 32 * ow + j;
-            if (c >= D.kcheck) break;
+        const int cl = 32 * ow + lane;
+        unsigned long long mine[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) mine[w] = cl < D.kcheck ? __ldg(D.check + (size_t)cl * W + w) : 0ull;
+        const int nc = min(32, D.kcheck - 32 * ow);
+        for (int j = 0; j < nc; ++j) {
             unsigned long long ck[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) ck[w] = __ldg(D.check + (size_t)c * W + w);
+            for (int w = 0; w < W; ++w) ck[w] = __shfl_sync(0xffffffffu, mine[w], j);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 int p = 0;

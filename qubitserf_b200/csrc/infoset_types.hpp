@@ -6,17 +6,17 @@ namespace qsfb {
 
 constexpr int kInfosetMaxK = 128;    // rows held in registers (4 slots x 32 lanes)
 constexpr int kInfosetMaxN = 128;    // columns (two 64-bit words per row)
-constexpr int kInfosetMaxSets = 8;   // sets per side on the device; more -> host construction
+constexpr int kInfosetMaxSets = 16;  // sets per side on the device; more -> host construction
 
-// Per-side results the host reads back (one 256-byte block per side).
+// Per-side results the host reads back (one 512-byte block per side).
 struct InfosetMeta {
     int sets;                                     // number of sets; -1: more than kInfosetMaxSets
     int rank[kInfosetMaxSets];                    // pivots of each set
     int g_off[kInfosetMaxSets];                   // each set's generator: offset (u64 words) in the heap
-    int pad_[15];
+    int pad_[31];
     unsigned long long piv[kInfosetMaxSets][2];   // pivot columns of each set (bit mask)
 };
-static_assert(sizeof(InfosetMeta) == 256, "meta block");
+static_assert(sizeof(InfosetMeta) == 512, "meta block");
 
 struct InfosetDesc {
     const unsigned long long* gen;    // K x W rows of the code generator

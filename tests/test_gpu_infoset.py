@@ -52,7 +52,7 @@ def test_matroid_partition_classes_on_device(native, ref):
     partition: the classes go to the device as explicit column lists."""
     from qubitserf_b200.workloads import classical_parity_from_rng
     rng = np.random.default_rng(11)
-    differ = 0
+    classes = 0
     for _ in range(80):
         n = int(rng.integers(20, 100))
         k = int(rng.integers(n // 4, n // 2 + 1))
@@ -65,8 +65,8 @@ def test_matroid_partition_classes_on_device(native, ref):
         if ref is not None:
             r = ref.problem_gammas(0, H)
             assert d["ranks"] == r["ranks"] and np.array_equal(d["gamma"], r["gamma"])
-        differ += d["ranks"].count(d["K"]) > 1
-    assert differ > 10
+        classes += d["classes"]   # the partition beat the greedy peel: built from class lists
+    assert classes > 10
 
 
 def test_golden_infosets_device_equals_host(native, golden, ref):
