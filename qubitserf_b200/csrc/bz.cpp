@@ -377,6 +377,7 @@ void BzJob::finish_setup() {
 }
 
 void BzJob::reset() {
+    final_.reset();
     if (zero) return;
     for (int i = 0; i < (pair ? 2 : 1); ++i) s[i].reset();
     w_ = 0;
@@ -486,7 +487,14 @@ void finish_witness(const BzSide& S, const Problem& p, BzResult& r, int side_idx
 }
 }  // namespace
 
-BzResult BzJob::result() {
+BzResult BzJob::result() { return final_result(); }
+
+const BzResult& BzJob::final_result() {
+    if (!final_) final_.reset(new BzResult(compute_result()));
+    return *final_;
+}
+
+BzResult BzJob::compute_result() {
     BzResult r;
     r.stats = stats;
     r.trace = trace;
@@ -704,6 +712,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
         // per-job slices (requests of one job are contiguous)
         const double ta0 = now_seconds();
         size_t k = 0;
+        std::vector<BzJob*> finished;
         for (size_t j = 0; j < jobs.size(); ++j) {
             if (jobs[j]->done()) continue;
             std::vector<const LevelOut*> o;
@@ -717,6 +726,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             }
             jobs[j]->stats.codewords += cw;
             jobs[j]->apply(o, sd);
+            if (jobs[j]->done()) finished.push_back(jobs[j]);
         }
         rs.host_apply_s += now_seconds() - ta0;
         if (stats) {
@@ -739,6 +749,9 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             jobs[0]->stats.launches += rs.launches;
             jobs[0]->stats.jobs += rs.jobs;
         }
+        // answers of the jobs this round finished (their witnesses rebuilt and verified)
+        // while the device runs the other job groups' kernels
+        for (BzJob* j : finished) j->final_result();
     }
     if (span_ms) {
         cudaEventRecord(e1, s->stream);

@@ -137,6 +137,10 @@ public:
     bool done() const { return done_; }
     void reset();                           // back to the post-setup state
     BzResult result();                      // final numbers + verified witness
+    // The result of a finished job, computed once (witness rebuilt and verified) and kept:
+    // the rounds call it as soon as a job is done, so that the answers of a batch are
+    // ready when its last round ends.
+    const BzResult& final_result();
 
     bool pair = false;
     Problem p[2];
@@ -146,6 +150,8 @@ public:
     std::vector<LevelRecord> trace;
 
 private:
+    BzResult compute_result();
+    std::unique_ptr<BzResult> final_;
     Builder build_;
     int w_ = 0;                // last stepped level
     int maxw_ = 0;

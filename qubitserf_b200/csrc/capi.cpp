@@ -216,6 +216,36 @@ struct QsfbBatchHandle {
 
 namespace {
 
+// Background deletion of finished batch handles whose device memory and session have
+// already been returned (only host memory is left).  One thread, started on first use and
+// never joined; its queue and lock are never destroyed, so exit cannot race them.
+void reap_later(QsfbBatchHandle* h) {
+    struct Reaper {
+        std::mutex mu;
+        std::condition_variable cv;
+        std::vector<QsfbBatchHandle*> q;
+        Reaper() {
+            std::thread([this]() {
+                for (;;) {
+                    std::vector<QsfbBatchHandle*> take;
+                    {
+                        std::unique_lock<std::mutex> lk(mu);
+                        cv.wait(lk, [this]() { return !q.empty(); });
+                        take.swap(q);
+                    }
+                    for (QsfbBatchHandle* x : take) delete x;
+                }
+            }).detach();
+        }
+    };
+    static Reaper* r = new Reaper();
+    {
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->q.push_back(h);
+    }
+    r->cv.notify_one();
+}
+
 // Chunks of a one-shot batch prepared while the first chunk's rounds run: a helper thread
 // publishes each prepared handle in order (nullptr if its preparation failed), and every
 // job group takes its round-robin share of each published chunk at its next round boundary,
@@ -339,8 +369,10 @@ int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_m
 // Witness rebuild, host verification and the per-query answers of an executed handle.
 // Results (witness rebuild + host verification) of every job of the handles, independent
 // per job: one pool over the host cores for all of them.
-std::vector<std::vector<BzResult>> results_of(const std::vector<QsfbBatchHandle*>& Hs) {
-    std::vector<std::vector<BzResult>> res(Hs.size());
+// Each job's final result (kept by the job; the rounds compute most of them as jobs
+// finish, the rest -- trivially zero operator weights, say -- are computed here in parallel).
+std::vector<std::vector<const BzResult*>> results_of(const std::vector<QsfbBatchHandle*>& Hs) {
+    std::vector<std::vector<const BzResult*>> res(Hs.size());
     std::vector<std::pair<size_t, size_t>> work;
     for (size_t h = 0; h < Hs.size(); ++h) {
         res[h].resize(Hs[h]->jobs.size());
@@ -349,7 +381,8 @@ std::vector<std::vector<BzResult>> results_of(const std::vector<QsfbBatchHandle*
     std::atomic<size_t> next{0};
     auto worker = [&]() {
         for (size_t w; (w = next.fetch_add(1)) < work.size();)
-            res[work[w].first][work[w].second] = Hs[work[w].first]->jobs[work[w].second]->result();
+            res[work[w].first][work[w].second] =
+                &Hs[work[w].first]->jobs[work[w].second]->final_result();
     };
     const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(),
                                               (int)work.size() / 8 + 1));
@@ -361,25 +394,32 @@ std::vector<std::vector<BzResult>> results_of(const std::vector<QsfbBatchHandle*
 }
 
 // The per-query answers of an executed handle from its jobs' results.
-void answers_of(QsfbBatchHandle* H, const std::vector<BzResult>& res, QsfbAnswer* out) {
+void answers_of(QsfbBatchHandle* H, const std::vector<const BzResult*>& res, QsfbAnswer* out) {
     for (size_t i = 0; i < H->map.size(); ++i) {
         QsfbAnswer& a = out[i];
         std::memset(&a, 0, sizeof(a));
         const auto& m = H->map[i];
         if (H->kinds[i] == 2) {
-            BzResult rz, rx;
-            int zw = m.zw, xw = m.xw;
+            int zw = m.zw, xw = m.xw, lz = 0, lx = 0;
             bool ok = true, proven = true;
-            if (m.job0 >= 0) { rz = res[m.job0]; zw = rz.distance; ok &= rz.witness_ok || zw <= 0; proven &= rz.proven; }
-            if (m.job1 >= 0) { rx = res[m.job1]; xw = rx.distance; ok &= rx.witness_ok || xw <= 0; proven &= rx.proven; }
+            if (m.job0 >= 0) {
+                const BzResult& rz = *res[m.job0];
+                zw = rz.distance; lz = rz.levels;
+                ok &= rz.witness_ok || zw <= 0; proven &= rz.proven;
+            }
+            if (m.job1 >= 0) {
+                const BzResult& rx = *res[m.job1];
+                xw = rx.distance; lx = rx.levels;
+                ok &= rx.witness_ok || xw <= 0; proven &= rx.proven;
+            }
             a.z_weight = zw;
             a.x_weight = xw;
             a.distance = std::max(zw, xw);
             a.proven = proven ? 1 : 0;
             a.witness_ok = ok ? 1 : 0;
-            a.levels = std::max(m.job0 >= 0 ? rz.levels : 0, m.job1 >= 0 ? rx.levels : 0);
+            a.levels = std::max(lz, lx);
         } else {
-            const BzResult& r = res[m.job0];
+            const BzResult& r = *res[m.job0];
             a.distance = r.distance;
             a.lower_bound = r.lower_bound;
             a.proven = r.proven ? 1 : 0;
@@ -954,13 +994,16 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     };
     // the chunks' handles are torn down in parallel (jobs' host state, device lists back to
     // the allocator's cache, sessions back to the pool)
+    // the chunks' device memory and sessions go back at once; the host-side teardown of
+    // their jobs (many small frees) runs on a background thread after the call returns
     auto release = [&]() {
-        std::vector<std::thread> th;
-        for (size_t c = 1; c < H.size(); ++c)
-            if (H[c]) th.emplace_back(qsfb_batch_free, H[c]);
-        qsfb_batch_free(H[0]);
-        for (auto& t : th) t.join();
-        for (QsfbBatchHandle*& h : H) h = nullptr;
+        for (QsfbBatchHandle*& h : H) {
+            if (!h) continue;
+            h->arena.reset();
+            h->lease.reset();
+            reap_later(h);
+            h = nullptr;
+        }
     };
     if (nchunks == 1) {
         prepare(0);
@@ -1004,7 +1047,7 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     for (int c = 0; c < nchunks && rc == kOk; ++c)
         if (prc[c] != kOk) rc = prc[c];
     if (rc == kOk && out) {
-        const std::vector<std::vector<BzResult>> res = results_of(H);
+        const std::vector<std::vector<const BzResult*>> res = results_of(H);
         for (int c = 0; c < nchunks; ++c) answers_of(H[c], res[c], out + cut[c]);
     }
     const double ta1 = now_seconds();

@@ -250,7 +250,7 @@ __device__ void side_sets(const InfosetDesc& D, int lane, unsigned long long* __
 }
 
 template <int W>
-__global__ void __launch_bounds__(128) infoset_kernel(const InfosetDesc* __restrict__ descs,
+__global__ void __launch_bounds__(32) infoset_kernel(const InfosetDesc* __restrict__ descs,
                                                       int ndesc,
                                                       unsigned long long* __restrict__ heap,
                                                       unsigned long long* __restrict__ heap_ctr) {
@@ -273,10 +273,11 @@ cudaError_t launch_infosets(int W, const InfosetDesc* d_descs, int ndesc,
                             unsigned long long* d_heap, unsigned long long* d_heap_ctr,
                             cudaStream_t st) {
     if (ndesc <= 0) return cudaSuccess;
-    const int warps_per_block = 4;
-    const int blocks = (ndesc + warps_per_block - 1) / warps_per_block;
-    if (W == 1) dev::infoset_kernel<1><<<blocks, 128, 0, st>>>(d_descs, ndesc, d_heap, d_heap_ctr);
-    else if (W == 2) dev::infoset_kernel<2><<<blocks, 128, 0, st>>>(d_descs, ndesc, d_heap, d_heap_ctr);
+    // one warp per block: it fits in the registers a running tensor-core sweep CTA leaves
+    // free on its SM, so it does not wait for the sweep's launch to end
+    const int blocks = ndesc;
+    if (W == 1) dev::infoset_kernel<1><<<blocks, 32, 0, st>>>(d_descs, ndesc, d_heap, d_heap_ctr);
+    else if (W == 2) dev::infoset_kernel<2><<<blocks, 32, 0, st>>>(d_descs, ndesc, d_heap, d_heap_ctr);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }

@@ -135,7 +135,7 @@ __device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
 }
 
 template <int W>
-__global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __restrict__ descs,
+__global__ void __launch_bounds__(64) seed_trials_kernel(const SeedDesc* __restrict__ descs,
                                                           int ndesc, int total_trials) {
     const int lane = threadIdx.x & 31;
     const int gt = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -161,10 +161,13 @@ __global__ void __launch_bounds__(128) seed_trials_kernel(const SeedDesc* __rest
 cudaError_t launch_seed_trials(int W, const SeedDesc* d_descs, int ndesc, int total_trials,
                                cudaStream_t st) {
     if (total_trials <= 0) return cudaSuccess;
-    const int warps_per_block = 4;
+    // Blocks of two warps (64 x <= 48 registers): they fit in the registers a running
+    // tensor-core sweep CTA leaves free on its SM (640 threads x 96), so a preparation that
+    // overlaps the rounds starts at once instead of queueing behind the sweep's launch.
+    const int warps_per_block = 2;
     const int blocks = (total_trials + warps_per_block - 1) / warps_per_block;
-    if (W == 1) dev::seed_trials_kernel<1><<<blocks, 128, 0, st>>>(d_descs, ndesc, total_trials);
-    else if (W == 2) dev::seed_trials_kernel<2><<<blocks, 128, 0, st>>>(d_descs, ndesc, total_trials);
+    if (W == 1) dev::seed_trials_kernel<1><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);
+    else if (W == 2) dev::seed_trials_kernel<2><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
