@@ -17,6 +17,7 @@
 #include <random>
 #include <thread>
 #include <cstring>
+#include <condition_variable>
 
 #include <nvtx3/nvToolsExt.h>
 
@@ -672,9 +673,57 @@ int setup_jobs(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
 }
 
 
+namespace {
+// Computes the final results (witness rebuilt and verified on the host) of the jobs a round
+// finished, on a thread of its own, so that the round loop goes straight on to launching
+// the next round.  The results are all in when the finisher is destroyed.
+class Finisher {
+public:
+    Finisher() : th_([this]() { loop(); }) {}
+    ~Finisher() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_one();
+        th_.join();
+    }
+    void push(const std::vector<BzJob*>& v) {
+        if (v.empty()) return;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.insert(q_.end(), v.begin(), v.end());
+        }
+        cv_.notify_one();
+    }
+
+private:
+    void loop() {
+        for (;;) {
+            std::vector<BzJob*> take;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this]() { return stop_ || !q_.empty(); });
+                take.swap(q_);
+                if (take.empty() && stop_) return;
+            }
+            for (BzJob* j : take) j->final_result();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::vector<BzJob*> q_;
+    bool stop_ = false;
+    std::thread th_;
+};
+}  // namespace
+
 int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* rounds,
                double* span_ms, const JobFeed* feed) {
     int nround = 0;
+    // a batch's answers are computed beside its rounds (a single job's by its caller)
+    std::unique_ptr<Finisher> finisher;
+    if (jobs.size() > 1 || feed) finisher.reset(new Finisher());
     std::vector<LevelReq> q;
     std::vector<int> side, owner;
     std::vector<LevelOut> outs;
@@ -749,9 +798,9 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             jobs[0]->stats.launches += rs.launches;
             jobs[0]->stats.jobs += rs.jobs;
         }
-        // answers of the jobs this round finished (their witnesses rebuilt and verified)
-        // while the device runs the other job groups' kernels
-        for (BzJob* j : finished) j->final_result();
+        // answers of the jobs this round finished (witnesses rebuilt and verified) are
+        // computed on the finisher's thread while the next rounds run
+        if (finisher) finisher->push(finished);
     }
     if (span_ms) {
         cudaEventRecord(e1, s->stream);

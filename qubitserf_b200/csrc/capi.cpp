@@ -27,8 +27,8 @@ using namespace qsfb;
 namespace qsfb {
 cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int packed,
                                int32_t* out, int* err, cudaStream_t st);
-int tc_tile_rows();
-int tc_tile_cols();
+int tc_selftest_rows();
+int tc_selftest_cols();
 cudaError_t microbench_peak(int which, int num_sms, uint32_t* d_out, cudaStream_t st,
                             double* ops_per_s);
 }
@@ -1111,7 +1111,7 @@ int qsfb_tc_selftest(int ksteps, int packed, const int8_t* A, const int8_t* B, i
     if (!dev) return rc;
     SessionLease lease(dev);
     if (!lease.s) return kErrDevice;
-    const int rows_a = tc_tile_rows(), rows_b = tc_tile_cols();
+    const int rows_a = tc_selftest_rows(), rows_b = tc_selftest_cols();
     const size_t bytes_a = (size_t)rows_a * kPmRowBytes, bytes_b = (size_t)rows_b * kPmRowBytes;
     const size_t bytes_d = (size_t)rows_a * rows_b * 4;
     // host swizzle: 16-byte chunk j of row e goes to chunk j ^ ((e >> 1) & 3)

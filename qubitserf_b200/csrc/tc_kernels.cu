@@ -35,6 +35,7 @@
 // gave up) and the CTA winds down without touching the device further.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstdlib>
 
 #include "engine_types.hpp"
 #include "enum_device.cuh"
@@ -69,6 +70,31 @@ static_assert(kPmRowBytes == 64, "operand rows are 64 bytes (64 int8 columns)");
 // both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
 constexpr uint32_t kTcIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
                               ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+
+// A sweep shape: ROWS prefix rows per job (ROWS / 128 MMA row blocks) against suffix tiles of
+// N rows, the MMA's N.  Both shapes fill the same two 256-column accumulator buffers, and
+// each buffer is read back by eight warps (two per TMEM lane quarter: the two prefix halves
+// of a 256 x 128 tile, or the two 128-column halves of a 128 x 256 one).  The wide shape
+// issues half as many MMAs for the same pairs: each tcgen05.mma occupies its issuing thread
+// ~80-130 cycles, four of them plus the commit were a third of a buffer's round trip.
+template <int ROWS, int N>
+struct TcShape {
+    static constexpr int kRows = ROWS, kN = N;
+    static constexpr int kHalves = ROWS / kTcM;           // MMA row blocks per prefix tile
+    static constexpr int kChunks = N / 128;               // 128-column read-back chunks per half
+    static constexpr uint32_t kABytes = ROWS * kPmRowBytes;
+    static constexpr uint32_t kBBytes = N * kPmRowBytes;
+    static constexpr uint32_t kOffB = 2 * kABytes;        // after the two prefix slots
+    static constexpr uint32_t kOffBar = kOffB + kTcBStages * kBBytes;
+    static constexpr uint32_t kSmem = kOffBar + 512 + 1024;   // + barriers, TMEM slot, alignment
+    static constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                                       ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+    static_assert(kHalves * N == 256, "a buffer is 256 accumulator columns");
+    static_assert(kHalves * kChunks == 2, "two read-back warps per lane quarter and buffer");
+    static_assert(kSmem <= 227 * 1024, "shared memory");
+};
+using TcHalvesShape = TcShape<256, 128>;
+using TcWideShape = TcShape<128, 256>;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -140,12 +166,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 }
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t accumulate) {
+                                       uint32_t accumulate, uint32_t idesc = kTcIdesc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -298,6 +324,7 @@ struct TcJobRec {
 };
 static_assert(sizeof(TcJobRec) == 64, "job record layout");
 
+template <class SH>
 __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restrict__ descs,
                                                       int ndesc, unsigned long long total,
                                                       const unsigned long long* __restrict__ B,
@@ -322,14 +349,14 @@ __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restric
         const unsigned long long nx = binom(B, p, D.a - 1);
         const unsigned long long ny = binom(B, D.K - 1 - p, D.b);
         const unsigned long long xoff = binom(B, p, D.a);
-        const unsigned long long nbt = (ny + kTcN - 1) / kTcN;
+        const unsigned long long nbt = (ny + SH::kN - 1) / SH::kN;
         const unsigned long long nbc = (nbt + kTcJB - 1) / kTcJB;
         const unsigned long long ia = idx / nbc, jc = idx - ia * nbc;
         TcJobRec R;
         R.xpm = D.xpm;
         R.ypm = D.ypm;
         R.key = D.key;
-        R.r0 = (unsigned int)((xoff & ~7ull) + ia * kTcRows);
+        R.r0 = (unsigned int)((xoff & ~7ull) + ia * SH::kRows);
         R.xoff = (unsigned int)xoff;
         R.nx = (unsigned int)nx;
         R.ny = (unsigned int)ny;
@@ -364,6 +391,7 @@ __device__ __forceinline__ TcJobRec tc_rec(const TcJobRec* __restrict__ recs,
     return R;
 }
 
+template <class SH>
 __global__ void __launch_bounds__(kTcThreads, 1)
 pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict__ recs,
                 unsigned long long total_jobs, const unsigned long long* __restrict__ B,
@@ -372,7 +400,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     // 1024-byte alignment of the operand tiles (covers the 512-byte swizzle atom)
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t s0 = smem_u32(smem);
-    const uint32_t bar = s0 + kTcOffBar;
+    const uint32_t bar = s0 + SH::kOffBar;
     // barrier slots (8 bytes each): a_full 0-1, a_empty 2-3, b_full 4-11, tile_done 12-19,
     // acc_empty 20-21.  One MMA commit per suffix tile signals both that its stage may be
     // refilled and that its accumulator is ready: the copier and the read-back warps wait
@@ -388,7 +416,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
     counts[2] = counts[3] = 2;   // a prefix slot is released by both MMA threads
     // one arrival per read-back warp of the buffer's group
     counts[4 + 2 * kTcBStages] = counts[5 + 2 * kTcBStages] = kTcEpiWarps / kTcEpiGroups;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcOffBar + 256);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + SH::kOffBar + 256);
     const uint32_t tmem = tc_setup(bar, kNBar, counts, tmem_slot);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -414,18 +442,18 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 const uint32_t sa = it_a & 1u;
                 if (par == 0) {
                     if (!(ok = mbar_wait(a_empty(sa), ((it_a >> 1) & 1u) ^ 1u))) break;
-                    mbar_expect_tx(a_full(sa), kTcABytes);
-                    bulk_g2s(s0 + kTcOffA + sa * kTcABytes, R.xpm + R.r0 * kPmRowBytes, kTcABytes,
-                             a_full(sa));
+                    mbar_expect_tx(a_full(sa), SH::kABytes);
+                    bulk_g2s(s0 + kTcOffA + sa * SH::kABytes, R.xpm + R.r0 * kPmRowBytes,
+                             SH::kABytes, a_full(sa));
                 }
                 ++it_a;
                 for (unsigned long long bt = R.b0; bt < R.b1; ++bt, ++it_b) {
                     if ((it_b & 1u) != par) continue;
                     const uint32_t sb = it_b % kTcBStages;
                     if (!(ok = mbar_wait(tile_done(sb), ((it_b / kTcBStages) & 1u) ^ 1u))) break;
-                    mbar_expect_tx(b_full(sb), kTcBBytes);
-                    bulk_g2s(s0 + kTcOffB + sb * kTcBBytes, ypm + bt * kTcN * kPmRowBytes,
-                             kTcBBytes, b_full(sb));
+                    mbar_expect_tx(b_full(sb), SH::kBBytes);
+                    bulk_g2s(s0 + SH::kOffB + sb * SH::kBBytes, ypm + bt * SH::kN * kPmRowBytes,
+                             SH::kBBytes, b_full(sb));
                 }
                 R = N;
             }
@@ -446,21 +474,21 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 // two arrivals of every release phase from different jobs apart)
                 if (!(ok = mbar_wait(a_full(sa), (it_a >> 1) & 1u))) break;
                 tc_fence_after();
-                const uint32_t a_addr = s0 + kTcOffA + sa * kTcABytes;
+                const uint32_t a_addr = s0 + kTcOffA + sa * SH::kABytes;
                 for (unsigned int bt = tb0; bt < tb1; ++bt, ++it_b) {
                     if ((it_b & 1u) != par) continue;
                     const uint32_t sb = it_b % kTcBStages, ac = par;   // buffer = tile parity
                     if (!(ok = mbar_wait(b_full(sb), (it_b / kTcBStages) & 1u))) break;
                     if (!(ok = mbar_wait(acc_empty(ac), ((it_b >> 1) & 1u) ^ 1u))) break;
                     tc_fence_after();
-                    const uint32_t b_addr = s0 + kTcOffB + sb * kTcBBytes;
+                    const uint32_t b_addr = s0 + SH::kOffB + sb * SH::kBBytes;
 #pragma unroll
-                    for (int h = 0; h < kTcHalves; ++h)
+                    for (int h = 0; h < SH::kHalves; ++h)
 #pragma unroll
                         for (int k = 0; k < kTcK; ++k)   // K = 32 int8 columns = 32 bytes
-                            mma_i8(tmem + (ac * kTcHalves + h) * kTcN,
+                            mma_i8(tmem + ac * 256u + h * SH::kN,
                                    smem_desc(a_addr + h * kTcHalfBytes + 32u * k),
-                                   smem_desc(b_addr + 32u * k), k > 0 ? 1u : 0u);
+                                   smem_desc(b_addr + 32u * k), k > 0 ? 1u : 0u, SH::kIdesc);
                     mma_commit(tile_done(sb));
                 }
                 if (!ok) break;
@@ -473,9 +501,12 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
         // ------------------------------------------------------------ read-back
         const int e = warp - 2;
         const int quarter = warp & 3;            // TMEM lanes [32*quarter, 32*quarter+32)
-        const int half = (e >> 2) & 1;           // accumulator / prefix half
+        const int sub = (e >> 2) & 1;            // which of the two warps of this quarter
+        const int half = SH::kHalves == 2 ? sub : 0;    // prefix half (256 x 128 tiles)
+        const int chunk = SH::kHalves == 2 ? 0 : sub;   // 128-column chunk (128 x 256 tiles)
         const uint32_t group = (uint32_t)(e >> 3);   // reads the tiles of this parity
         const int row = half * kTcM + quarter * 32 + lane;   // prefix-tile row
+        const uint32_t col0 = (uint32_t)(half * SH::kN + chunk * 128);   // within a buffer
         uint32_t it_c = 0;
         bool ok = true;
         TcJobRec R = tc_rec(recs, j0, total_jobs);
@@ -508,9 +539,9 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 const int thr = n_live - 2 * (T - 1 - w);
                 // the accumulators are in [-64, 64]: read them as packed 16-bit halves
                 uint32_t v[64];
-                tmem_ld128_p16(tmem + ((uint32_t)(quarter * 32) << 16) + (ac * kTcHalves + half) * kTcN,
-                               v);
-                tc_fence_before();
+                tmem_ld128_p16(tmem + ((uint32_t)(quarter * 32) << 16) + ac * 256u + col0, v);
+                // tcgen05.wait::ld (inside the load) has completed the reads of these columns,
+                // so the release below needs no further tcgen05 fence
                 __syncwarp();
                 if (lane == 0) mbar_arrive(acc_empty(ac));   // one arrival per warp
                 // per 64-column slice (32 registers), four chains of 16-bit x2 3-input maxima
@@ -543,11 +574,12 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                     const int HP = D.HP;
                     uint32_t xr[4] = {0u, 0u, 0u, 0u};
                     for (int h = 0; h < HP; ++h) xr[h] = __ldg(D.la + rr * HP + h);
-                    for (int sl = 0; sl < kTcN / kTcSlice; ++sl) {
+                    for (int sl = 0; sl < 128 / kTcSlice; ++sl) {
                         if (!(fl >> sl & 1u)) continue;
                         for (int part = 0; part < kTcSlice / 32; ++part) {
                             const unsigned long long c =
-                                bt * kTcN + (unsigned long long)(sl * kTcSlice + part * 32 + lane);
+                                bt * SH::kN + chunk * 128 +
+                                (unsigned long long)(sl * kTcSlice + part * 32 + lane);
                             bool cand = false;
                             if (c < C.ny) {
                                 int lb = D.a + D.b;
@@ -574,9 +606,9 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             if (warp == 2 && lane == 0) {
                 const unsigned long long lo = r0 > C.xoff ? r0 : C.xoff;
                 const unsigned long long hi =
-                    r0 + kTcRows < C.xoff + C.nx ? r0 + kTcRows : C.xoff + C.nx;
-                const unsigned long long c_lo = b0 * kTcN;
-                const unsigned long long c_hi = b1 * kTcN < C.ny ? b1 * kTcN : C.ny;
+                    r0 + SH::kRows < C.xoff + C.nx ? r0 + SH::kRows : C.xoff + C.nx;
+                const unsigned long long c_lo = b0 * SH::kN;
+                const unsigned long long c_hi = b1 * SH::kN < C.ny ? b1 * SH::kN : C.ny;
                 if (hi > lo && c_hi > c_lo) atomicAdd(D.count, (hi - lo) * (c_hi - c_lo));
             }
         }
@@ -677,9 +709,22 @@ tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, 
 }  // namespace dev
 
 // ---------------------------------------------------------------- host launchers
-int tc_tile_rows() { return dev::kTcRows; }
-int tc_tile_cols() { return dev::kTcN; }
+// The sweep's tile shape, read once: QSFB_TC_SHAPE=0 for 256 x 128 tiles (two prefix halves
+// per suffix tile), 1 (default) for 128 x 256 tiles (one MMA row block, N = 256).  Both give
+// the same answers and counts; the planner and the job decoder follow the active shape.
+int tc_shape() {
+    static const int shape = []() {
+        const char* e = std::getenv("QSFB_TC_SHAPE");
+        return (e && std::atoi(e) == 0) ? 0 : 1;
+    }();
+    return shape;
+}
+int tc_tile_rows() { return tc_shape() == 0 ? dev::TcHalvesShape::kRows : dev::TcWideShape::kRows; }
+int tc_tile_cols() { return tc_shape() == 0 ? dev::TcHalvesShape::kN : dev::TcWideShape::kN; }
 int tc_job_tiles() { return dev::kTcJB; }
+// the operand-layout self-test runs the 256 x 128 tile (its A and B are that size)
+int tc_selftest_rows() { return dev::kTcRows; }
+int tc_selftest_cols() { return dev::kTcN; }
 
 cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_rows,
                              int num_sms, cudaStream_t st) {
@@ -693,30 +738,39 @@ cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long tot
 
 size_t tc_job_record_bytes() { return sizeof(dev::TcJobRec); }
 
-cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
-                            const unsigned long long* B, void* job_recs, int* err, int num_sms,
-                            cudaStream_t st) {
-    if (jobs == 0) return cudaSuccess;
-    dev::TcJobRec* recs = (dev::TcJobRec*)job_recs;
+template <class SH>
+static cudaError_t launch_pairs_tc_t(const LevelDesc* d, int nd, unsigned long long jobs,
+                                     const unsigned long long* B, dev::TcJobRec* recs, int* err,
+                                     int num_sms, cudaStream_t st) {
     {
         unsigned long long blocks = (jobs + 255) / 256;
         const unsigned long long cap = (unsigned long long)num_sms * 8;
         if (blocks > cap) blocks = cap;
-        dev::tc_jobs_kernel<<<(unsigned)blocks, 256, 0, st>>>(d, nd, jobs, B, recs);
+        dev::tc_jobs_kernel<SH><<<(unsigned)blocks, 256, 0, st>>>(d, nd, jobs, B, recs);
     }
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(dev::pairs_tc_kernel,
+        cudaError_t e = cudaFuncSetAttribute(dev::pairs_tc_kernel<SH>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)dev::kTcSmem);
+                                             (int)SH::kSmem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
     unsigned long long blocks = (unsigned long long)num_sms;
     if (jobs < blocks) blocks = jobs;
-    dev::pairs_tc_kernel<<<(unsigned)blocks, dev::kTcThreads, dev::kTcSmem, st>>>(d, recs, jobs,
-                                                                                 B, err);
+    dev::pairs_tc_kernel<SH><<<(unsigned)blocks, dev::kTcThreads, SH::kSmem, st>>>(d, recs, jobs,
+                                                                                   B, err);
     return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
+                            const unsigned long long* B, void* job_recs, int* err, int num_sms,
+                            cudaStream_t st) {
+    if (jobs == 0) return cudaSuccess;
+    dev::TcJobRec* recs = (dev::TcJobRec*)job_recs;
+    return tc_shape() == 0
+               ? launch_pairs_tc_t<dev::TcHalvesShape>(d, nd, jobs, B, recs, err, num_sms, st)
+               : launch_pairs_tc_t<dev::TcWideShape>(d, nd, jobs, B, recs, err, num_sms, st);
 }
 
 cudaError_t launch_tc_selftest(const int8_t* A, const int8_t* Bm, int ksteps, int packed,
