@@ -476,6 +476,7 @@ def main():
                         "chunks (all but the first overlap the rounds); rounds_span_s is the "
                         "merged rounds' device span"},
         "gpu_launches": launches,
+        "tuning": tuning_summary(_native),
         "clocks": clocks,
         "distance_checksum": int(np.sum(np.array(full_dists, dtype=np.int64) *
                                         np.arange(1, len(full_dists) + 1))),
@@ -664,6 +665,19 @@ def bench_mitm(args, rank, world, local, pg):
         "e2e": {"value": value, "unit": "certs/s",
                 "h2d_bytes_per_step": int(Hx.size + Hz.size), "d2h_bytes_per_step": 48},
         "gpu_launches": rep.kernel_launches, "clocks": clk.summary()}), flush=True)
+
+
+def tuning_summary(native):
+    """The launch shapes in effect and, when they come from the tuning table, the gain the
+    tuner measured over the defaults on the same batch (its header lines)."""
+    t = native.tuning()
+    out = {"values": {k: v for k, v in t.items() if k != "source"}, "source": t.get("source")}
+    src = str(t.get("source", ""))
+    path = Path(src.split(" + ")[0])
+    if path.exists():
+        out["measured_gain"] = [l[2:].strip() for l in path.read_text().splitlines()
+                                if l.startswith("# resident") or l.startswith("# one-shot")]
+    return out
 
 
 def tc_traffic_per_launch(tc_cw_per_step):

@@ -291,6 +291,13 @@ int qsfb_enumerate_plan_noalloc(int n, int stride, int K, int d, int num_gamma,
                                 unsigned long long* d_out_counts, int* d_out_g,
                                 unsigned long long* d_out_rank, void* stream);
 
+/* The launch shapes in effect (no reference counterpart): `key value` lines -- the
+ * tensor-core sweep's tile shape and job size per level-size class, the CUDA-core loop
+ * tile, the tensor/CUDA-core cost ratio, the batch pipeline's group and chunk counts --
+ * and where they came from (defaults, the tuning table beside the library written by
+ * `python -m qubitserf_b200.tune`, QSFB_TUNING, QSFB_TUNE_<KEY>).  Returns 0, 1, 7. */
+int qsfb_tuning(char* out, int cap);
+
 /* Measured integer-pipe peak (ops/s over the whole device): which = 0 for 32-bit POPC
  * (the XU pipe), 1 for LOP3 (the ALU pipe).  Roofline denominators of the pair kernel. */
 int qsfb_microbench(int which, double* ops_per_s);

@@ -128,6 +128,7 @@ SIGNATURES = [
                                 ctypes.c_longlong, _u64p, ctypes.c_longlong, _u32p,
                                 ctypes.c_longlong, _u32p, ctypes.c_longlong]),
     ("qsfb_last_report", _i, [ctypes.POINTER(QsfbReport)]),
+    ("qsfb_tuning", _i, [ctypes.c_char_p, _i]),
     ("qsfb_last_witness", _i, [_u8p, _i]),
     ("qsfb_last_counts", _i, [_ip, _ip, _ip, _ullp, _i]),
     ("qsfb_batch", _i, [ctypes.POINTER(QsfbQuery), _i, _i, ctypes.POINTER(QsfbAnswer),
@@ -380,6 +381,23 @@ def prepare_sides(kind, A, B=None, on_device=True):
             "syn": syn[: ng * K * SWP].reshape(ng, K, SWP).copy(),
             "even": bool(even), "count_all": bool(count_all), "seed_upper": seed_upper,
             "device": bool(on_dev), "classes": bool(classes)}
+
+
+def tuning() -> dict:
+    """The launch shapes in effect and their source (the tuning table, or defaults)."""
+    buf = ctypes.create_string_buffer(4096)
+    _check(lib().qsfb_tuning(buf, len(buf)), "qsfb_tuning")
+    out = {}
+    for line in buf.value.decode().splitlines():
+        key, _, val = line.partition(" ")
+        try:
+            out[key] = int(val)
+        except ValueError:
+            try:
+                out[key] = float(val)
+            except ValueError:
+                out[key] = val
+    return out
 
 
 def last_report() -> QsfbReport:

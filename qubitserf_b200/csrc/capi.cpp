@@ -18,6 +18,7 @@
 
 #include "bz.hpp"
 #include "infoset_types.hpp"
+#include "tuning.hpp"
 #include "engine.hpp"
 #include "mitm.hpp"
 #include "problem.hpp"
@@ -293,7 +294,7 @@ struct ChunkFeed {
 int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_ms,
                    int max_groups, ChunkFeed* F = nullptr, size_t total_jobs = 0) {
     const char* ge = std::getenv("QSFB_EXEC_GROUPS");   // read per call (benchmarks switch it)
-    const int groups_env = std::max(1, std::min(ge ? std::atoi(ge) : 3, 8));
+    const int groups_env = std::max(1, std::min(ge ? std::atoi(ge) : tuning().exec_groups, 8));
     const size_t njobs = std::max(H->ptrs.size(), total_jobs);
     const int G = std::max(1, std::min({groups_env, max_groups, (int)(njobs / 64)}));
     std::vector<size_t> taken(G, 0);
@@ -963,7 +964,7 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     constexpr int kPipeMin = 256;   // below this the batch runs in one piece
     // QSFB_BATCH_CHUNKS: number of pipeline chunks (default 4; 1 = one piece), read per call.
     const char* ce = std::getenv("QSFB_BATCH_CHUNKS");
-    const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : 4, 64));
+    const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : tuning().batch_chunks, 64));
     std::vector<int> cut{0};
     if (nq >= kPipeMin && chunks > 1) {
         const int first = std::max(32, nq / (2 * chunks));
@@ -985,15 +986,13 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     const int all = host_threads > 0 ? host_threads
                                      : std::max(1, (int)std::thread::hardware_concurrency());
     const int overlap_threads = pe ? std::max(1, std::atoi(pe)) : std::max(1, all - 4);
-    const int overlap_groups = ge ? std::max(1, std::atoi(ge)) : 3;
+    const int overlap_groups = ge ? std::max(1, std::atoi(ge)) : tuning().overlap_groups;
     auto prepare = [&](int c) {
         tp0[c] = now_seconds();
         prc[c] = qsfb_batch_prepare(queries + cut[c], cut[c + 1] - cut[c],
                                     c == 0 ? host_threads : overlap_threads, &H[c]);
         tp1[c] = now_seconds();
     };
-    // the chunks' handles are torn down in parallel (jobs' host state, device lists back to
-    // the allocator's cache, sessions back to the pool)
     // the chunks' device memory and sessions go back at once; the host-side teardown of
     // their jobs (many small frees) runs on a background thread after the call returns
     auto release = [&]() {
@@ -1086,6 +1085,20 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
         std::fprintf(stderr, "qsfb_batch: answers %.2f ms, release %.2f ms, call %.2f ms\n",
                      1e3 * (ta1 - te1), 1e3 * (now_seconds() - ta1), 1e3 * (now_seconds() - t0));
     return rc;
+}
+
+int qsfb_tuning(char* out, int cap) {
+    if (!out || cap <= 0) return kErrNull;
+    const Tuning& t = tuning();
+    const int n = std::snprintf(
+        out, (size_t)cap,
+        "tc_shape %d\ntc_job_tiles.small %d\ntc_job_tiles.large %d\ntc_small_tiles %lld\n"
+        "cc_jobs_per_warp %d\ntc_cost_ratio %g\nexec_groups %d\nbatch_chunks %d\n"
+        "overlap_groups %d\nsource %s\n",
+        t.tc_shape, t.tc_job_tiles_small, t.tc_job_tiles_large, t.tc_small_tiles,
+        t.cc_jobs_per_warp, t.tc_cost_ratio, t.exec_groups, t.batch_chunks, t.overlap_groups,
+        t.source.c_str());
+    return n < cap ? kOk : 7;
 }
 
 int qsfb_microbench(int which, double* ops_per_s) {

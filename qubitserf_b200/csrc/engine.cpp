@@ -1,6 +1,7 @@
 // Host side of the device engine: context, allocator, side upload and the level runner.
 #include "engine.hpp"
 #include "filter_plan.hpp"
+#include "tuning.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -24,7 +25,6 @@ cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
 size_t tc_job_record_bytes();
 int tc_tile_rows();
 int tc_tile_cols();
-int tc_job_tiles();
 
 namespace {
 constexpr unsigned long long kSat = ~0ull;
@@ -454,7 +454,7 @@ int tc_depth(int n_enc, int t, int popcs, int* n_live) {
     const double pass = hamming_pass_rate(nl, t);
     const double cost = 262.0 + 512.0 * 64.0 * pass * 1300.0 / 8.0;
     const double cc = popcs > 0 ? 2048.0 * popcs : 1280.0;
-    if (cost >= 0.6 * cc) return 0;
+    if (cost >= tuning().tc_cost_ratio * cc) return 0;
     *n_live = nl;
     return 2;
 }
@@ -508,7 +508,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     const auto tp0 = std::chrono::steady_clock::now();
     outs.assign(reqs.size(), LevelOut());
     if (reqs.empty()) return kOk;
-    const int tcM = tc_tile_rows(), tcN = tc_tile_cols(), tcJB = tc_job_tiles();
+    const int tcM = tc_tile_rows(), tcN = tc_tile_cols();
 
     // 1) plan every (request, set); a full-rank set may split into a tensor-core plan for
     //    the terms whose rectangles fill the MMA tiles and CUDA-core plans for the rest
@@ -611,7 +611,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     }
     // loop tile: enough jobs to keep every resident warp busy several times over
     // ~16 jobs per resident warp: the launch tail (one job) stays a few % of the level
-    const unsigned long long want_jobs = (unsigned long long)dev->num_sms * 24 * 16;
+    const unsigned long long want_jobs =
+        (unsigned long long)dev->num_sms * 24 * (unsigned long long)tuning().cc_jobs_per_warp;
     unsigned long long lt = cc_pairs / ((unsigned long long)kRegTile * want_jobs);
     lt = std::max<unsigned long long>(32, std::min<unsigned long long>(1024, lt));
     const int loop_tile = (int)((lt + 31) / 32 * 32);
@@ -740,6 +741,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     //    differ only in their lists
     unsigned long long tc_jobs = 0;
     std::vector<std::vector<unsigned long long>> tables;
+    std::vector<int> table_jb;                              // tensor-core job tiles per table
     std::unordered_map<unsigned long long, int> table_of;   // packed (K, a, b, tc, p_lo, nterms)
     for (Plan& P : plans) {
         const unsigned long long tkey =
@@ -751,6 +753,18 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             const int K = reqs[P.req].side->K;
             std::vector<unsigned long long> tj(P.nterms + 1, 0ull);
             unsigned long long acc = 0;
+            // tensor-core plans: suffix tiles per job by the level's size class (tuned)
+            int jb = 0;
+            if (P.tc) {
+                unsigned long long tiles = 0;
+                for (int t = 0; t < P.nterms; ++t) {
+                    const int p = P.p_lo + t;
+                    const unsigned long long xoff = dev->binom(p, P.a);
+                    const unsigned long long na = ((xoff & 7ull) + dev->binom(p, P.a - 1) + tcM - 1) / tcM;
+                    tiles += na * ((dev->binom(K - 1 - p, P.b) + tcN - 1) / tcN);
+                }
+                jb = tc_job_tiles_for(tiles);
+            }
             for (int t = 0; t < P.nterms; ++t) {
                 const int p = P.p_lo + t;
                 const unsigned long long nx = dev->binom(p, P.a - 1);
@@ -761,7 +775,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                     const unsigned long long xoff = dev->binom(p, P.a);
                     const unsigned long long na = ((xoff & 7ull) + nx + tcM - 1) / tcM;
                     const unsigned long long nbt = (ny + tcN - 1) / tcN;
-                    acc += na * ((nbt + tcJB - 1) / tcJB);
+                    acc += na * ((nbt + jb - 1) / jb);
                 } else {
                     const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
                     acc += ((rn + kRegTile - 1) / kRegTile) * ((ln + loop_tile - 1) / loop_tile);
@@ -770,6 +784,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             tj[P.nterms] = acc;
             it = table_of.emplace(tkey, (int)tables.size()).first;
             tables.push_back(std::move(tj));
+            table_jb.push_back(jb);
         }
         P.table = it->second;
         P.jobs = tables[P.table].back();
@@ -786,7 +801,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 const unsigned long long xoff = dev->binom(p, P.a);
                 const unsigned long long na = ((xoff & 7ull) + nx + tcM - 1) / tcM;
                 tiles += na * ((ny + tcN - 1) / tcN);
-                atiles += na * ((((ny + tcN - 1) / tcN) + tcJB - 1) / tcJB);
+                const unsigned long long jb = (unsigned long long)table_jb[P.table];
+                atiles += na * ((((ny + tcN - 1) / tcN) + jb - 1) / jb);
                 pairs += nx * ny;
             }
         }
@@ -921,11 +937,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         while (bits < 64 && (P.pairs - 1) >> bits) ++bits;
         D.rank_shift = std::max(0, bits - kKeyGShift);
         D.count_all = S->count_all ? 1 : 0;
+        D.tc_job_tiles = 0;
         if (P.tc) {
             D.ksteps = P.ksteps;
             D.n_live = P.n_live;
             D.xpm = La.pm;
             D.ypm = Rb.pm;
+            D.tc_job_tiles = table_jb[P.table];
         }
         Gp.jobs += P.jobs;
         Gp.count += 1;

@@ -51,7 +51,7 @@ struct LevelDesc {
     const int8_t* xpm;        // la rows
     const int8_t* ypm;        // rb rows
     int n_live;               // live +-1 columns among the first 32 * ksteps
-    int pad_;
+    int tc_job_tiles;         // suffix tiles per tensor-core job of this level
 };
 
 constexpr int kGenRun = 4;         // consecutive list entries generated by one thread (measured: 2, 8 and 32 are slower)

@@ -39,6 +39,7 @@
 
 #include "engine_types.hpp"
 #include "enum_device.cuh"
+#include "tuning.hpp"
 
 namespace qsfb {
 namespace dev {
@@ -49,7 +50,6 @@ constexpr int kTcRows = kTcM * kTcHalves;  // prefix rows per tile
 constexpr int kTcN = 128;                  // suffix rows per tile (UMMA N)
 constexpr int kTcK = 2;                    // K = 32 steps (64 columns)
 constexpr int kTcBStages = 8;              // suffix tiles in flight
-constexpr int kTcJB = 16;                  // suffix tiles per job
 constexpr int kTcSlice = 64;               // accumulator columns per rescan slice
 constexpr int kTcEpiGroups = 2;            // read-back groups: one per accumulator buffer
 constexpr int kTcEpiWarps = 8 * kTcEpiGroups;   // x 2 halves x 4 lane quarters
@@ -350,7 +350,8 @@ __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restric
         const unsigned long long ny = binom(B, D.K - 1 - p, D.b);
         const unsigned long long xoff = binom(B, p, D.a);
         const unsigned long long nbt = (ny + SH::kN - 1) / SH::kN;
-        const unsigned long long nbc = (nbt + kTcJB - 1) / kTcJB;
+        const unsigned long long jb = (unsigned long long)D.tc_job_tiles;
+        const unsigned long long nbc = (nbt + jb - 1) / jb;
         const unsigned long long ia = idx / nbc, jc = idx - ia * nbc;
         TcJobRec R;
         R.xpm = D.xpm;
@@ -361,8 +362,8 @@ __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restric
         R.nx = (unsigned int)nx;
         R.ny = (unsigned int)ny;
         R.d = (unsigned int)lo;
-        R.b0 = (unsigned int)(jc * kTcJB);
-        R.b1 = (unsigned int)(jc * kTcJB + kTcJB < nbt ? jc * kTcJB + kTcJB : nbt);
+        R.b0 = (unsigned int)(jc * jb);
+        R.b1 = (unsigned int)(jc * jb + jb < nbt ? jc * jb + jb : nbt);
         const unsigned int T0 = (unsigned int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
         R.tnw = (T0 & 0xFFFu) | ((unsigned int)D.n_live << 12) | ((unsigned int)D.w << 20);
         R.pad = 0;
@@ -709,19 +710,20 @@ tc_selftest_kernel(const int8_t* __restrict__ A, const int8_t* __restrict__ Bm, 
 }  // namespace dev
 
 // ---------------------------------------------------------------- host launchers
-// The sweep's tile shape, read once: QSFB_TC_SHAPE=0 for 256 x 128 tiles (two prefix halves
-// per suffix tile), 1 (default) for 128 x 256 tiles (one MMA row block, N = 256).  Both give
-// the same answers and counts; the planner and the job decoder follow the active shape.
+// The sweep's tile shape, read once: 0 for 256 x 128 tiles (two prefix halves per suffix
+// tile), 1 for 128 x 256 tiles (one MMA row block, N = 256); the tuning table's tc_shape,
+// or QSFB_TC_SHAPE.  Both give the same answers and counts; the planner and the job decoder
+// follow the active shape.
 int tc_shape() {
     static const int shape = []() {
         const char* e = std::getenv("QSFB_TC_SHAPE");
-        return (e && std::atoi(e) == 0) ? 0 : 1;
+        if (e) return std::atoi(e) == 0 ? 0 : 1;
+        return tuning().tc_shape;
     }();
     return shape;
 }
 int tc_tile_rows() { return tc_shape() == 0 ? dev::TcHalvesShape::kRows : dev::TcWideShape::kRows; }
 int tc_tile_cols() { return tc_shape() == 0 ? dev::TcHalvesShape::kN : dev::TcWideShape::kN; }
-int tc_job_tiles() { return dev::kTcJB; }
 // the operand-layout self-test runs the 256 x 128 tile (its A and B are that size)
 int tc_selftest_rows() { return dev::kTcRows; }
 int tc_selftest_cols() { return dev::kTcN; }

@@ -375,3 +375,29 @@ def test_reference_python_binds_the_drop_in(native):
         assert "rc=5" in out["cpu"] and "rc=4" in out["auto"]
     else:
         assert "gpu" in out["backends"] and out["gpu"] == "ok" and "rc=5" in out["cpu"]
+
+
+def test_tuning_table_and_overrides(native, tmp_path):
+    """The library reads its launch shapes once: defaults, then a `key value` table
+    (QSFB_TUNING, else tuning.txt beside the library), then QSFB_TUNE_<KEY> overrides;
+    unknown keys and malformed lines are ignored, values are clamped to their ranges."""
+    import json
+    table = tmp_path / "t.txt"
+    table.write_text("# comment\ntc_shape 0\ntc_job_tiles.large 8  # trailing\n"
+                     "cc_jobs_per_warp 9999\nbogus 3\ntc_cost_ratio x\nbatch_chunks 6\n")
+    code = ("import sys, json; sys.path.insert(0, sys.argv[1]); "
+            "from qubitserf_b200 import _native as N; print(json.dumps(N.tuning()))")
+    env = dict(os.environ, QSFB_TUNING=str(table), QSFB_TUNE_EXEC_GROUPS="2",
+               QSFB_TUNE_TC_JOB_TILES_SMALL="4")
+    p = subprocess.run([sys.executable, "-c", code, str(ROOT)], env=env, capture_output=True,
+                       text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    t = json.loads(p.stdout.strip().splitlines()[-1])
+    assert (t["tc_shape"], t["tc_job_tiles.large"], t["batch_chunks"]) == (0, 8, 6)
+    assert t["cc_jobs_per_warp"] == 256 and t["tc_cost_ratio"] == 0.6   # clamped / kept
+    assert (t["exec_groups"], t["tc_job_tiles.small"]) == (2, 4)
+    assert str(table) in t["source"] and "QSFB_TUNE_EXEC_GROUPS" in t["source"]
+    env = dict(os.environ, QSFB_TUNING=str(tmp_path / "absent.txt"))
+    p = subprocess.run([sys.executable, "-c", code, str(ROOT)], env=env, capture_output=True,
+                       text=True, timeout=120)
+    assert json.loads(p.stdout.strip().splitlines()[-1])["source"] == "defaults"
