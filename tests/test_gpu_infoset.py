@@ -48,25 +48,31 @@ def test_batch_infosets_device_equals_host(native, ref):
 
 
 def test_matroid_partition_classes_on_device(native, ref):
-    """Classical codes whose greedy peel packs fewer full-rank sets than the matroid
-    partition: the classes go to the device as explicit column lists."""
+    """Sides whose greedy peel packs fewer full-rank sets than the matroid partition: the
+    classes go to the device as explicit column lists (the batch's classical codes have
+    dozens of them), and sparse random codes with zero columns exercise many-set peels."""
+    from qubitserf_b200 import workloads as W
     from qubitserf_b200.workloads import classical_parity_from_rng
-    rng = np.random.default_rng(11)
     classes = 0
-    for _ in range(80):
+    for cs in W.batch_1024(1024)[:512:2]:      # 256 of the classical codes
+        d = native.prepare_sides(0, *cs.mats, on_device=True)
+        h = native.prepare_sides(0, *cs.mats, on_device=False)
+        _same(d, h, cs.n)
+        classes += d["classes"]
+        if ref is not None and d["classes"]:
+            r = ref.problem_gammas(0, *cs.mats)
+            assert d["ranks"] == r["ranks"] and np.array_equal(d["gamma"], r["gamma"])
+    assert classes >= 5
+    rng = np.random.default_rng(11)
+    for _ in range(40):
         n = int(rng.integers(20, 100))
         k = int(rng.integers(n // 4, n // 2 + 1))
         H = classical_parity_from_rng(rng, n, k)
-        H[:, rng.integers(0, n, n // 5)] = 0   # zero columns: greedy leaves rank behind
+        H[:, rng.integers(0, n, n // 5)] = 0   # zero columns: peels of up to 13 sets
         d = native.prepare_sides(0, H, on_device=True)
         h = native.prepare_sides(0, H, on_device=False)
         _same(d, h, n)
         assert d["device"]
-        if ref is not None:
-            r = ref.problem_gammas(0, H)
-            assert d["ranks"] == r["ranks"] and np.array_equal(d["gamma"], r["gamma"])
-        classes += d["classes"]   # the partition beat the greedy peel: built from class lists
-    assert classes > 10
 
 
 def test_golden_infosets_device_equals_host(native, golden, ref):
