@@ -35,6 +35,7 @@ size_t round_bucket(size_t b) {
     return r;
 }
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+constexpr size_t kMinHostStage = 8ull << 20;   // pinned staging of a new session
 }  // namespace
 
 // ------------------------------------------------------------------ Device
@@ -216,6 +217,13 @@ Session* Device::acquire() {
             delete s;
             return nullptr;
         }
+    // Pinned staging sized up front for a chunk's seed trials and information sets: growing
+    // it later (cudaFreeHost + cudaMallocHost, several ms) would stall a preparation that
+    // overlaps running rounds.  Sessions are pooled, so this is paid once per session.
+    if (s->ensure(0, kMinHostStage) != kOk) {
+        delete s;
+        return nullptr;
+    }
     return s;
 }
 

@@ -30,6 +30,25 @@ namespace {
 
 size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 
+// f(0..n-1) on up to hardware_concurrency() threads (inline when small)
+template <class F>
+void parallel_for(size_t n, F f) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t th_n = std::min<size_t>({n, hw, 16});
+    if (th_n <= 1) {
+        for (size_t k = 0; k < n; ++k) f(k);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < th_n; ++t)
+        pool.emplace_back([&]() {
+            for (size_t k; (k = next.fetch_add(1)) < n;) f(k);
+        });
+    for (size_t k; (k = next.fetch_add(1)) < n;) f(k);
+    for (auto& th : pool) th.join();
+}
+
 enum ItemState { kPending = 0, kDone = 1, kHost = 2, kClasses = 3 };
 
 struct Item {
@@ -226,19 +245,7 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
         if (matroid_sets(it->p->code_gen, full_sets(it->sets, it->K), &it->lists, &it->class_ranks))
             it->state = (int)it->lists.size() <= kInfosetMaxSets ? kClasses : kHost;
     };
-    const int nth = std::max(1, std::min<int>((int)cand.size(),
-                                              (int)std::thread::hardware_concurrency()));
-    if (nth <= 1) {
-        for (Item* it : cand) decide(it);
-    } else {
-        std::atomic<size_t> next{0};
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nth; ++t)
-            pool.emplace_back([&]() {
-                for (size_t k; (k = next.fetch_add(1)) < cand.size();) decide(cand[k]);
-            });
-        for (auto& th : pool) th.join();
-    }
+    parallel_for(cand.size(), [&](size_t k) { decide(cand[k]); });
     pass.clear();
     for (Item* it : cand)
         if (it->state == kClasses) pass.push_back(it);
@@ -249,16 +256,21 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
     const double t3 = now_seconds();
     int nhost = 0;
 
-    for (Item& it : items) {
+    std::atomic<int> arc{kOk};
+    parallel_for(items.size(), [&](size_t k) {   // host descriptions of the sets, per side
+        Item& it = items[k];
         BzSide& S = *it.side;
-        nhost += it.state != kDone;
         S.sets_from_classes = it.state == kDone && !it.lists.empty();
-        rc = it.state == kDone
-                 ? S.adopt_sets(std::move(it.sets), it.red, it.syn, it.W32, it.SWP, s->dev, arena)
-                 : S.adopt_sets(information_sets(it.p->code_gen), nullptr, nullptr, 0, 0, s->dev,
-                                arena);
-        if (rc != kOk) return rc;
-    }
+        const int r = it.state == kDone
+                          ? S.adopt_sets(std::move(it.sets), it.red, it.syn, it.W32, it.SWP,
+                                         s->dev, arena)
+                          : S.adopt_sets(information_sets(it.p->code_gen), nullptr, nullptr, 0,
+                                         0, s->dev, arena);
+        if (r != kOk) arc.store(r);
+    });
+    for (const Item& it : items) nhost += it.state != kDone;
+    rc = arc.load();
+    if (rc != kOk) return rc;
     if (trace)
         std::fprintf(stderr, "qsfb device sets: %zu sides: greedy pass %.2f ms, partition "
                      "search %.2f ms (%zu candidates, %zu replaced), class pass %.2f ms, "

@@ -43,7 +43,7 @@ RESIDENT_KNOBS = [
     ("exec_groups", [3, 2, 4]),
 ]
 E2E_KNOBS = [
-    ("batch_chunks", [4, 2, 3, 6]),
+    ("batch_chunks", [4, 1, 2, 3, 6]),
     ("overlap_groups", [3, 2, 4]),
 ]
 DEFAULTS = {k: v[0] for k, v in RESIDENT_KNOBS + E2E_KNOBS}
