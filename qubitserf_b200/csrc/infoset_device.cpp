@@ -64,8 +64,11 @@ struct Item {
 };
 
 // One launch pass (greedy peel, or the explicit class lists) over `items`.
-int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) {
+// tm[0..3] += seconds spent filling the staging, waiting for the kernels and the meta
+// read-back, reading the generator heap back, and building the host descriptions
+int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes, double* tm) {
     if (items.empty()) return kOk;
+    const double ta = now_seconds();
     std::stable_sort(items.begin(), items.end(),
                      [](const Item* a, const Item* b) { return a->W < b->W; });
     const size_t n = items.size();
@@ -141,6 +144,7 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
     unsigned long long* d_heap = (unsigned long long*)(d + off_heap);
     unsigned long long* d_ctr = (unsigned long long*)(d + off_ctr);
     cudaStream_t st = s->urgent;
+    const double tb = now_seconds();
     if (cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         launch_infosets(1, (const InfosetDesc*)(d + off_desc), (int)nw1, d_heap, d_ctr, st) !=
             cudaSuccess ||
@@ -152,6 +156,7 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
         cudaGetLastError();
         return kErrDevice;
     }
+    const double tc = now_seconds();
     const unsigned long long used = *(const unsigned long long*)(h + off_ctr);
     if (used > cap) return kErrDevice;
     thread_local std::vector<u64> heap_host;
@@ -162,6 +167,7 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
         return kErrDevice;
     }
     const u64* heap = heap_host.data();
+    const double td = now_seconds();
     for (size_t i = 0; i < n; ++i) {
         Item& it = *items[i];
         const InfosetMeta& M = *((const InfosetMeta*)(h + off_meta) + i);
@@ -191,6 +197,10 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes) 
         }
         it.state = ok ? kDone : kHost;
     }
+    tm[0] += tb - ta;
+    tm[1] += tc - tb;
+    tm[2] += td - tc;
+    tm[3] += now_seconds() - td;
     return kOk;
 }
 
@@ -227,7 +237,8 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
     }
     std::vector<Item*> pass;
     for (Item& it : items) pass.push_back(&it);
-    int rc = run_pass(s, arena, pass, false);
+    double tm[4] = {0, 0, 0, 0};
+    int rc = run_pass(s, arena, pass, false, tm);
     if (rc != kOk) return rc;
     const double t1 = now_seconds();
 
@@ -251,7 +262,7 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
         if (it->state == kClasses) pass.push_back(it);
     const double t2 = now_seconds();
     const size_t nclasses = pass.size();
-    rc = run_pass(s, arena, pass, true);
+    rc = run_pass(s, arena, pass, true, tm);
     if (rc != kOk) return rc;
     const double t3 = now_seconds();
     int nhost = 0;
@@ -274,9 +285,11 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
     if (trace)
         std::fprintf(stderr, "qsfb device sets: %zu sides: greedy pass %.2f ms, partition "
                      "search %.2f ms (%zu candidates, %zu replaced), class pass %.2f ms, "
-                     "adopt %.2f ms (%d built on the host)\n", items.size(), 1e3 * (t1 - t0),
+                     "adopt %.2f ms (%d built on the host); passes: staging %.2f, device %.2f, "
+                     "heap read-back %.2f, host sets %.2f ms\n", items.size(), 1e3 * (t1 - t0),
                      1e3 * (t2 - t1), cand.size(), nclasses, 1e3 * (t3 - t2),
-                     1e3 * (now_seconds() - t3), nhost);
+                     1e3 * (now_seconds() - t3), nhost, 1e3 * tm[0], 1e3 * tm[1], 1e3 * tm[2],
+                     1e3 * tm[3]);
     if (stats) {
         stats->device_sets_s += now_seconds() - t0;
         stats->launches += 2;

@@ -277,6 +277,13 @@ __device__ __forceinline__ void tmem_ld128_p16(uint32_t taddr, uint32_t (&v)[64]
         : "memory");
 }
 
+// An empty statement that reads and writes all 64 loaded registers: arithmetic on them
+// cannot be scheduled before it, so a buffer's release (issued just before) is not delayed
+// by the slice maxima that only need the registers.
+__device__ __forceinline__ void after_release(uint32_t (&v)[64]) {
+    asm volatile("" : "+r"(v[0]),"+r"(v[1]),"+r"(v[2]),"+r"(v[3]),"+r"(v[4]),"+r"(v[5]),"+r"(v[6]),"+r"(v[7]),"+r"(v[8]),"+r"(v[9]),"+r"(v[10]),"+r"(v[11]),"+r"(v[12]),"+r"(v[13]),"+r"(v[14]),"+r"(v[15]),"+r"(v[16]),"+r"(v[17]),"+r"(v[18]),"+r"(v[19]),"+r"(v[20]),"+r"(v[21]),"+r"(v[22]),"+r"(v[23]),"+r"(v[24]),"+r"(v[25]),"+r"(v[26]),"+r"(v[27]),"+r"(v[28]),"+r"(v[29]),"+r"(v[30]),"+r"(v[31]),"+r"(v[32]),"+r"(v[33]),"+r"(v[34]),"+r"(v[35]),"+r"(v[36]),"+r"(v[37]),"+r"(v[38]),"+r"(v[39]),"+r"(v[40]),"+r"(v[41]),"+r"(v[42]),"+r"(v[43]),"+r"(v[44]),"+r"(v[45]),"+r"(v[46]),"+r"(v[47]),"+r"(v[48]),"+r"(v[49]),"+r"(v[50]),"+r"(v[51]),"+r"(v[52]),"+r"(v[53]),"+r"(v[54]),"+r"(v[55]),"+r"(v[56]),"+r"(v[57]),"+r"(v[58]),"+r"(v[59]),"+r"(v[60]),"+r"(v[61]),"+r"(v[62]),"+r"(v[63]));
+}
+
 // Shared setup of both tensor-core kernels: barriers by thread 0, TMEM by warp 1.
 __device__ __forceinline__ uint32_t tc_setup(uint32_t bar0, int nbar, const uint32_t* counts,
                                              uint32_t* tmem_slot) {
@@ -545,6 +552,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 // so the release below needs no further tcgen05 fence
                 __syncwarp();
                 if (lane == 0) mbar_arrive(acc_empty(ac));   // one arrival per warp
+                after_release(v);
                 // per 64-column slice (32 registers), four chains of 16-bit x2 3-input maxima
                 uint32_t fbits = 0;
 #pragma unroll
