@@ -212,12 +212,15 @@ typedef struct {
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free.  Batches of 256 queries or more are pipelined in
- * chunks (four by default, QSFB_BATCH_CHUNKS to change): the first, small chunk's rounds
- * start at once as three job groups, and each later chunk, prepared meanwhile on all host
- * cores but four, joins those groups at their next round boundary.  The answers are those
- * of one batch; the stats give the merged rounds and sum the chunks' preparation phases
- * (device_bytes: all chunks together).  QSFB_BATCH_TRACE prints each chunk's phase times
- * to stderr. */
+ * chunks (the count of the library's tuning table, QSFB_BATCH_CHUNKS to change): the
+ * first, small chunk's rounds start at once as three job groups, and each later chunk,
+ * prepared meanwhile on all host cores but four, joins those groups at their next round
+ * boundary.  The queries go to the chunks in the order of their shape's Gilbert-Varshamov
+ * distance, largest first (later chunks join later, and a code needs one round per level;
+ * QSFB_BATCH_ORDER=index keeps the caller's order).  out[i] answers queries[i] either way,
+ * and the answers are those of one batch; the stats give the merged rounds and sum the
+ * chunks' preparation phases (device_bytes: all chunks together).  QSFB_BATCH_TRACE prints
+ * each chunk's phase times to stderr. */
 int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* out,
                QsfbBatchStats* stats);
 

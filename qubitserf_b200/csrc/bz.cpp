@@ -535,115 +535,143 @@ BzResult BzJob::compute_result() {
 cudaError_t launch_seed_trials(int W, const SeedDesc* d_descs, int ndesc, int total_trials,
                                cudaStream_t st);
 
-// Run every pending seed trial of every job in one launch per row width, then fold the
-// per-side keys into the bounds.
-int device_seeds(Session* s, Arena* arena, std::vector<BzJob*>& jobs, RunStats* stats) {
+namespace {
+// Seed trials in flight: launched by seeds_begin, folded into the bounds by seeds_end.
+struct SeedLaunch {
+    std::vector<BzSide*> sides;   // in the order of `keys`
+    unsigned* keys = nullptr;     // pinned host copy of the keys
+    const unsigned* d_keys = nullptr;
+    cudaStream_t st = nullptr;
+    bool launched = false;
+    double t0 = 0.0;
+};
+
+// Every pending seed trial of every job, one launch per row width, on the session's
+// `urgent2` stream: staging in the session's seed buffer, so that other preparation work
+// may use the main staging while the trials run.
+int seeds_begin(Session* s, Arena* arena, std::vector<BzJob*>& jobs, SeedLaunch* L) {
+    L->t0 = now_seconds();
     std::vector<BzSide*> pend[3];   // by row words W = 1, 2
     for (BzJob* j : jobs)
         for (int i = 0; i < (j->pair ? 2 : 1); ++i)
             if (j->s[i].seed_pending) pend[words_for(j->s[i].prob->n)].push_back(&j->s[i]);
-    const double t0 = now_seconds();
-    bool any = false;
-    for (int W = 1; W <= 2; ++W) {
-        std::vector<BzSide*>& v = pend[W];
-        if (v.empty()) continue;
-        any = true;
-        // layout: descs | keys | per side: gen, check, perm
-        size_t off = 0;
-        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-        const size_t off_desc = off;
-        off = al(off + v.size() * sizeof(SeedDesc));
-        const size_t off_keys = off;
-        off = al(off + v.size() * 4);
-        // the column orders are shared by every side of the same length: one copy each
-        std::vector<size_t> og(v.size()), oc(v.size()), op(v.size());
-        std::map<const std::vector<uint8_t>*, size_t> perm_off;
-        for (size_t i = 0; i < v.size(); ++i) {
-            const Problem& p = *v[i]->prob;
-            og[i] = off; off = al(off + (size_t)p.code_gen.rows * W * 8);
-            oc[i] = off; off = al(off + (size_t)std::max(1, p.check.rows) * W * 8);
-            const std::vector<uint8_t>* pp = v[i]->seed_perm.get();
-            auto it = perm_off.find(pp);
-            if (it == perm_off.end()) {
-                it = perm_off.emplace(pp, off).first;
-                off = al(off + pp->size());
-            }
-            op[i] = it->second;
+    for (int W = 1; W <= 2; ++W) L->sides.insert(L->sides.end(), pend[W].begin(), pend[W].end());
+    const size_t n = L->sides.size();
+    if (n == 0) return kOk;
+    // layout: keys (all sides) | descs (all sides, W = 1 first) | per side: gen, check |
+    // the column orders, shared by every side of the same length (one copy each)
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    size_t off = 0;
+    const size_t off_keys = off;
+    off = al(off + n * 4);
+    const size_t off_desc = off;
+    off = al(off + n * sizeof(SeedDesc));
+    std::vector<size_t> og(n), oc(n), op(n);
+    std::map<const std::vector<uint8_t>*, size_t> perm_off;
+    for (size_t i = 0; i < n; ++i) {
+        const Problem& p = *L->sides[i]->prob;
+        const int W = words_for(p.n);
+        og[i] = off; off = al(off + (size_t)p.code_gen.rows * W * 8);
+        oc[i] = off; off = al(off + (size_t)std::max(1, p.check.rows) * W * 8);
+        const std::vector<uint8_t>* pp = L->sides[i]->seed_perm.get();
+        auto it = perm_off.find(pp);
+        if (it == perm_off.end()) {
+            it = perm_off.emplace(pp, off).first;
+            off = al(off + pp->size());
         }
-        char* d = (char*)arena->alloc(off);
-        if (!d) return kErrMemory;
-        int rc = s->ensure(0, off);
-        if (rc != kOk) return rc;
-        char* h = (char*)s->h_stage.h;
-        SeedDesc* hd = (SeedDesc*)(h + off_desc);
-        unsigned* hk = (unsigned*)(h + off_keys);
-        int trials = 0;
-        for (size_t i = 0; i < v.size(); ++i) {
-            const Problem& p = *v[i]->prob;
-            u64* g = (u64*)(h + og[i]);
-            for (int r = 0; r < p.code_gen.rows; ++r)
-                for (int w = 0; w < W; ++w) g[(size_t)r * W + w] = p.code_gen.row(r)[w];
-            u64* c = (u64*)(h + oc[i]);
-            for (int r = 0; r < p.check.rows; ++r)
-                for (int w = 0; w < W; ++w) c[(size_t)r * W + w] = p.check.row(r)[w];
-            SeedDesc& D = hd[i];
-            D.gen = (const unsigned long long*)(d + og[i]);
-            D.check = (const unsigned long long*)(d + oc[i]);
-            D.perm = (const uint8_t*)(d + op[i]);
-            D.key = (unsigned*)(d + off_keys) + i;
-            D.trial_base = trials;
-            D.K = p.code_gen.rows;
-            D.n = p.n;
-            D.kcheck = p.count_all ? 0 : p.check.rows;
-            D.count_all = p.count_all ? 1 : 0;
-            D.init_best = v[i]->inner;
-            hk[i] = 0xffffffffu;
-            trials += v[i]->seed_trials;
-        }
-        for (const auto& po : perm_off) std::memcpy(h + po.second, po.first->data(), po.first->size());
-        // on the session's high-priority stream: in a pipelined batch or a server, the
-        // rounds of other codes fill the SMs meanwhile, and these codes wait for the result
+        op[i] = it->second;
+    }
+    char* d = (char*)arena->alloc(off);
+    if (!d) return kErrMemory;
+    int rc = s->grow_pinned(s->h_seed, off);
+    if (rc != kOk) return rc;
+    char* h = (char*)s->h_seed.h;
+    SeedDesc* hd = (SeedDesc*)(h + off_desc);
+    unsigned* hk = (unsigned*)(h + off_keys);
+    int trials[3] = {0, 0, 0};
+    for (size_t i = 0; i < n; ++i) {
+        const BzSide& S = *L->sides[i];
+        const Problem& p = *S.prob;
+        const int W = words_for(p.n);
+        u64* g = (u64*)(h + og[i]);
+        for (int r = 0; r < p.code_gen.rows; ++r)
+            for (int w = 0; w < W; ++w) g[(size_t)r * W + w] = p.code_gen.row(r)[w];
+        u64* c = (u64*)(h + oc[i]);
+        for (int r = 0; r < p.check.rows; ++r)
+            for (int w = 0; w < W; ++w) c[(size_t)r * W + w] = p.check.row(r)[w];
+        SeedDesc& D = hd[i];
+        D.gen = (const unsigned long long*)(d + og[i]);
+        D.check = (const unsigned long long*)(d + oc[i]);
+        D.perm = (const uint8_t*)(d + op[i]);
+        D.key = (unsigned*)(d + off_keys) + i;
+        D.trial_base = trials[W];
+        D.K = p.code_gen.rows;
+        D.n = p.n;
+        D.kcheck = p.count_all ? 0 : p.check.rows;
+        D.count_all = p.count_all ? 1 : 0;
+        D.init_best = S.inner;
+        D.pad_ = 0;
+        hk[i] = 0xffffffffu;
+        trials[W] += S.seed_trials;
+    }
+    for (const auto& po : perm_off) std::memcpy(h + po.second, po.first->data(), po.first->size());
+    // on a stream above the rounds' priority: in a pipelined batch or a server, the rounds
+    // of other codes fill the SMs meanwhile, and these codes wait for the result
+    const size_t n1 = pend[1].size();
+    const SeedDesc* dd = (const SeedDesc*)(d + off_desc);
+    // the keys' read-back is queued by seeds_end: queued here, behind the trials, it would
+    // hold back every later device-to-host copy of the preparation on the same copy engine
+    L->st = s->urgent2;
+    L->keys = hk;
+    L->d_keys = (const unsigned*)(d + off_keys);
+    L->launched = true;
+    if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, L->st) != cudaSuccess ||
+        (n1 > 0 && launch_seed_trials(1, dd, (int)n1, trials[1], L->st) != cudaSuccess) ||
+        (n > n1 && launch_seed_trials(2, dd + n1, (int)(n - n1), trials[2], L->st) !=
+                       cudaSuccess)) {
+        cudaGetLastError();
+        cudaStreamSynchronize(L->st);
+        cudaGetLastError();
+        L->launched = false;
+        return kErrDevice;
+    }
+    return kOk;
+}
+
+// Waits for the trials of seeds_begin and folds the per-side keys into the bounds.
+int seeds_end(std::vector<BzJob*>& jobs, SeedLaunch* L, RunStats* stats) {
+    if (L->launched) {
         const double tw0 = now_seconds();
-        if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s->urgent) != cudaSuccess ||
-            launch_seed_trials(W, (const SeedDesc*)(d + off_desc), (int)v.size(), trials,
-                               s->urgent) != cudaSuccess ||
-            cudaMemcpyAsync(h + off_keys, d + off_keys, v.size() * 4, cudaMemcpyDeviceToHost,
-                            s->urgent) != cudaSuccess ||
-            cudaStreamSynchronize(s->urgent) != cudaSuccess) {
+        L->launched = false;
+        if (cudaMemcpyAsync(L->keys, L->d_keys, L->sides.size() * 4, cudaMemcpyDeviceToHost,
+                            L->st) != cudaSuccess ||
+            cudaStreamSynchronize(L->st) != cudaSuccess) {
             cudaGetLastError();
             return kErrDevice;
         }
-        if (stats) stats->device_seed_wait_s += now_seconds() - tw0;
-        for (size_t i = 0; i < v.size(); ++i) v[i]->apply_device_seed(hk[i]);
-        if (stats) stats->launches += 1;
+        if (stats) {
+            stats->device_seed_wait_s += now_seconds() - tw0;
+            stats->launches += 1 + (words_for(L->sides.front()->prob->n) !=
+                                    words_for(L->sides.back()->prob->n));
+        }
+        for (size_t i = 0; i < L->sides.size(); ++i) L->sides[i]->apply_device_seed(L->keys[i]);
     }
-    if (any)
+    if (!L->sides.empty())
         for (BzJob* j : jobs) j->finish_setup();
-    if (stats) stats->device_seed_s += now_seconds() - t0;
+    if (stats) stats->device_seed_s += now_seconds() - L->t0;
     return kOk;
 }
+}  // namespace
 
 int setup_jobs_host(std::vector<BzJob*>& jobs, int host_threads, RunStats* stats) {
     const double th0 = now_seconds();
     int nth = host_threads > 0 ? host_threads : (int)std::thread::hardware_concurrency();
     nth = std::max(1, std::min<int>(nth, (int)jobs.size()));
-    std::atomic<size_t> next{0};
     std::atomic<int> err{kOk};
-    auto worker = [&]() {
-        for (;;) {
-            const size_t i = next.fetch_add(1);
-            if (i >= jobs.size()) break;
-            const int rc = jobs[i]->setup_host();
-            if (rc != kOk) err.store(rc);
-        }
-    };
-    if (nth == 1) {
-        worker();
-    } else {
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nth; ++t) pool.emplace_back(worker);
-        for (auto& th : pool) th.join();
-    }
+    host_parallel_for(jobs.size(), [&](size_t i) {
+        const int rc = jobs[i]->setup_host();
+        if (rc != kOk) err.store(rc);
+    }, nth);
     if (err.load() != kOk) return err.load();
     if (stats) stats->host_setup_s += now_seconds() - th0;
     return kOk;
@@ -651,15 +679,19 @@ int setup_jobs_host(std::vector<BzJob*>& jobs, int host_threads, RunStats* stats
 
 int setup_jobs_device(Device* dev, Session* s, Arena* arena, std::vector<BzJob*>& jobs,
                       RunStats* stats) {
-    int rc = device_seeds(s, arena, jobs, stats);
-    if (rc != kOk) return rc;
+    // the seed trials and the information-set eliminations are independent: the trials run
+    // on one stream while the sets are built on another and finished on the host
+    SeedLaunch L;
+    int rc = seeds_begin(s, arena, jobs, &L);
     std::vector<BzSide*> pend;
     for (BzJob* j : jobs)
         if (!j->zero)
             for (int i = 0; i < (j->pair ? 2 : 1); ++i)
                 if (j->s[i].infoset_pending) pend.push_back(&j->s[i]);
-    rc = device_infosets(s, arena, pend, stats);
+    if (rc == kOk) rc = device_infosets(s, arena, pend, stats);
+    const int rc2 = seeds_end(jobs, &L, stats);   // also after a failure: nothing left in flight
     if (rc != kOk) return rc;
+    if (rc2 != kOk) return rc2;
     std::vector<SideDev*> sides;
     for (BzJob* j : jobs)
         for (SideDev* sd : j->device_sides()) sides.push_back(sd);

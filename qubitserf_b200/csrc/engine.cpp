@@ -36,6 +36,7 @@ size_t round_bucket(size_t b) {
 }
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 constexpr size_t kMinHostStage = 8ull << 20;   // pinned staging of a new session
+constexpr size_t kMinSeedStage = 4ull << 20;   // and its seed-trial staging
 }  // namespace
 
 // ------------------------------------------------------------------ Device
@@ -115,12 +116,19 @@ void* Device::alloc(size_t bytes) {
     const size_t b = round_bucket(bytes);
     {
         std::lock_guard<std::mutex> lk(mu_);
+        // The bucket itself, else a cached block of the next bucket: a miss maps new memory
+        // (milliseconds for large blocks, kept by the pool for good), while the number of
+        // blocks of one size live at once varies with the timing of concurrent work.  A
+        // block keeps its own size through later releases.
         auto it = free_.find(b);
+        if (it == free_.end()) it = free_.find(2 * b);
         if (it != free_.end()) {
             void* p = it->second;
+            const size_t sz = it->first;
             free_.erase(it);
-            cached_ -= b;
-            in_use_ += b;
+            cached_ -= sz;
+            in_use_ += sz;
+            live_[p] = sz;
             return p;
         }
     }
@@ -161,6 +169,7 @@ void* Device::alloc(size_t bytes) {
     }
     std::lock_guard<std::mutex> lk(mu_);
     in_use_ += b;
+    live_[p] = b;
     return p;
 }
 
@@ -176,8 +185,13 @@ void Device::reserve(size_t bytes) {
 
 void Device::release(void* p, size_t bytes) {
     if (!p) return;
-    const size_t b = round_bucket(bytes);
     std::lock_guard<std::mutex> lk(mu_);
+    size_t b = round_bucket(bytes);
+    auto it = live_.find(p);
+    if (it != live_.end()) {
+        b = it->second;
+        live_.erase(it);
+    }
     free_.emplace(b, p);
     in_use_ -= b;
     cached_ += b;
@@ -203,6 +217,8 @@ Session* Device::acquire() {
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithPriority(&s->urgent, cudaStreamNonBlocking, prio_greatest) !=
             cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->urgent2, cudaStreamNonBlocking,
+                                     std::min(prio_least, prio_greatest + 1)) != cudaSuccess ||
         cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess ||
         cudaEventCreate(&s->ev_tc0) != cudaSuccess || cudaEventCreate(&s->ev_tc1) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
@@ -220,7 +236,7 @@ Session* Device::acquire() {
     // Pinned staging sized up front for a chunk's seed trials and information sets: growing
     // it later (cudaFreeHost + cudaMallocHost, several ms) would stall a preparation that
     // overlaps running rounds.  Sessions are pooled, so this is paid once per session.
-    if (s->ensure(0, kMinHostStage) != kOk) {
+    if (s->ensure(0, kMinHostStage) != kOk || s->grow_pinned(s->h_seed, kMinSeedStage) != kOk) {
         delete s;
         return nullptr;
     }
@@ -239,24 +255,29 @@ int Session::ensure(size_t dbytes, size_t hbytes) {
         d_stage.d = dev->alloc(d_stage.cap);
         if (!d_stage.d) { d_stage.cap = 0; return kErrMemory; }
     }
-    if (h_stage.cap < hbytes) {
-        const double tm0 = now_seconds();
-        if (h_stage.h) cudaFreeHost(h_stage.h);
-        h_stage.cap = round_bucket(hbytes);
-        const cudaError_t he = cudaMallocHost(&h_stage.h, h_stage.cap);
-        dev->n_pinned_alloc.fetch_add(1);
-        dev->ns_pinned_alloc.fetch_add((long long)((now_seconds() - tm0) * 1e9));
-        if (he != cudaSuccess) {
-            cudaGetLastError();
-            h_stage.h = nullptr;
-            h_stage.cap = 0;
-            return kErrMemory;
-        }
-    }
+    const int rc = grow_pinned(h_stage, hbytes);
+    if (rc != kOk) return rc;
     if (!d_ctr.d) {
         d_ctr.cap = 64 * sizeof(unsigned long long);
         d_ctr.d = dev->alloc(d_ctr.cap);
         if (!d_ctr.d) return kErrMemory;
+    }
+    return kOk;
+}
+
+int Session::grow_pinned(HostScratch& hs, size_t hbytes) {
+    if (hs.cap >= hbytes) return kOk;
+    const double tm0 = now_seconds();
+    if (hs.h) cudaFreeHost(hs.h);
+    hs.cap = round_bucket(hbytes);
+    const cudaError_t he = cudaMallocHost(&hs.h, hs.cap);
+    dev->n_pinned_alloc.fetch_add(1);
+    dev->ns_pinned_alloc.fetch_add((long long)((now_seconds() - tm0) * 1e9));
+    if (he != cudaSuccess) {
+        cudaGetLastError();
+        hs.h = nullptr;
+        hs.cap = 0;
+        return kErrMemory;
     }
     return kOk;
 }

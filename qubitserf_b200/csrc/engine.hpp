@@ -13,10 +13,12 @@
 
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <unordered_map>
 #include <vector>
 
 #include "engine_types.hpp"
@@ -39,6 +41,10 @@ enum Status : int {
 struct Session;
 
 double now_seconds();   // steady clock, seconds
+
+// f(0..n-1) on the calling thread and up to max_threads - 1 threads of a process-wide pool
+// (threads of the call's own while the pool serves another caller); returns when all ran
+void host_parallel_for(size_t n, const std::function<void(size_t)>& f, int max_threads = 16);
 
 class Device {
 public:
@@ -74,7 +80,8 @@ private:
     Device() = default;
     int init();
     std::mutex mu_;
-    std::multimap<size_t, void*> free_;
+    std::multimap<size_t, void*> free_;           // cached blocks by size
+    std::unordered_map<void*, size_t> live_;      // size of every block handed out
     // Cache misses are served by the stream-ordered allocator from the device's default
     // memory pool (release threshold: keep everything), on a stream of their own that is
     // synchronised before the pointer is handed out, so any stream may use it at once.
@@ -102,6 +109,10 @@ struct Session {
     // SMs (the random-information-set seed eliminations of a preparation) goes here, so its
     // blocks are scheduled first as SMs free up
     cudaStream_t urgent = nullptr;
+    // one priority step below `urgent` (still above the rounds): a preparation's seed
+    // trials run on it while its information-set eliminations, a short kernel on the
+    // critical path, run on `urgent` and take the SMs first as blocks retire
+    cudaStream_t urgent2 = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_tc0 = nullptr, ev_tc1 = nullptr;   // around the tensor-core sweep
     // pair launches of a round are spread over these streams (forked after the list
@@ -112,8 +123,10 @@ struct Session {
     cudaEvent_t ev_join[kAux] = {nullptr, nullptr, nullptr};
     DevScratch d_stage;    // descriptors + term tables + keys/counts
     HostScratch h_stage;   // pinned mirror of d_stage
+    HostScratch h_seed;    // pinned staging of the seed trials, in flight beside h_stage's
     DevScratch d_ctr;      // job counters (one per kernel variant)
     int ensure(size_t dbytes, size_t hbytes);
+    int grow_pinned(HostScratch& hs, size_t hbytes);   // contents are not kept
 };
 
 // RAII lease of a session from the device pool.

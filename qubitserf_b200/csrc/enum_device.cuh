@@ -130,18 +130,23 @@ static __device__ __noinline__ int survivor_scan(const LevelDesc& D, const unsig
     return T;
 }
 
+// 4 bits -> the low bit of 4 bytes: the multiplier puts copies of the nibble 7 bits apart
+// (bits 0-3, 7-10, 14-17, 21-24, no overlap, so no carries), and bit i of the nibble lands
+// on bit 8i of copy i.
+__device__ __forceinline__ uint32_t spread4(uint32_t nib) {
+    return (nib * 0x00204081u) & 0x01010101u;
+}
+
 // 16 probe bits -> 16 int8 columns of a +-1 row: set -> +1, clear -> -1, dead (beyond the
-// live columns, `live` bit clear) -> 0.
+// live columns, `live` bit clear) -> 0.  Per byte 0xFF - 0xFE * bit is 0x01 or 0xFF (no
+// borrows between bytes); the live mask is applied only on the row's last chunks.
 __device__ __forceinline__ uint4 pm_chunk(uint32_t bits, uint32_t live) {
     uint32_t q[4];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-        const uint32_t b = (bits >> (4 * n)) & 0xFu, l = (live >> (4 * n)) & 0xFu;
-        // one byte per column: 0/1 spread of the nibble
-        const uint32_t sb = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
-        const uint32_t sl = (l & 1u) | ((l & 2u) << 7) | ((l & 4u) << 14) | ((l & 8u) << 21);
-        // set -> 0x01, clear -> 0xFF, dead -> 0x00
-        q[n] = (0xFFFFFFFFu - 0xFEu * sb) & (sl * 0xFFu);
+    for (int n = 0; n < 4; ++n) q[n] = 0xFFFFFFFFu - 0xFEu * spread4((bits >> (4 * n)) & 0xFu);
+    if (live != 0xFFFFu) {
+#pragma unroll
+        for (int n = 0; n < 4; ++n) q[n] &= spread4((live >> (4 * n)) & 0xFu) * 0xFFu;
     }
     return make_uint4(q[0], q[1], q[2], q[3]);
 }

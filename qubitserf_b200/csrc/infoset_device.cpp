@@ -30,25 +30,6 @@ namespace {
 
 size_t al256(size_t x) { return (x + 255) / 256 * 256; }
 
-// f(0..n-1) on up to hardware_concurrency() threads (inline when small)
-template <class F>
-void parallel_for(size_t n, F f) {
-    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t th_n = std::min<size_t>({n, hw, 16});
-    if (th_n <= 1) {
-        for (size_t k = 0; k < n; ++k) f(k);
-        return;
-    }
-    std::atomic<size_t> next{0};
-    std::vector<std::thread> pool;
-    for (size_t t = 1; t < th_n; ++t)
-        pool.emplace_back([&]() {
-            for (size_t k; (k = next.fetch_add(1)) < n;) f(k);
-        });
-    for (size_t k; (k = next.fetch_add(1)) < n;) f(k);
-    for (auto& th : pool) th.join();
-}
-
 enum ItemState { kPending = 0, kDone = 1, kHost = 2, kClasses = 3 };
 
 struct Item {
@@ -108,10 +89,10 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes, 
     InfosetDesc* hd = (InfosetDesc*)(h + off_desc);
     std::memset(h + off_meta, 0, off_heap - off_meta);
     size_t nw1 = 0;
-    for (size_t i = 0; i < n; ++i) {
+    for (size_t i = 0; i < n; ++i) nw1 += items[i]->W == 1;
+    host_parallel_for(n, [&](size_t i) {
         const Item& it = *items[i];
         const Problem& p = *it.p;
-        nw1 += it.W == 1;
         u64* g = (u64*)(h + og[i]);
         for (int r = 0; r < it.K; ++r) std::memcpy(g + (size_t)r * it.W, p.code_gen.row(r), it.W * 8);
         u64* c = (u64*)(h + oc[i]);
@@ -140,10 +121,10 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes, 
         D.W32 = it.W32;
         D.SWP = it.SWP;
         hd[i] = D;
-    }
+    });
     unsigned long long* d_heap = (unsigned long long*)(d + off_heap);
     unsigned long long* d_ctr = (unsigned long long*)(d + off_ctr);
-    cudaStream_t st = s->urgent;
+    cudaStream_t st = s->urgent;   // the seed trials run beside it on `urgent2`
     const double tb = now_seconds();
     if (cudaMemcpyAsync(d, h, staged, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         launch_infosets(1, (const InfosetDesc*)(d + off_desc), (int)nw1, d_heap, d_ctr, st) !=
@@ -168,13 +149,13 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes, 
     }
     const u64* heap = heap_host.data();
     const double td = now_seconds();
-    for (size_t i = 0; i < n; ++i) {
+    host_parallel_for(n, [&](size_t i) {
         Item& it = *items[i];
         const InfosetMeta& M = *((const InfosetMeta*)(h + off_meta) + i);
         const int nsets = M.sets;
         if (nsets < 1 || nsets > kInfosetMaxSets || (classes && nsets != (int)it.lists.size())) {
             it.state = kHost;
-            continue;
+            return;
         }
         it.sets.assign(nsets, InfoSet());
         bool ok = true;
@@ -196,7 +177,7 @@ int run_pass(Session* s, Arena* arena, std::vector<Item*>& items, bool classes, 
             ok = ok && (int)S.pivots.size() == S.rank;
         }
         it.state = ok ? kDone : kHost;
-    }
+    });
     tm[0] += tb - ta;
     tm[1] += tc - tb;
     tm[2] += td - tc;
@@ -256,7 +237,7 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
         if (matroid_sets(it->p->code_gen, full_sets(it->sets, it->K), &it->lists, &it->class_ranks))
             it->state = (int)it->lists.size() <= kInfosetMaxSets ? kClasses : kHost;
     };
-    parallel_for(cand.size(), [&](size_t k) { decide(cand[k]); });
+    host_parallel_for(cand.size(), [&](size_t k) { decide(cand[k]); });
     pass.clear();
     for (Item* it : cand)
         if (it->state == kClasses) pass.push_back(it);
@@ -268,7 +249,7 @@ int device_infosets(Session* s, Arena* arena, const std::vector<BzSide*>& sides,
     int nhost = 0;
 
     std::atomic<int> arc{kOk};
-    parallel_for(items.size(), [&](size_t k) {   // host descriptions of the sets, per side
+    host_parallel_for(items.size(), [&](size_t k) {   // host descriptions of the sets, per side
         Item& it = items[k];
         BzSide& S = *it.side;
         S.sets_from_classes = it.state == kDone && !it.lists.empty();

@@ -3,12 +3,18 @@
 // host draws the column orders exactly as the reference does (std::mt19937 + std::shuffle
 // per stream); here one warp takes one trial: the K x n code generator (K <= 128 rows,
 // n <= 128 columns) sits in registers, row i on lane i%32 slot i/32, and is put in
-// restricted row-echelon form over the trial's column order with the reference's pivot rule
-// (first row at or below the rank with a 1 in the column, swapped into position `rank`,
-// then cleared from every other row).  The number of slots in use, S = ceil(K/32), is a
-// compile-time constant of the trial's body (one body per S, chosen per trial).  Per
-// column: the column index from a register by shuffle, one ballot per slot, one pivot
-// broadcast by shuffle, one masked XOR per slot.
+// reduced row-echelon form over the trial's column order.  The reference's pivot rule takes
+// the first row at or below the rank with a 1 in the column, swaps it into position `rank`
+// and clears the column from every other row.  The rows that result do not depend on which
+// candidate row is taken (the reduced row of each pivot column is unique), and row `rank`
+// of the reference's matrix is the one reduced on the rank-th pivot column.  So no row
+// moves here: the pivot is the first row not yet used as a pivot that has a 1 in the
+// column, and each row remembers the rank at which it became a pivot, its position in the
+// reference's matrix.  A row that is no pivot when the trial ends is zero in every column
+// (the code generator's rows are independent, so normally none is left).  The number of slots
+// in use, S = ceil(K/32), is a compile-time constant of the trial's body (one body per S,
+// chosen per trial).  Per column: the column index from a register by shuffle, one ballot
+// per slot, one pivot broadcast by shuffle, one masked XOR per slot.
 // The lightest logical nonzero row of every trial is folded into the side's 32-bit key
 // (weight:17 | trial:8 | row:7) with one atomicMin per warp.
 #include <cuda_runtime.h>
@@ -29,17 +35,6 @@ __device__ __forceinline__ void get_slot(const unsigned long long (&r)[S][W], in
         for (int q = 1; q < S; ++q)
             if (q == s) out[w] = r[q][w];
     }
-}
-
-template <int W, int S>
-__device__ __forceinline__ void put_slot(unsigned long long (&r)[S][W], int s,
-                                         const unsigned long long (&v)[W]) {
-#pragma unroll
-    for (int q = 0; q < S; ++q)
-        if (q == s) {
-#pragma unroll
-            for (int w = 0; w < W; ++w) r[q][w] = v[w];
-        }
 }
 
 // One trial with the K rows in S slots of 32 (K <= 32 S): S and W fixed at compile time,
@@ -63,41 +58,40 @@ __device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
         if (c < n) pw |= (uint32_t)__ldg(perm + c) << (8 * j);
     }
     int rank = 0;
+    uint32_t piv = 0u;   // bit s: row 32 s + lane is a pivot row
+    uint32_t pos = 0u;   // byte s: the rank at which it became one
     for (int ci = 0; ci < n && rank < K; ++ci) {
         const int col = (int)((__shfl_sync(0xffffffffu, pw, ci >> 2) >> (8 * (ci & 3))) & 0xffu);
         const int wd = col >> 6;
         const unsigned long long bit = 1ull << (col & 63);
-        // the first row at or below `rank` with a 1 in the column
+        // the first row, in row order, that is no pivot row yet and has a 1 in the column
         int sel = -1;
 #pragma unroll
         for (int s = S - 1; s >= 0; --s) {
             unsigned long long v = r[s][0];
 #pragma unroll
             for (int w = 1; w < W; ++w) if (w == wd) v = r[s][w];
-            unsigned m = __ballot_sync(0xffffffffu, (v & bit) != 0ull);
-            const int first = 32 * s;
-            if (rank >= first + 32) m = 0u;
-            else if (rank > first) m &= ~0u << (rank - first);
-            if (m) sel = first + __ffs(m) - 1;
+            const unsigned m =
+                __ballot_sync(0xffffffffu, (v & bit) != 0ull && ((piv >> s) & 1u) == 0u);
+            if (m) sel = 32 * s + __ffs(m) - 1;
         }
         if (sel < 0) continue;
-        const int ps = sel >> 5, pl = sel & 31, rs = rank >> 5, rl = rank & 31;
-        unsigned long long pv[W], ov[W], tmp[W];
+        const int ps = sel >> 5, pl = sel & 31;
+        unsigned long long pv[W], tmp[W];
         get_slot<W, S>(r, ps, tmp);
 #pragma unroll
         for (int w = 0; w < W; ++w) pv[w] = __shfl_sync(0xffffffffu, tmp[w], pl);
-        get_slot<W, S>(r, rs, tmp);
-#pragma unroll
-        for (int w = 0; w < W; ++w) ov[w] = __shfl_sync(0xffffffffu, tmp[w], rl);
-        if (lane == pl) put_slot<W, S>(r, ps, ov);   // old row `rank` moves to `sel`
-        if (lane == rl) put_slot<W, S>(r, rs, pv);   // pivot row moves to `rank`
+        if (lane == pl) {
+            piv |= 1u << ps;
+            pos |= (uint32_t)rank << (8 * ps);
+        }
+        // clear the column from every other row
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            const int row = 32 * s + lane;
             unsigned long long v = r[s][0];
 #pragma unroll
             for (int w = 1; w < W; ++w) if (w == wd) v = r[s][w];
-            if (row != rank && (v & bit)) {
+            if ((v & bit) && !(s == ps && lane == pl)) {
 #pragma unroll
                 for (int w = 0; w < W; ++w) r[s][w] ^= pv[w];
             }
@@ -109,8 +103,8 @@ __device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
     unsigned key = 0xffffffffu;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        const int row = 32 * s + lane;
-        if (row >= K) continue;
+        if (!((piv >> s) & 1u)) continue;   // not a pivot row: zero
+        const int row = (int)((pos >> (8 * s)) & 0xffu);   // its row in the reference's matrix
         int wt = 0;
 #pragma unroll
         for (int w = 0; w < W; ++w) wt += __popcll(r[s][w]);

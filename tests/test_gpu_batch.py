@@ -106,8 +106,9 @@ def test_full_1024_batch_matches_reference(native):
 def test_one_shot_pipeline_equals_single_batch(native):
     """qsfb_batch cuts batches of 256+ queries into chunks whose jobs join the running job
     groups at round boundaries (each chunk at whatever round its preparation ends); with
-    any chunk and group count the answers, levels and codeword counts equal one prepared
-    batch executed as a whole."""
+    any chunk and group count, and in the caller's order or the estimated-distance order
+    of the chunks, the answers, levels and codeword counts equal one prepared batch
+    executed as a whole."""
     import os
     from qubitserf_b200 import workloads as W
     items = native.batch_items(W.batch_1024(300))
@@ -118,9 +119,11 @@ def test_one_shot_pipeline_equals_single_batch(native):
     want = [(r.distance, r.lower_bound, r.proven, r.levels, r.z_weight, r.x_weight)
             for r in ref]
     try:
-        for chunks, groups in [("4", "3"), ("2", "1"), ("8", "4"), ("3", "2")]:
+        for chunks, groups, order in [("4", "3", "gv"), ("2", "1", "gv"), ("8", "4", "gv"),
+                                      ("3", "2", "gv"), ("3", "3", "index")]:
             os.environ["QSFB_BATCH_CHUNKS"] = chunks
             os.environ["QSFB_OVERLAP_GROUPS"] = groups
+            os.environ["QSFB_BATCH_ORDER"] = order
             ans, st = native.Batch(items).run()
             got = [(a.distance, a.lower_bound, a.proven, a.levels, a.z_weight, a.x_weight)
                    for a in ans]
@@ -131,6 +134,7 @@ def test_one_shot_pipeline_equals_single_batch(native):
     finally:
         os.environ.pop("QSFB_BATCH_CHUNKS", None)
         os.environ.pop("QSFB_OVERLAP_GROUPS", None)
+        os.environ.pop("QSFB_BATCH_ORDER", None)
 
 
 def test_job_groups_do_not_change_answers(native):
