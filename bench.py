@@ -438,6 +438,7 @@ def main():
             "bound": "tensor", "kernel": "pairs_tc_kernel",
             "achieved": tc_ops / 1e12, "peak": tc_peak / 1e12, "unit": "TOP/s (int8)",
             "frac": tc_ops / tc_peak, "traffic": tc_traffic,
+            "algorithmic_bytes_per_launch": tc_operand_bytes_per_launch(st1.tc_operand_bytes),
             "peak_source": ("2 x measured bf16 dense (MEASURED_PEAKS.json bf16_tflops, burst)"
                             if bf16 else "2 x fallback bf16 1.59 PFLOP/s"),
             "numerator": "tensor-core codewords x 128 int8 ops (64 columns) / kernel time",
@@ -454,7 +455,7 @@ def main():
             "bound": "int-pipe (POPC on the XU pipe)", "kernel": "pairs_kernel",
             "achieved": cc_cw_rate * popc_per_cw / 1e9, "peak": popc_peak / 1e9,
             "unit": "Gpopc32/s", "frac": cc_cw_rate * popc_per_cw / popc_peak,
-            "traffic": traffic_per_launch(),
+            "traffic": traffic_per_launch((cw - tc_cw) / max(args.steps, 1)),
             "numerator": "codewords/s of the pair kernel x 2W POPC32 of the full evaluation "
                          "(W = ceil(n/64)); the kernel issues fewer (pivot columns removed, "
                          "probe words, zero test)",
@@ -694,12 +695,29 @@ def tc_traffic_per_launch(tc_cw_per_step):
     return per_cw * tc_cw_per_step / launches
 
 
-def traffic_per_launch():
-    """DRAM bytes per pair-kernel launch from the committed ncu capture, or None."""
+def tc_operand_bytes_per_launch(operand_bytes_per_step):
+    """+-1 row bytes a tensor-core launch must read at least once (the union per round of the
+    row ranges each list serves), per launch of the statistics pass, for comparison with
+    the DRAM traffic per launch."""
+    p = ROOT / "profiles" / "pairs_tc_kernel_traffic.json"
+    if not p.exists():
+        return None
+    launches = json.loads(p.read_text()).get("launches_per_step_full_batch")
+    return operand_bytes_per_step / launches if launches else None
+
+
+def traffic_per_launch(cc_cw_per_step):
+    """DRAM bytes per CUDA-core pair launch: the committed per-codeword traffic of an ncu
+    capture on a smaller batch, scaled by the codewords of an average launch of this run."""
     p = ROOT / "profiles" / "pairs_kernel_traffic.json"
-    if p.exists():
-        return json.loads(p.read_text()).get("dram_bytes_per_launch")
-    return None
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    per_cw = d.get("dram_bytes_per_codeword")
+    launches = d.get("launches_per_step_full_batch")
+    if per_cw is None or not launches:
+        return None
+    return per_cw * cc_cw_per_step / launches
 
 
 def ctypes_sizeof_answers(n):

@@ -209,6 +209,9 @@ typedef struct {
     double tc_ms;                /* tensor-core sweep launches alone (CUDA events) */
     double device_sets_seconds;  /* information sets + packed rows on the device (copies,
                                     kernels, read-back, host partition step) */
+    unsigned long long tc_operand_bytes;  /* +-1 row bytes the tensor-core launches must read
+                                             at least once (per round, the union of the row
+                                             ranges of each list) */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free.  Batches of 256 queries or more are pipelined in

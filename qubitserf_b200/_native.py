@@ -75,7 +75,8 @@ class QsfbBatchStats(ctypes.Structure):
                 ("certificates", ctypes.c_int), ("device_bytes", ctypes.c_longlong),
                 ("gen_ms", ctypes.c_double), ("host_plan_seconds", ctypes.c_double),
                 ("host_apply_seconds", ctypes.c_double), ("tc_codewords", ctypes.c_ulonglong),
-                ("tc_ms", ctypes.c_double), ("device_sets_seconds", ctypes.c_double)]
+                ("tc_ms", ctypes.c_double), ("device_sets_seconds", ctypes.c_double),
+                ("tc_operand_bytes", ctypes.c_ulonglong)]
 
 
 class QsfbTiming(ctypes.Structure):

@@ -821,6 +821,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             stats->popc_issued += rs.popc_issued;
             stats->zero_codewords += rs.zero_codewords;
             stats->tc_codewords += rs.tc_codewords;
+            stats->tc_operand_bytes += rs.tc_operand_bytes;
             stats->launches += rs.launches;
         }
         if (jobs.size() == 1) {

@@ -358,6 +358,7 @@ int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_m
         rs->popc_issued += st[g].popc_issued;
         rs->zero_codewords += st[g].zero_codewords;
         rs->tc_codewords += st[g].tc_codewords;
+        rs->tc_operand_bytes += st[g].tc_operand_bytes;
         rs->launches += st[g].launches;
         *rounds = std::max(*rounds, rr[g]);
     }
@@ -442,6 +443,7 @@ void fill_exec_stats(const RunStats& rs, int rounds, double span, QsfbBatchStats
     stats->popc_issued = rs.popc_issued;
     stats->zero_codewords = rs.zero_codewords;
     stats->tc_codewords = rs.tc_codewords;
+    stats->tc_operand_bytes = rs.tc_operand_bytes;
     stats->rounds = rounds;
     stats->kernel_launches = rs.launches;
     stats->gen_ms = rs.ms_gen;
@@ -943,14 +945,11 @@ void qsfb_batch_free(QsfbBatchHandle* H) { delete H; }
 
 // One-shot batch.  A large batch is cut into chunks: the first (small, so the device
 // starts early) is prepared on all host cores and its rounds start; a helper thread
-// prepares the others in order (host reduction; seed eliminations and upload on its own
-// stream, beside the next chunk's host reduction) and publishes each to the running job
-// groups, which take their share of its jobs
-// at their next round boundary: the chunks' rounds merge into one execution with one tail.
-// Codes are independent and a job's answer depends only on its own levels, so the answers
-// are those of one batch.  1024-code batch, end to end: one piece 17.9-18.4k certs/s, two
-// chunks run one after the other 18.5-19.4k, merged (2-8 chunks, 3-4 groups) 20.0-20.7k;
-// separate job groups for the later chunks 17-19k; widest codes first no change.
+// prepares the others in order (host reduction, then the seed trials and information sets
+// on the device, beside the next chunk's host reduction) and publishes each to the running
+// job groups, which take their share of its jobs at their next round boundary: the chunks'
+// rounds merge into one execution with one tail.  Codes are independent and a job's answer
+// depends only on its own levels, so the answers are those of one batch.
 namespace {
 // Inverse of the binary entropy on [0, 1/2], to 1/8192: a table of H2 on that grid (made
 // once) and a binary search in it.

@@ -19,6 +19,7 @@ cudaError_t launch_pairs(int filt, int HP, int mode, const LevelDesc* d, int nd,
                          const unsigned long long* B, int num_sms, cudaStream_t st);
 cudaError_t launch_expand_pm(const ExpandDesc* d, int nd, unsigned long long total_rows,
                              int num_sms, cudaStream_t st);
+cudaError_t launch_zero_pads(int8_t* const* d_pads, int npads, int num_sms, cudaStream_t st);
 cudaError_t launch_pairs_tc(const LevelDesc* d, int nd, unsigned long long jobs,
                             const unsigned long long* B, void* job_recs, int* err, int num_sms,
                             cudaStream_t st);
@@ -664,7 +665,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     };
     std::vector<GenReq> gens;
     std::vector<ExpReq> exps;
-    std::vector<std::pair<int8_t*, size_t>> pad_zero;   // new +-1 buffers: zero their tail rows
+    std::vector<int8_t*> pad_zero;   // new +-1 buffers: their kPmPadRows tail rows, zeroed
     // the `queued` marks only live for this call, whatever path it leaves by
     struct ClearQueued {
         std::vector<GenReq>& g;
@@ -682,6 +683,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             }
         }
     } clear_queued{gens, exps};
+    // per list, the hull of the +-1 rows this call's tensor plans read (operand bytes)
+    std::unordered_map<const ListBuf*, std::pair<unsigned long long, unsigned long long>> tc_rows;
     for (Plan& P : plans) {
         SideDev* S = reqs[P.req].side;
         for (int side = 0; side < 2; ++side) {
@@ -723,14 +726,20 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 n_lo = 0;
                 n_hi = std::min(L.count, dev->binom(S->K - 1 - P.p_lo, P.b) + (unsigned long long)tcN);
             }
+            {
+                auto ins = tc_rows.emplace(&L, std::make_pair(n_lo, n_hi));
+                if (!ins.second) {
+                    ins.first->second.first = std::min(ins.first->second.first, n_lo);
+                    ins.first->second.second = std::max(ins.first->second.second, n_hi);
+                }
+            }
             if (L.pm_ready && n_lo >= L.pm_lo && n_hi <= L.pm_hi) continue;   // already written
             if (!L.pm) {
                 L.bytes_pm = (size_t)(L.count + kPmPadRows) * kPmRowBytes;
                 L.pm = (int8_t*)(L.arena ? S->arena->alloc(L.bytes_pm) : dev->alloc(L.bytes_pm));
                 if (!L.pm) return kErrMemory;
                 S->list_bytes += L.bytes_pm;
-                pad_zero.push_back({L.pm + (size_t)L.count * kPmRowBytes,
-                                    (size_t)kPmPadRows * kPmRowBytes});
+                pad_zero.push_back(L.pm + (size_t)L.count * kPmRowBytes);
             }
             const int nred = (int)S->nonpivot[P.g].size();
             const int n_enc = std::min(nred, kPmRowBytes);
@@ -868,6 +877,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     off = off + nplans * 8;
     const size_t off_err = off;
     off = align_up(off + 8, 64);
+    const size_t off_pads = off;                    // new +-1 lists' pad areas to zero
+    off = align_up(off + pad_zero.size() * sizeof(int8_t*), 64);
     const size_t total_bytes = off;                 // host-written part
     const size_t off_recs = off;                    // device-only: decoded tensor-core jobs
     off = align_up(off + tc_jobs * tc_job_record_bytes(), 64);
@@ -916,6 +927,9 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.n_enc = E.n_enc;
         exp_total += D.rows;
     }
+
+    int8_t** hpads = (int8_t**)(h + off_pads);
+    for (size_t i = 0; i < pad_zero.size(); ++i) hpads[i] = pad_zero[i];
 
     unsigned long long* hkeys = (unsigned long long*)(h + off_keys);
     for (size_t r = 0; r < reqs.size(); ++r)
@@ -998,11 +1012,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         cudaGetLastError();
         return kErrDevice;
     }
-    for (const auto& z : pad_zero)
-        if (cudaMemsetAsync(z.first, 0, z.second, st) != cudaSuccess) {
-            cudaGetLastError();
-            return kErrDevice;
-        }
+    // one launch for every new +-1 list's pad rows (a memset per list cost a launch each,
+    // thousands in a batch's first execution)
+    if (launch_zero_pads((int8_t* const*)(d + off_pads), (int)pad_zero.size(), dev->num_sms,
+                         st) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrDevice;
+    }
     cudaEventRecord(s->ev0, st);
     int launches = 0;
     if (!gens.empty()) {
@@ -1149,6 +1165,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         stats->popc_issued += popc;
         stats->zero_codewords += zcw;
         stats->tc_codewords += tcw;
+        for (const auto& kv : tc_rows)
+            stats->tc_operand_bytes += (kv.second.second - kv.second.first) * kPmRowBytes;
         stats->launches += launches;
     }
     cudaEventDestroy(evm);

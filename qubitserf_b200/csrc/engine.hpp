@@ -235,6 +235,9 @@ struct RunStats {
     unsigned long long popc_issued = 0;    // POPC the pair kernels issue (H per pair, 0 in zero mode)
     unsigned long long zero_codewords = 0; // codewords swept by the zero-test mode
     unsigned long long tc_codewords = 0;   // codewords swept by the tensor-core kernel
+    // +-1 row bytes the tensor-core launches must read at least once: per round, the union
+    // of the row ranges its tensor plans read from each list
+    unsigned long long tc_operand_bytes = 0;
     int launches = 0;
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)

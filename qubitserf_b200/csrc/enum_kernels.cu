@@ -17,6 +17,7 @@
 // words, tested against the detector syndromes and folded into the side's packed witness
 // key with one 64-bit atomicMin.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 
 #include "engine_types.hpp"
@@ -398,9 +399,27 @@ __global__ void __launch_bounds__(128) pairs_kernel(const LevelDesc* __restrict_
     }
 }
 
+// Zero the kPmPadRows rows after each new +-1 list (whole-tile operand copies read past a
+// list's last entry): one block per pad area per pass, 256 threads x 16 bytes per store.
+__global__ void __launch_bounds__(256) zero_pads_kernel(int8_t* const* __restrict__ pads,
+                                                        int npads) {
+    constexpr int kVecs = kPmPadRows * kPmRowBytes / 16;   // 16-byte stores per pad area
+    for (int p = blockIdx.x; p < npads; p += gridDim.x) {
+        uint4* o = reinterpret_cast<uint4*>(pads[p]);
+        for (int i = threadIdx.x; i < kVecs; i += blockDim.x) o[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
 }  // namespace dev
 
 // ---------------------------------------------------------------- host launchers
+cudaError_t launch_zero_pads(int8_t* const* d_pads, int npads, int num_sms, cudaStream_t st) {
+    if (npads <= 0) return cudaSuccess;
+    const int blocks = std::min(npads, num_sms * 8);
+    dev::zero_pads_kernel<<<blocks, 256, 0, st>>>(d_pads, npads);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gen_lists(const GenDesc* d_descs, int ndesc, unsigned long long total,
                              const unsigned long long* d_binom, int num_sms, cudaStream_t st) {
     if (total == 0) return cudaSuccess;   // total: runs of kGenRun entries
