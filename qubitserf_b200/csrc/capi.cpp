@@ -996,7 +996,10 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
     const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : tuning().batch_chunks, 64));
     std::vector<int> cut{0};
     if (nq >= kPipeMin && chunks > 1) {
-        const int first = std::max(32, nq / (2 * chunks));
+        const int fp = tuning().batch_first_permille;
+        const int first = std::min(nq - (chunks - 1),
+                                   std::max(32, fp > 0 ? (int)((long long)nq * fp / 1000)
+                                                       : nq / (2 * chunks)));
         cut.push_back(first);
         const int rest = nq - first, parts = chunks - 1;
         for (int i = 1; i <= parts; ++i) cut.push_back(first + (int)((long long)rest * i / parts));
@@ -1147,10 +1150,10 @@ int qsfb_tuning(char* out, int cap) {
         out, (size_t)cap,
         "tc_shape %d\ntc_job_tiles.small %d\ntc_job_tiles.large %d\ntc_small_tiles %lld\n"
         "cc_jobs_per_warp %d\ntc_cost_ratio %g\nexec_groups %d\nbatch_chunks %d\n"
-        "overlap_groups %d\nsource %s\n",
+        "overlap_groups %d\nbatch_first_permille %d\nsource %s\n",
         t.tc_shape, t.tc_job_tiles_small, t.tc_job_tiles_large, t.tc_small_tiles,
         t.cc_jobs_per_warp, t.tc_cost_ratio, t.exec_groups, t.batch_chunks, t.overlap_groups,
-        t.source.c_str());
+        t.batch_first_permille, t.source.c_str());
     return n < cap ? kOk : 7;
 }
 

@@ -20,20 +20,61 @@ __device__ __forceinline__ unsigned long long binom(const unsigned long long* __
     return __ldg(B + (size_t)n * kLd + k);
 }
 
+// log2(i!) and 1/i for the estimate in colex_top
+static __constant__ float kLog2Fact[kBinomMaxK + 1] = {
+    0.0f, 0.0f, 1.0f, 2.5849625f, 4.5849625f, 6.9068906f,
+    9.4918531f, 12.299208f, 15.299208f, 18.469133f, 21.7910611f, 25.2504927f,
+    28.8354552f, 32.535895f, 36.3432499f, 40.2501405f, 44.2501405f, 48.3376033f,
+    52.5075283f, 56.7554558f, 61.0773839f, 65.4697013f, 69.929133f, 74.4526949f,
+    79.0376574f, 83.6815136f, 88.3819533f, 93.1368408f, 97.9441958f, 102.802177f,
+    107.709067f, 112.663264f, 117.663264f, 122.707658f, 127.795121f, 132.924404f,
+    138.094329f, 143.303782f, 148.55171f, 153.837112f, 159.15904f, 164.516592f,
+    169.908909f, 175.335174f, 180.794606f, 186.286459f, 191.810021f, 197.36461f,
+    202.949572f, 208.564282f, 214.208138f, 219.880563f, 225.581003f, 231.308924f,
+    237.063811f, 242.845171f, 248.652526f, 254.485416f, 260.343397f, 266.22604f,
+    272.13293f, 278.063668f, 284.017864f, 289.995144f, 295.995144f};
+static __constant__ float kInvK[kBinomMaxK + 1] = {
+    0.0f, 1.0f, 0.5f, 0.333333333f, 0.25f, 0.2f,
+    0.166666667f, 0.142857143f, 0.125f, 0.111111111f, 0.1f, 0.0909090909f,
+    0.0833333333f, 0.0769230769f, 0.0714285714f, 0.0666666667f, 0.0625f, 0.0588235294f,
+    0.0555555556f, 0.0526315789f, 0.05f, 0.0476190476f, 0.0454545455f, 0.0434782609f,
+    0.0416666667f, 0.04f, 0.0384615385f, 0.037037037f, 0.0357142857f, 0.0344827586f,
+    0.0333333333f, 0.0322580645f, 0.03125f, 0.0303030303f, 0.0294117647f, 0.0285714286f,
+    0.0277777778f, 0.027027027f, 0.0263157895f, 0.0256410256f, 0.025f, 0.0243902439f,
+    0.0238095238f, 0.023255814f, 0.0227272727f, 0.0222222222f, 0.0217391304f, 0.0212765957f,
+    0.0208333333f, 0.0204081633f, 0.02f, 0.0196078431f, 0.0192307692f, 0.0188679245f,
+    0.0185185185f, 0.0181818182f, 0.0178571429f, 0.0175438596f, 0.0172413793f, 0.0169491525f,
+    0.0166666667f, 0.0163934426f, 0.0161290323f, 0.0158730159f, 0.015625f};
+
+// The largest x in [i-1, hi-1] with C(x, i) <= r (C(i-1, i) = 0, so one exists).  A binary
+// search costs ~log2(hi) dependent table reads; here C(x, i) ~ (x - (i-1)/2)^i / i! gives
+// the estimate x ~ (r i!)^(1/i) + (i-1)/2, and the exact answer is within a step or two of
+// it, found by walking up while C(x+1, i) <= r and down while C(x, i) > r (C is increasing
+// in x on [i-1, hi-1]; saturated entries compare as larger than any r).
+__device__ __forceinline__ int colex_top(const unsigned long long* __restrict__ B,
+                                         unsigned long long r, int i, int hi) {
+    int x;
+    if (i == 1) {
+        x = r < (unsigned long long)(hi - 1) ? (int)r : hi - 1;   // C(x, 1) = x
+        return x;
+    }
+    const float g = exp2f((log2f((float)r + 1.0f) + kLog2Fact[i]) * kInvK[i]) + 0.5f * (float)(i - 1);
+    x = g >= (float)(hi - 1) ? hi - 1 : (int)g;
+    x = x < i - 1 ? i - 1 : x;
+    while (x + 1 <= hi - 1 && binom(B, x + 1, i) <= r) ++x;
+    while (x > i - 1 && binom(B, x, i) > r) --x;
+    return x;
+}
+
 // Colex unrank: the r-th s-subset of [0, hi) in colex order, written largest first into
 // c[0..s-1] (c[0] > c[1] > ...).  r = sum_i C(c_i, s - i).
 __device__ __forceinline__ void colex_unrank(const unsigned long long* __restrict__ B,
                                              unsigned long long r, int s, int hi, int* c) {
     for (int i = s; i >= 1; --i) {
-        // largest x in [i-1, hi-1] with C(x, i) <= r
-        int lo = i - 1, top = hi - 1;
-        while (lo < top) {
-            const int mid = (lo + top + 1) >> 1;
-            if (binom(B, mid, i) <= r) lo = mid; else top = mid - 1;
-        }
-        c[s - i] = lo;
-        r -= binom(B, lo, i);
-        hi = lo;
+        const int x = colex_top(B, r, i, hi);   // largest x in [i-1, hi-1] with C(x, i) <= r
+        c[s - i] = x;
+        r -= binom(B, x, i);
+        hi = x;
     }
 }
 

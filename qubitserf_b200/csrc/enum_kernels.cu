@@ -73,11 +73,7 @@ __device__ __forceinline__ void gen_run_mask(const GenDesc& D, const unsigned lo
         unsigned long long r = e0;
         int hi = K;
         for (int i = s; i >= 1; --i) {   // colex unrank, largest element first
-            int lo = i - 1, top = hi - 1;
-            while (lo < top) {
-                const int mid = (lo + top + 1) >> 1;
-                if (binom(B, mid, i) <= r) lo = mid; else top = mid - 1;
-            }
+            const int lo = colex_top(B, r, i, hi);
             x |= (u128)1 << lo;
             r -= binom(B, lo, i);
             hi = lo;

@@ -25,16 +25,42 @@
 namespace qsfb {
 namespace dev {
 
-template <int W, int S>
-__device__ __forceinline__ void get_slot(const unsigned long long (&r)[S][W], int s,
-                                         unsigned long long (&out)[W]) {
+// One column of the elimination, with the column's word WD fixed at compile time: the
+// column is the same for the whole warp, so the caller branches on its word once instead
+// of every row selecting it.  Returns false when no row is left to pivot on.
+template <int W, int S, int WD>
+__device__ __forceinline__ bool eliminate_column(unsigned long long (&r)[S][W],
+                                                 unsigned long long bit, uint32_t& piv,
+                                                 uint32_t& pos, int rank, int lane) {
+    // the first row, in row order, that is no pivot row yet and has a 1 in the column
+    int sel = -1;
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-        out[w] = r[0][w];
-#pragma unroll
-        for (int q = 1; q < S; ++q)
-            if (q == s) out[w] = r[q][w];
+    for (int s = S - 1; s >= 0; --s) {
+        const unsigned m =
+            __ballot_sync(0xffffffffu, (r[s][WD] & bit) != 0ull && ((piv >> s) & 1u) == 0u);
+        if (m) sel = 32 * s + __ffs(m) - 1;
     }
+    if (sel < 0) return false;
+    const int ps = sel >> 5, pl = sel & 31;   // the same on every lane
+    unsigned long long pv[W];
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if (s == ps) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) pv[w] = __shfl_sync(0xffffffffu, r[s][w], pl);
+        }
+    if (lane == pl) {
+        piv |= 1u << ps;
+        pos |= (uint32_t)rank << (8 * ps);
+    }
+    // clear the column from every other row
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if ((r[s][WD] & bit) && !(s == ps && lane == pl)) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) r[s][w] ^= pv[w];
+        }
+    return true;
 }
 
 // One trial with the K rows in S slots of 32 (K <= 32 S): S and W fixed at compile time,
@@ -62,41 +88,11 @@ __device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
     uint32_t pos = 0u;   // byte s: the rank at which it became one
     for (int ci = 0; ci < n && rank < K; ++ci) {
         const int col = (int)((__shfl_sync(0xffffffffu, pw, ci >> 2) >> (8 * (ci & 3))) & 0xffu);
-        const int wd = col >> 6;
         const unsigned long long bit = 1ull << (col & 63);
-        // the first row, in row order, that is no pivot row yet and has a 1 in the column
-        int sel = -1;
-#pragma unroll
-        for (int s = S - 1; s >= 0; --s) {
-            unsigned long long v = r[s][0];
-#pragma unroll
-            for (int w = 1; w < W; ++w) if (w == wd) v = r[s][w];
-            const unsigned m =
-                __ballot_sync(0xffffffffu, (v & bit) != 0ull && ((piv >> s) & 1u) == 0u);
-            if (m) sel = 32 * s + __ffs(m) - 1;
-        }
-        if (sel < 0) continue;
-        const int ps = sel >> 5, pl = sel & 31;
-        unsigned long long pv[W], tmp[W];
-        get_slot<W, S>(r, ps, tmp);
-#pragma unroll
-        for (int w = 0; w < W; ++w) pv[w] = __shfl_sync(0xffffffffu, tmp[w], pl);
-        if (lane == pl) {
-            piv |= 1u << ps;
-            pos |= (uint32_t)rank << (8 * ps);
-        }
-        // clear the column from every other row
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            unsigned long long v = r[s][0];
-#pragma unroll
-            for (int w = 1; w < W; ++w) if (w == wd) v = r[s][w];
-            if ((v & bit) && !(s == ps && lane == pl)) {
-#pragma unroll
-                for (int w = 0; w < W; ++w) r[s][w] ^= pv[w];
-            }
-        }
-        ++rank;
+        const bool took = (W == 1 || col < 64)
+                              ? eliminate_column<W, S, 0>(r, bit, piv, pos, rank, lane)
+                              : eliminate_column<W, S, W - 1>(r, bit, piv, pos, rank, lane);
+        rank += took ? 1 : 0;
     }
 
     // lightest logical nonzero row of this trial
@@ -129,7 +125,7 @@ __device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
 }
 
 template <int W>
-__global__ void __launch_bounds__(64) seed_trials_kernel(const SeedDesc* __restrict__ descs,
+__global__ void __launch_bounds__(64, 16) seed_trials_kernel(const SeedDesc* __restrict__ descs,
                                                           int ndesc, int total_trials) {
     const int lane = threadIdx.x & 31;
     const int gt = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -155,9 +151,10 @@ __global__ void __launch_bounds__(64) seed_trials_kernel(const SeedDesc* __restr
 cudaError_t launch_seed_trials(int W, const SeedDesc* d_descs, int ndesc, int total_trials,
                                cudaStream_t st) {
     if (total_trials <= 0) return cudaSuccess;
-    // Blocks of two warps (64 x <= 48 registers): they fit in the registers a running
-    // tensor-core sweep CTA leaves free on its SM (640 threads x 96), so a preparation that
-    // overlaps the rounds starts at once instead of queueing behind the sweep's launch.
+    // Blocks of two warps (64 threads x at most 64 registers, the kernel's launch bound):
+    // they fit in the 4,096 registers a running tensor-core sweep CTA (640 threads x 96)
+    // leaves free on its SM, so a preparation that overlaps the rounds starts at once
+    // instead of queueing behind the sweep's launch.
     const int warps_per_block = 2;
     const int blocks = (total_trials + warps_per_block - 1) / warps_per_block;
     if (W == 1) dev::seed_trials_kernel<1><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);

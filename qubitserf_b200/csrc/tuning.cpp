@@ -27,6 +27,8 @@ bool set_key(Tuning& t, const std::string& key, const std::string& val) {
     else if (key == "exec_groups") t.exec_groups = (int)std::max(1ll, std::min(16ll, iv));
     else if (key == "batch_chunks") t.batch_chunks = (int)std::max(1ll, std::min(64ll, iv));
     else if (key == "overlap_groups") t.overlap_groups = (int)std::max(1ll, std::min(16ll, iv));
+    else if (key == "batch_first_permille")
+        t.batch_first_permille = (int)std::max(0ll, std::min(1000ll, iv));
     else return false;
     return true;
 }
@@ -59,7 +61,8 @@ Tuning load() {
     }
     static const char* const keys[] = {"tc_shape", "tc_job_tiles.small", "tc_job_tiles.large",
                                        "tc_small_tiles", "cc_jobs_per_warp", "tc_cost_ratio",
-                                       "exec_groups", "batch_chunks", "overlap_groups"};
+                                       "exec_groups", "batch_chunks", "overlap_groups",
+                                       "batch_first_permille"};
     for (const char* k : keys) {
         std::string name = "QSFB_TUNE_";
         for (const char* c = k; *c; ++c) name += *c == '.' ? '_' : (char)std::toupper(*c);

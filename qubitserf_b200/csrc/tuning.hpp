@@ -19,6 +19,9 @@ struct Tuning {
     double tc_cost_ratio = 0.6;        // tensor plan when its cost < ratio x CUDA-core cost
     int exec_groups = 3;               // interleaved job groups of qsfb_batch_execute
     int batch_chunks = 4;              // pipeline chunks of the one-shot qsfb_batch
+    // the first chunk's share of the batch in 1/1000 (0: half a chunk, nq / (2 chunks));
+    // it is prepared before any round starts
+    int batch_first_permille = 0;
     int overlap_groups = 3;            // job groups of the one-shot qsfb_batch
     std::string source = "defaults";   // where the values came from
 };

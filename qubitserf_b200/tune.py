@@ -45,6 +45,7 @@ RESIDENT_KNOBS = [
 E2E_KNOBS = [
     ("batch_chunks", [4, 1, 2, 3, 6]),
     ("overlap_groups", [3, 2, 4]),
+    ("batch_first_permille", [0, 31, 62, 250]),
 ]
 DEFAULTS = {k: v[0] for k, v in RESIDENT_KNOBS + E2E_KNOBS}
 

@@ -384,7 +384,8 @@ def test_tuning_table_and_overrides(native, tmp_path):
     import json
     table = tmp_path / "t.txt"
     table.write_text("# comment\ntc_shape 0\ntc_job_tiles.large 8  # trailing\n"
-                     "cc_jobs_per_warp 9999\nbogus 3\ntc_cost_ratio x\nbatch_chunks 6\n")
+                     "cc_jobs_per_warp 9999\nbogus 3\ntc_cost_ratio x\nbatch_chunks 6\n"
+                     "batch_first_permille 5000\n")
     code = ("import sys, json; sys.path.insert(0, sys.argv[1]); "
             "from qubitserf_b200 import _native as N; print(json.dumps(N.tuning()))")
     env = dict(os.environ, QSFB_TUNING=str(table), QSFB_TUNE_EXEC_GROUPS="2",
@@ -395,6 +396,7 @@ def test_tuning_table_and_overrides(native, tmp_path):
     t = json.loads(p.stdout.strip().splitlines()[-1])
     assert (t["tc_shape"], t["tc_job_tiles.large"], t["batch_chunks"]) == (0, 8, 6)
     assert t["cc_jobs_per_warp"] == 256 and t["tc_cost_ratio"] == 0.6   # clamped / kept
+    assert t["batch_first_permille"] == 1000                              # clamped
     assert (t["exec_groups"], t["tc_job_tiles.small"]) == (2, 4)
     assert str(table) in t["source"] and "QSFB_TUNE_EXEC_GROUPS" in t["source"]
     env = dict(os.environ, QSFB_TUNING=str(tmp_path / "absent.txt"))
