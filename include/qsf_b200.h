@@ -212,6 +212,8 @@ typedef struct {
     unsigned long long tc_operand_bytes;  /* +-1 row bytes the tensor-core launches must read
                                              at least once (per round, the union of the row
                                              ranges of each list) */
+    unsigned long long list_bytes_written;  /* bytes the list generation must write (probe
+                                               words, pivot counts, +-1 rows) */
 } QsfbBatchStats;
 
 /* One-shot: prepare + execute + free.  Batches of 256 queries or more are pipelined in

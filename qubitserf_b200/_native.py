@@ -76,7 +76,8 @@ class QsfbBatchStats(ctypes.Structure):
                 ("gen_ms", ctypes.c_double), ("host_plan_seconds", ctypes.c_double),
                 ("host_apply_seconds", ctypes.c_double), ("tc_codewords", ctypes.c_ulonglong),
                 ("tc_ms", ctypes.c_double), ("device_sets_seconds", ctypes.c_double),
-                ("tc_operand_bytes", ctypes.c_ulonglong)]
+                ("tc_operand_bytes", ctypes.c_ulonglong),
+                ("list_bytes_written", ctypes.c_ulonglong)]
 
 
 class QsfbTiming(ctypes.Structure):

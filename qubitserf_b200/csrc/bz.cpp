@@ -822,6 +822,7 @@ int run_rounds(Session* s, std::vector<BzJob*>& jobs, RunStats* stats, int* roun
             stats->zero_codewords += rs.zero_codewords;
             stats->tc_codewords += rs.tc_codewords;
             stats->tc_operand_bytes += rs.tc_operand_bytes;
+            stats->list_bytes_written += rs.list_bytes_written;
             stats->launches += rs.launches;
         }
         if (jobs.size() == 1) {

@@ -359,6 +359,7 @@ int execute_groups(QsfbBatchHandle* H, RunStats* rs, int* rounds, double* span_m
         rs->zero_codewords += st[g].zero_codewords;
         rs->tc_codewords += st[g].tc_codewords;
         rs->tc_operand_bytes += st[g].tc_operand_bytes;
+        rs->list_bytes_written += st[g].list_bytes_written;
         rs->launches += st[g].launches;
         *rounds = std::max(*rounds, rr[g]);
     }
@@ -444,6 +445,7 @@ void fill_exec_stats(const RunStats& rs, int rounds, double span, QsfbBatchStats
     stats->zero_codewords = rs.zero_codewords;
     stats->tc_codewords = rs.tc_codewords;
     stats->tc_operand_bytes = rs.tc_operand_bytes;
+    stats->list_bytes_written = rs.list_bytes_written;
     stats->rounds = rounds;
     stats->kernel_launches = rs.launches;
     stats->gen_ms = rs.ms_gen;

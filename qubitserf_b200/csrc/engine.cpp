@@ -890,6 +890,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
 
     GenDesc* hg = (GenDesc*)(h + off_gen);
     unsigned long long gen_total = 0;
+    unsigned long long list_written = 0;   // algorithmic bytes of the list generation
     for (size_t i = 0; i < gens.size(); ++i) {
         const GenReq& G = gens[i];
         ListBuf& L = G.S->lists[std::make_tuple(G.g, G.size, G.reflect)];
@@ -910,6 +911,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.rank = G.S->ranks[G.g];
         D.reflect = G.reflect;
         gen_total += (L.count + kGenRun - 1) / kGenRun;
+        list_written += L.count * (unsigned long long)G.HP * 4 + (L.pc ? L.count : 0) +
+                        (G.pm ? (G.pm_hi - G.pm_lo) * kPmRowBytes : 0);
     }
     ExpandDesc* he = (ExpandDesc*)(h + off_exp);
     unsigned long long exp_total = 0;
@@ -926,6 +929,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.HP = E.HP;
         D.n_enc = E.n_enc;
         exp_total += D.rows;
+        list_written += D.rows * kPmRowBytes;
     }
 
     int8_t** hpads = (int8_t**)(h + off_pads);
@@ -1165,6 +1169,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         stats->popc_issued += popc;
         stats->zero_codewords += zcw;
         stats->tc_codewords += tcw;
+        stats->list_bytes_written += list_written;
         for (const auto& kv : tc_rows)
             stats->tc_operand_bytes += (kv.second.second - kv.second.first) * kPmRowBytes;
         stats->launches += launches;

@@ -238,6 +238,9 @@ struct RunStats {
     // +-1 row bytes the tensor-core launches must read at least once: per round, the union
     // of the row ranges its tensor plans read from each list
     unsigned long long tc_operand_bytes = 0;
+    // bytes the list generation must write: probe words, pivot counts and +-1 rows of the
+    // generated lists, +-1 rows added to earlier lists
+    unsigned long long list_bytes_written = 0;
     int launches = 0;
     double host_setup_s = 0.0;
     double device_seed_s = 0.0;   // wall time of the device seed phase (copy + kernel)

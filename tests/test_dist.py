@@ -71,7 +71,7 @@ def test_reference_arm_under_torchrun():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"),
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
-           "--codes", "64", "--ref-budget", "1"]
+           "--codes", "64", "--ref-stride", "64"]
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=str(ROOT))
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
