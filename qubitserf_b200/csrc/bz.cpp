@@ -543,6 +543,7 @@ struct SeedLaunch {
     const unsigned* d_keys = nullptr;
     cudaStream_t st = nullptr;
     bool launched = false;
+    int launches = 0;
     double t0 = 0.0;
 };
 
@@ -551,11 +552,11 @@ struct SeedLaunch {
 // may use the main staging while the trials run.
 int seeds_begin(Session* s, Arena* arena, std::vector<BzJob*>& jobs, SeedLaunch* L) {
     L->t0 = now_seconds();
-    std::vector<BzSide*> pend[3];   // by row words W = 1, 2
+    std::vector<BzSide*> pend[5];   // by row words W = 1 .. 4
     for (BzJob* j : jobs)
         for (int i = 0; i < (j->pair ? 2 : 1); ++i)
             if (j->s[i].seed_pending) pend[words_for(j->s[i].prob->n)].push_back(&j->s[i]);
-    for (int W = 1; W <= 2; ++W) L->sides.insert(L->sides.end(), pend[W].begin(), pend[W].end());
+    for (int W = 1; W <= 4; ++W) L->sides.insert(L->sides.end(), pend[W].begin(), pend[W].end());
     const size_t n = L->sides.size();
     if (n == 0) return kOk;
     // layout: keys (all sides) | descs (all sides, W = 1 first) | per side: gen, check |
@@ -588,7 +589,7 @@ int seeds_begin(Session* s, Arena* arena, std::vector<BzJob*>& jobs, SeedLaunch*
     char* h = (char*)s->h_seed.h;
     SeedDesc* hd = (SeedDesc*)(h + off_desc);
     unsigned* hk = (unsigned*)(h + off_keys);
-    int trials[3] = {0, 0, 0};
+    int trials[5] = {0, 0, 0, 0, 0};
     for (size_t i = 0; i < n; ++i) {
         const BzSide& S = *L->sides[i];
         const Problem& p = *S.prob;
@@ -617,7 +618,6 @@ int seeds_begin(Session* s, Arena* arena, std::vector<BzJob*>& jobs, SeedLaunch*
     for (const auto& po : perm_off) std::memcpy(h + po.second, po.first->data(), po.first->size());
     // on a stream above the rounds' priority: in a pipelined batch or a server, the rounds
     // of other codes fill the SMs meanwhile, and these codes wait for the result
-    const size_t n1 = pend[1].size();
     const SeedDesc* dd = (const SeedDesc*)(d + off_desc);
     // the keys' read-back is queued by seeds_end: queued here, behind the trials, it would
     // hold back every later device-to-host copy of the preparation on the same copy engine
@@ -625,10 +625,16 @@ int seeds_begin(Session* s, Arena* arena, std::vector<BzJob*>& jobs, SeedLaunch*
     L->keys = hk;
     L->d_keys = (const unsigned*)(d + off_keys);
     L->launched = true;
-    if (cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, L->st) != cudaSuccess ||
-        (n1 > 0 && launch_seed_trials(1, dd, (int)n1, trials[1], L->st) != cudaSuccess) ||
-        (n > n1 && launch_seed_trials(2, dd + n1, (int)(n - n1), trials[2], L->st) !=
-                       cudaSuccess)) {
+    bool ok = cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, L->st) == cudaSuccess;
+    size_t first = 0;   // descriptors are grouped by W, W = 1 first
+    for (int W = 1; W <= 4 && ok; ++W) {
+        const size_t nw = pend[W].size();
+        if (nw > 0)
+            ok = launch_seed_trials(W, dd + first, (int)nw, trials[W], L->st) == cudaSuccess;
+        first += nw;
+        L->launches += nw > 0 ? 1 : 0;
+    }
+    if (!ok) {
         cudaGetLastError();
         cudaStreamSynchronize(L->st);
         cudaGetLastError();
@@ -651,8 +657,7 @@ int seeds_end(std::vector<BzJob*>& jobs, SeedLaunch* L, RunStats* stats) {
         }
         if (stats) {
             stats->device_seed_wait_s += now_seconds() - tw0;
-            stats->launches += 1 + (words_for(L->sides.front()->prob->n) !=
-                                    words_for(L->sides.back()->prob->n));
+            stats->launches += L->launches;
         }
         for (size_t i = 0; i < L->sides.size(); ++i) L->sides[i]->apply_device_seed(L->keys[i]);
     }

@@ -29,7 +29,9 @@ struct BzOptions {
     bool no_early_stop = false;  // enumerate every level up to K (single sides; count parity)
     int seed_trials = 256;
     bool parallel_seed = true;   // host seed trials on hardware_concurrency threads
-    bool device_seed = true;     // eliminations of the seed trials on the GPU when K, n <= 128
+    // eliminations of the seed trials on the GPU when K <= 128 and n <= 256 (QSFB_HOST_SEEDS=1:
+    // on the host threads, with the same streams and results)
+    bool device_seed = std::getenv("QSFB_HOST_SEEDS") == nullptr;
     // information sets (and the packed rows) built on the GPU when K, n <= 128;
     // QSFB_HOST_INFOSETS=1 builds them on the host instead (same results)
     bool device_infosets = std::getenv("QSFB_HOST_INFOSETS") == nullptr;

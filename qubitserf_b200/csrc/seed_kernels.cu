@@ -2,7 +2,7 @@
 // reference's random_is_seed (cpp/distfind/bz.cpp:24-70, the trial loop at :36-51).  The
 // host draws the column orders exactly as the reference does (std::mt19937 + std::shuffle
 // per stream); here one warp takes one trial: the K x n code generator (K <= 128 rows,
-// n <= 128 columns) sits in registers, row i on lane i%32 slot i/32, and is put in
+// n <= 256 columns, W = ceil(n/64) words per row) sits in registers, row i on lane i%32 slot i/32, and is put in
 // reduced row-echelon form over the trial's column order.  The reference's pivot rule takes
 // the first row at or below the rank with a 1 in the column, swaps it into position `rank`
 // and clears the column from every other row.  The rows that result do not depend on which
@@ -75,23 +75,36 @@ __device__ __forceinline__ void run_trial(const SeedDesc& D, int t, int lane) {
 #pragma unroll
         for (int w = 0; w < W; ++w) r[s][w] = row < K ? __ldg(D.gen + (size_t)row * W + w) : 0ull;
     }
-    // the trial's column order (n <= 128 bytes): bytes 4 lane .. 4 lane + 3 on this lane
+    // the trial's column order: bytes PB lane .. PB lane + PB - 1 on this lane (PB = 4 for
+    // n <= 128, 8 for n <= 256)
+    constexpr int PB = W <= 2 ? 4 : 8;
     const uint8_t* perm = D.perm + (size_t)t * n;
-    uint32_t pw = 0;
+    uint32_t pw[PB / 4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int c = 4 * lane + j;
-        if (c < n) pw |= (uint32_t)__ldg(perm + c) << (8 * j);
+    for (int j = 0; j < PB / 4; ++j) pw[j] = 0u;
+#pragma unroll
+    for (int j = 0; j < PB; ++j) {
+        const int c = PB * lane + j;
+        if (c < n) pw[j >> 2] |= (uint32_t)__ldg(perm + c) << (8 * (j & 3));
     }
     int rank = 0;
     uint32_t piv = 0u;   // bit s: row 32 s + lane is a pivot row
     uint32_t pos = 0u;   // byte s: the rank at which it became one
     for (int ci = 0; ci < n && rank < K; ++ci) {
-        const int col = (int)((__shfl_sync(0xffffffffu, pw, ci >> 2) >> (8 * (ci & 3))) & 0xffu);
+        const uint32_t src = PB == 4 ? pw[0] : pw[(ci >> 2) & (PB / 4 - 1)];   // uniform
+        const int col =
+            (int)((__shfl_sync(0xffffffffu, src, ci / PB) >> (8 * (ci & 3))) & 0xffu);
         const unsigned long long bit = 1ull << (col & 63);
-        const bool took = (W == 1 || col < 64)
-                              ? eliminate_column<W, S, 0>(r, bit, piv, pos, rank, lane)
-                              : eliminate_column<W, S, W - 1>(r, bit, piv, pos, rank, lane);
+        const int wd = W == 1 ? 0 : col >> 6;   // the column's word, uniform over the warp
+        bool took;
+        if (W == 1 || wd == 0)
+            took = eliminate_column<W, S, 0>(r, bit, piv, pos, rank, lane);
+        else if (W == 2 || wd == 1)
+            took = eliminate_column<W, S, (W > 1 ? 1 : 0)>(r, bit, piv, pos, rank, lane);
+        else if (W == 3 || wd == 2)
+            took = eliminate_column<W, S, (W > 2 ? 2 : 0)>(r, bit, piv, pos, rank, lane);
+        else
+            took = eliminate_column<W, S, (W > 3 ? 3 : 0)>(r, bit, piv, pos, rank, lane);
         rank += took ? 1 : 0;
     }
 
@@ -159,6 +172,8 @@ cudaError_t launch_seed_trials(int W, const SeedDesc* d_descs, int ndesc, int to
     const int blocks = (total_trials + warps_per_block - 1) / warps_per_block;
     if (W == 1) dev::seed_trials_kernel<1><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);
     else if (W == 2) dev::seed_trials_kernel<2><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);
+    else if (W == 3) dev::seed_trials_kernel<3><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);
+    else if (W == 4) dev::seed_trials_kernel<4><<<blocks, 64, 0, st>>>(d_descs, ndesc, total_trials);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
