@@ -396,10 +396,12 @@ def main():
     for _ in range(max(1, min(args.warmup, 2))):
         batch.run()
     e2e_t = []
+    alloc0 = _native.alloc_counters()
     for _ in range(args.steps):
         t = time.perf_counter()
         ans2, st2 = batch.run()
         e2e_t.append(time.perf_counter() - t)
+    alloc1 = _native.alloc_counters()
     assert [a.distance for a in ans2] == dists
     e2e_s = max_over_ranks(pg, sum(e2e_t))
     e2e = units * args.steps / e2e_s
@@ -495,6 +497,11 @@ def main():
                 "prepare_s": st2.prepare_seconds, "host_setup_s": host_setup,
                 "device_seed_s": st2.device_seed_seconds,
                 "rounds_span_s": st2.device_span_ms / 1e3,
+                "calls_ms": [round(x * 1e3, 2) for x in e2e_t],
+                "driver_allocations": {"device": alloc1[0] - alloc0[0],
+                                       "device_s": alloc1[1] - alloc0[1],
+                                       "pinned": alloc1[2] - alloc0[2],
+                                       "pinned_s": alloc1[3] - alloc0[3]},
                 "note": "last call: prepare/host_setup/device_seed summed over the pipeline "
                         "chunks (all but the first overlap the rounds); rounds_span_s is the "
                         "merged rounds' device span"},

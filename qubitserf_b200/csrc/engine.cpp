@@ -657,6 +657,19 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         bool pm;
         int n_enc;
         unsigned long long pm_lo, pm_hi;
+        const ListBuf* src = nullptr;   // complete list one size smaller (built from it)
+    };
+    // The list one size smaller of the same set and orientation, when an earlier round left
+    // it complete (ready and not being rebuilt in this call): the new list is built from it
+    // by one XOR per entry instead of unranking.  Its pivot counts are needed when the new
+    // list stores them.
+    auto smaller_list = [](SideDev* S, int g, int size, int side, bool full) -> const ListBuf* {
+        if (size < 2) return nullptr;
+        auto it = S->lists.find(std::make_tuple(g, size - 1, side));
+        if (it == S->lists.end()) return nullptr;
+        const ListBuf& L = it->second;
+        if (!L.ready || L.queued || !L.words || (!full && !L.pc)) return nullptr;
+        return &L;
     };
     struct ExpReq {
         SideDev* S;
@@ -696,7 +709,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                 if (L.words) {   // allocated by an earlier execution: regenerate in place
                     L.queued = true;
                     L.gen_idx = (int)gens.size();
-                    gens.push_back({S, P.g, size, side, P.HP, false, 0, 0, 0});
+                    gens.push_back({S, P.g, size, side, P.HP, false, 0, 0, 0,
+                                    smaller_list(S, P.g, size, side, P.full)});
                 } else {
                     L.queued = true;
                     L.count = dev->binom(S->K, size);
@@ -711,7 +725,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
                     }
                     S->list_bytes += L.bytes_w + L.bytes_pc;
                     L.gen_idx = (int)gens.size();
-                    gens.push_back({S, P.g, size, side, P.HP, false, 0, 0, 0});
+                    gens.push_back({S, P.g, size, side, P.HP, false, 0, 0, 0,
+                                    smaller_list(S, P.g, size, side, P.full)});
                 }
             }
             if (!P.tc) continue;
@@ -910,6 +925,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         D.HP = G.HP;
         D.rank = G.S->ranks[G.g];
         D.reflect = G.reflect;
+        D.src = G.src ? G.src->words : nullptr;
+        D.src_pc = G.src ? G.src->pc : nullptr;
         gen_total += (L.count + kGenRun - 1) / kGenRun;
         list_written += L.count * (unsigned long long)G.HP * 4 + (L.pc ? L.count : 0) +
                         (G.pm ? (G.pm_hi - G.pm_lo) * kPmRowBytes : 0);

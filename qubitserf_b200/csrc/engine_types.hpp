@@ -78,6 +78,11 @@ struct GenDesc {
     unsigned long long entry_base;  // first global run (kGenRun entries) of this descriptor
     unsigned long long count;
     unsigned long long pm_lo, pm_hi;  // entries whose +-1 rows are written (pm only)
+    // the complete list one size smaller of the same set and orientation (HP words per
+    // entry, and its pivot counts when `pc` is written), or null: entries are then built
+    // from it instead of by unranking
+    const uint32_t* src;
+    const uint8_t* src_pc;
     int K, size, W32, HP, rank, reflect;
     int n_enc;                // live +-1 columns (pm only)
     int pad_;

@@ -114,6 +114,45 @@ __device__ __forceinline__ void gen_run_mask(const GenDesc& D, const unsigned lo
     }
 }
 
+// Lists built from the list one size smaller of the same set and orientation.  In colex
+// order the s-subsets whose largest element is c come as one block, after the C(c, s)
+// subsets of [0, c), and in the order of their other s-1 elements, which are exactly the
+// first C(c, s-1) entries of the smaller list.  So entry C(c, s) + j is entry j of the
+// smaller list with row c added: its probe words the smaller entry's XOR row c, its pivot
+// count the smaller entry's plus one when row c is a pivot row.  Only the run's first
+// entry is located (its largest element, by colex_top); the rest stream through the
+// smaller list.
+__device__ __forceinline__ void gen_run_rec(const GenDesc& D, const unsigned long long* B,
+                                            unsigned long long e0, int n) {
+    const int s = D.size, K = D.K;
+    int c = colex_top(B, e0, s, K);
+    unsigned long long j = e0 - binom(B, c, s);
+    unsigned long long blk = binom(B, c, s - 1);   // entries whose largest element is c
+    for (int k = 0; k < n; ++k) {
+        while (j >= blk) {   // into the next block (blk >= 1: c >= s - 1)
+            j -= blk;
+            ++c;
+            blk = binom(B, c, s - 1);
+        }
+        const int row = D.reflect ? K - 1 - c : c;
+        uint32_t acc[4] = {0u, 0u, 0u, 0u};
+        const uint32_t* in = D.src + j * (unsigned long long)D.HP;
+        if (D.HP == 4) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(in));
+            acc[0] = q.x; acc[1] = q.y; acc[2] = q.z; acc[3] = q.w;
+        } else if (D.HP == 2) {
+            const uint2 q = __ldg(reinterpret_cast<const uint2*>(in));
+            acc[0] = q.x; acc[1] = q.y;
+        } else {
+            acc[0] = __ldg(in);
+        }
+        xor_row(D, row, acc);
+        const int pc = D.src_pc ? (int)__ldg(D.src_pc + j) + (row < D.rank ? 1 : 0) : 0;
+        put_entry(D, e0 + k, acc, pc);
+        ++j;
+    }
+}
+
 __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restrict__ descs,
                                                         int ndesc, unsigned long long total,
                                                         const unsigned long long* __restrict__ B) {
@@ -128,6 +167,10 @@ __global__ void __launch_bounds__(256) gen_lists_kernel(const GenDesc* __restric
         const GenDesc& D = descs[lo];
         const unsigned long long e0 = (gr - D.entry_base) * kGenRun;
         const int n = (int)(D.count - e0 < (unsigned long long)kGenRun ? D.count - e0 : kGenRun);
+        if (D.src) {
+            gen_run_rec(D, B, e0, n);
+            continue;
+        }
         if (D.K <= 128) {
             gen_run_mask(D, B, e0, n);
             continue;
