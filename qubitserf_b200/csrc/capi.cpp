@@ -1151,10 +1151,11 @@ int qsfb_tuning(char* out, int cap) {
     const int n = std::snprintf(
         out, (size_t)cap,
         "tc_shape %d\ntc_job_tiles.small %d\ntc_job_tiles.large %d\ntc_small_tiles %lld\n"
-        "cc_jobs_per_warp %d\ntc_cost_ratio %g\nexec_groups %d\nbatch_chunks %d\n"
+        "cc_jobs_per_warp %d\ntc_cost_ratio %g\ntc_edge_div %d\nexec_groups %d\nbatch_chunks %d\n"
         "overlap_groups %d\nbatch_first_permille %d\nsource %s\n",
         t.tc_shape, t.tc_job_tiles_small, t.tc_job_tiles_large, t.tc_small_tiles,
-        t.cc_jobs_per_warp, t.tc_cost_ratio, t.exec_groups, t.batch_chunks, t.overlap_groups,
+        t.cc_jobs_per_warp, t.tc_cost_ratio, t.tc_edge_div, t.exec_groups, t.batch_chunks,
+        t.overlap_groups,
         t.batch_first_permille, t.source.c_str());
     return n < cap ? kOk : 7;
 }

@@ -544,6 +544,10 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     //    the terms whose rectangles fill the MMA tiles and CUDA-core plans for the rest
     std::vector<Plan> plans;
     unsigned long long cc_pairs = 0;
+    // QSFB_DEBUG=5: pairs of this call by sweep and by why a plan stays on the CUDA cores
+    // (rank-deficient, zero test, one probe word, no second list, list over 2^28 entries,
+    // the cost model, the terms outside the tensor range)
+    unsigned long long why[8] = {0, 0, 0, 0, 0, 0, 0, 0}, tc_sum = 0;
     for (size_t r = 0; r < reqs.size(); ++r) {
         const LevelReq& q = reqs[r];
         SideDev* S = q.side;
@@ -554,22 +558,25 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         int a, b;
         level_split(pairs, w, &a, &b);
         // tensor-core term range of this level (the same for every set): terms whose
-        // rectangles keep at least half of every tile busy; nx grows and ny shrinks with p
+        // rectangles fill at least 1/div of a tile's rows and of its columns (div from the
+        // tuning table, 2 by default); nx grows and ny shrinks with p
         int p1 = -1, p2 = -1;
         unsigned long long tc_pairs = 0, lo_pairs = 0, hi_pairs = 0;
         bool range_done = false;
         auto tc_range = [&]() {
             range_done = true;
             const int plo = a - 1, pend = K - b;   // terms p in [plo, pend)
-            int lo = plo, hi = pend;               // first p with nx >= tcM / 2
+            const int div = tuning().tc_edge_div;
+            const unsigned long long min_rows = std::max(1, tcM / div), min_cols = std::max(1, tcN / div);
+            int lo = plo, hi = pend;               // first p with nx >= min_rows
             while (lo < hi) {
                 const int mid = (lo + hi) / 2;
-                if (dev->binom(mid, a - 1) >= (unsigned long long)(tcM / 2)) hi = mid; else lo = mid + 1;
+                if (dev->binom(mid, a - 1) >= min_rows) hi = mid; else lo = mid + 1;
             }
-            int l2 = plo - 1, h2 = pend - 1;       // last p with ny >= tcN / 2
+            int l2 = plo - 1, h2 = pend - 1;       // last p with ny >= min_cols
             while (l2 < h2) {
                 const int mid = (l2 + h2 + 1) / 2;
-                if (dev->binom(K - 1 - mid, b) >= (unsigned long long)(tcN / 2)) l2 = mid; else h2 = mid - 1;
+                if (dev->binom(K - 1 - mid, b) >= min_cols) l2 = mid; else h2 = mid - 1;
             }
             if (lo > l2) return;
             p1 = lo;
@@ -610,8 +617,16 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             if (ks == 0 || p1 < 0) {
                 P.range_pairs = pairs;
                 cc_pairs += pairs;
+                if (debug_level() == 5)
+                    why[!P.full ? 0 : P.mode == 2 ? 1 : P.HP < 2 ? 2 : b == 0 ? 3
+                        : (dev->binom(K, a) >= (1ull << 28) || dev->binom(K, b) >= (1ull << 28)) ? 4
+                        : ks == 0 ? 5 : 6] += pairs;
                 plans.push_back(std::move(P));
                 continue;
+            }
+            if (debug_level() == 5) {
+                why[6] += lo_pairs + hi_pairs;
+                tc_sum += tc_pairs;
             }
             const int p_end = P.p_lo + P.nterms;   // one past the last term
             Plan TP = P;
@@ -639,6 +654,10 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             plans.push_back(std::move(TP));
         }
     }
+    if (debug_level() == 5)
+        std::fprintf(stderr, "qsfb plan pairs: tc %llu | cc rank-deficient %llu zero-test %llu "
+                     "one-word %llu one-list %llu big-list %llu cost-model %llu edge-terms %llu\n",
+                     tc_sum, why[0], why[1], why[2], why[3], why[4], why[5], why[6]);
     // loop tile: enough jobs to keep every resident warp busy several times over
     // ~16 jobs per resident warp: the launch tail (one job) stays a few % of the level
     const unsigned long long want_jobs =

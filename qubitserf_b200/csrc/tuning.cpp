@@ -24,6 +24,7 @@ bool set_key(Tuning& t, const std::string& key, const std::string& val) {
     else if (key == "tc_small_tiles") t.tc_small_tiles = std::max(0ll, iv);
     else if (key == "cc_jobs_per_warp") t.cc_jobs_per_warp = (int)std::max(1ll, std::min(256ll, iv));
     else if (key == "tc_cost_ratio") t.tc_cost_ratio = std::max(0.0, std::min(4.0, v));
+    else if (key == "tc_edge_div") t.tc_edge_div = (int)std::max(1ll, std::min(64ll, iv));
     else if (key == "exec_groups") t.exec_groups = (int)std::max(1ll, std::min(16ll, iv));
     else if (key == "batch_chunks") t.batch_chunks = (int)std::max(1ll, std::min(64ll, iv));
     else if (key == "overlap_groups") t.overlap_groups = (int)std::max(1ll, std::min(16ll, iv));
@@ -61,6 +62,7 @@ Tuning load() {
     }
     static const char* const keys[] = {"tc_shape", "tc_job_tiles.small", "tc_job_tiles.large",
                                        "tc_small_tiles", "cc_jobs_per_warp", "tc_cost_ratio",
+                                       "tc_edge_div",
                                        "exec_groups", "batch_chunks", "overlap_groups",
                                        "batch_first_permille"};
     for (const char* k : keys) {

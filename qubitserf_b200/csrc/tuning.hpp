@@ -17,6 +17,9 @@ struct Tuning {
     long long tc_small_tiles = 4096;   // level-size class boundary: tiles of its tensor plan
     int cc_jobs_per_warp = 16;         // CUDA-core sweep: jobs per resident warp (loop tile)
     double tc_cost_ratio = 0.6;        // tensor plan when its cost < ratio x CUDA-core cost
+    // terms join a level's tensor-core range while their prefix rows reach tile rows / div
+    // and their suffix columns tile columns / div (the rest go to the CUDA cores)
+    int tc_edge_div = 2;
     int exec_groups = 3;               // interleaved job groups of qsfb_batch_execute
     int batch_chunks = 4;              // pipeline chunks of the one-shot qsfb_batch
     // the first chunk's share of the batch in 1/1000 (0: half a chunk, nq / (2 chunks));

@@ -40,6 +40,7 @@ RESIDENT_KNOBS = [
     ("tc_small_tiles", [4096, 1024, 16384]),
     ("cc_jobs_per_warp", [16, 8, 32]),
     ("tc_cost_ratio", [0.6, 0.4, 0.8, 1.0]),
+    ("tc_edge_div", [2, 4, 8, 16]),
     ("exec_groups", [3, 2, 4]),
 ]
 E2E_KNOBS = [
