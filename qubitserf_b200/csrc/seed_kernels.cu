@@ -32,14 +32,22 @@ template <int W, int S, int WD>
 __device__ __forceinline__ bool eliminate_column(unsigned long long (&r)[S][W],
                                                  unsigned long long bit, uint32_t& piv,
                                                  uint32_t& pos, int rank, int lane) {
-    // the first row, in row order, that is no pivot row yet and has a 1 in the column
+    // the first row, in row order, that is no pivot row yet and has a 1 in the column (the
+    // rows' bits in the column are read once, for this search and for the clearing below)
+    bool hit[S];
+    unsigned m[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        hit[s] = (r[s][WD] & bit) != 0ull;
+        m[s] = __ballot_sync(0xffffffffu, hit[s] && ((piv >> s) & 1u) == 0u);
+    }
     int sel = -1;
 #pragma unroll
-    for (int s = S - 1; s >= 0; --s) {
-        const unsigned m =
-            __ballot_sync(0xffffffffu, (r[s][WD] & bit) != 0ull && ((piv >> s) & 1u) == 0u);
-        if (m) sel = 32 * s + __ffs(m) - 1;
-    }
+    for (int s = 0; s < S; ++s)
+        if (m[s]) {   // the same on every lane
+            sel = 32 * s + __ffs(m[s]) - 1;
+            break;
+        }
     if (sel < 0) return false;
     const int ps = sel >> 5, pl = sel & 31;   // the same on every lane
     unsigned long long pv[W];
@@ -56,7 +64,7 @@ __device__ __forceinline__ bool eliminate_column(unsigned long long (&r)[S][W],
     // clear the column from every other row
 #pragma unroll
     for (int s = 0; s < S; ++s)
-        if ((r[s][WD] & bit) && !(s == ps && lane == pl)) {
+        if (hit[s] && !(s == ps && lane == pl)) {
 #pragma unroll
             for (int w = 0; w < W; ++w) r[s][w] ^= pv[w];
         }
