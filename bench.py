@@ -33,6 +33,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "certs/s batched vs plain on 1 B200 (exact d); Gcodewords/s vs int-pipe peak"
 TC_OPS_PER_PAIR = 2 * 64  # int8 multiply-adds of the tensor-core filter: 64 columns per pair
 POPC_PER_CLK_SM = 16     # 32-bit POPC results per clock per SM (CUDA arithmetic throughput table)
+TC_ACCUMULATORS_PER_SM = 2 * 128 * 256   # tensor sweep: two 128 x 256 TMEM buffers per SM
+TC_ROUND_TRIP_CYCLES = 1450              # one buffer's MMA -> read-back -> release, measured
 
 
 def peaks():
@@ -471,7 +473,17 @@ def main():
                                     "all below saturation)",
                         "tmem_columns_read_gbs": tc_cw * 4 / max(tc_s, 1e-12) / 1e9,
                         "tmem_bytes_per_clk_per_sm": tc_cw * 4 / max(tc_s, 1e-12) /
-                                                     (nsm * f_mhz * 1e6)},
+                                                     (nsm * f_mhz * 1e6),
+                        # 65,536 accumulators per SM retire once per buffer round trip; the
+                        # round trip (1,300-1,600 cycles) was measured by a clock64-stamped
+                        # build of the kernel (profiles/pairs_tc_kernel_batch128.md)
+                        "round_trip_cycles": TC_ROUND_TRIP_CYCLES,
+                        "bound_pairs_per_s": TC_ACCUMULATORS_PER_SM * nsm * f_mhz * 1e6 /
+                                             TC_ROUND_TRIP_CYCLES,
+                        "pairs_per_s": tc_cw / max(tc_s, 1e-12),
+                        "frac_of_bound": tc_cw / max(tc_s, 1e-12) /
+                                         (TC_ACCUMULATORS_PER_SM * nsm * f_mhz * 1e6 /
+                                          TC_ROUND_TRIP_CYCLES)},
             "codeword_share": tc_cw / max(cw, 1),
             "kernel_ms_per_step": tc_ms / max(args.steps, 1)},
         "roofline_list_generation": list_generation_roofline(st1, pk),
