@@ -476,7 +476,7 @@ def main():
                                                      (nsm * f_mhz * 1e6),
                         # 65,536 accumulators per SM retire once per buffer round trip; the
                         # round trip (1,300-1,600 cycles) was measured by a clock64-stamped
-                        # build of the kernel (profiles/pairs_tc_kernel_batch128.md)
+                        # build of the kernel
                         "round_trip_cycles": TC_ROUND_TRIP_CYCLES,
                         "bound_pairs_per_s": TC_ACCUMULATORS_PER_SM * nsm * f_mhz * 1e6 /
                                              TC_ROUND_TRIP_CYCLES,
