@@ -993,7 +993,8 @@ int qsfb_batch(const QsfbQuery* queries, int nq, int host_threads, QsfbAnswer* o
         alloc0[2] = tdev->n_pinned_alloc; alloc0[3] = tdev->ns_pinned_alloc;
     }
     constexpr int kPipeMin = 256;   // below this the batch runs in one piece
-    // QSFB_BATCH_CHUNKS: number of pipeline chunks (default 4; 1 = one piece), read per call.
+    // QSFB_BATCH_CHUNKS: number of pipeline chunks (default: the tuning table's; 1 = one
+    // piece), read per call.
     const char* ce = std::getenv("QSFB_BATCH_CHUNKS");
     const int chunks = std::max(1, std::min(ce ? std::atoi(ce) : tuning().batch_chunks, 64));
     std::vector<int> cut{0};
