@@ -463,6 +463,15 @@ int debug_level() {
     return lvl;
 }
 
+// Rank-deficient sets on the tensor-core sweep (QSFB_TENSOR_RD=0: on the CUDA cores).
+bool rd_tensor() {
+    static const bool on = [] {
+        const char* e = std::getenv("QSFB_TENSOR_RD");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // Tensor-core sweep switch: QSFB_TENSOR=0 keeps every level on the CUDA-core kernels.
 bool tensor_enabled() {
     static const bool on = [] {
@@ -606,9 +615,13 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             P.nterms = K - b - a + 1;
             int ks = 0, nl = 0;
             // (+-1 lists hold 64 bytes per entry: keep them, and their 32-bit row indices, modest)
-            if (tensor_enabled() && P.full && P.HP >= 2 && b > 0 &&
+            // a rank-deficient set: the sweep adds each prefix entry's own pivot-row count and
+            // the fewest a suffix entry can hold, b - (K - rank); for the cost model a prefix
+            // entry typically holds all a of its rows as pivots
+            const int rd_allow = T - 1 - (a + std::max(0, b - (K - rank)));
+            if (tensor_enabled() && P.HP >= 2 && b > 0 && (P.full || rd_tensor()) &&
                 dev->binom(K, a) < (1ull << 28) && dev->binom(K, b) < (1ull << 28))
-                ks = tc_depth(nred, T - 1 - w, P.popcs, &nl);
+                ks = tc_depth(nred, P.full ? T - 1 - w : rd_allow, P.popcs, &nl);
             if (debug_level() == 2 && pairs > (1ull << 26))
                 std::fprintf(stderr, "qsfb plan: K=%d w=%d a=%d b=%d nred=%d rank=%d HP=%d T=%d "
                              "mode=%d filt=%d ks=%d\n", K, w, a, b, nred, rank, P.HP, T, P.mode,

@@ -326,7 +326,10 @@ struct TcJobRec {
     unsigned long long* key;
     unsigned int r0, xoff, nx, ny;
     unsigned int d, b0, b1;
-    unsigned int tnw;     // bound field (bits 0-11) | n_live << 12 | w << 20
+    // bound field (bits 0-11) | n_live << 12 | w << 20; for a rank-deficient set the w field
+    // holds the fewest pivot rows a suffix entry can have, and bit 31 says that each prefix
+    // row adds its own pivot-row count
+    unsigned int tnw;
     unsigned long long pad;
 };
 static_assert(sizeof(TcJobRec) == 64, "job record layout");
@@ -372,7 +375,10 @@ __global__ void __launch_bounds__(256) tc_jobs_kernel(const LevelDesc* __restric
         R.b0 = (unsigned int)(jc * jb);
         R.b1 = (unsigned int)(jc * jb + jb < nbt ? jc * jb + jb : nbt);
         const unsigned int T0 = (unsigned int)(*((volatile unsigned long long*)D.key) >> kKeyWtShift);
-        R.tnw = (T0 & 0xFFFu) | ((unsigned int)D.n_live << 12) | ((unsigned int)D.w << 20);
+        // rank-deficient set: a suffix entry holds at least b - (K - rank) pivot rows
+        const unsigned int wf =
+            D.pca ? ((unsigned int)max(0, D.b - (D.K - D.rank)) | 0x800u) : (unsigned int)D.w;
+        R.tnw = (T0 & 0xFFFu) | ((unsigned int)D.n_live << 12) | (wf << 20);
         R.pad = 0;
         recs[job] = R;
     }
@@ -533,7 +539,12 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
             int T = (int)(C.tnw & 0xFFFu);
             if (C.key == kptr) T = min(T, tkey);
             const unsigned long long kv = *((volatile unsigned long long*)C.key);
-            const int n_live = (int)((C.tnw >> 12) & 0xFFu), w = (int)(C.tnw >> 20);
+            const int n_live = (int)((C.tnw >> 12) & 0xFFu);
+            const bool rd = ((C.tnw >> 20) & 0x800u) != 0u;   // rank-deficient set
+            const int w = (int)((C.tnw >> 20) & 0x7FFu);
+            // pivot rows of this lane's prefix entry (its own count on a rank-deficient set,
+            // else part of w); the bound below holds for every suffix entry of the set
+            const int pcx = rd && valid ? (int)__ldg(D.pca + r) : 0;
             for (unsigned long long bt = b0; bt < b1; ++bt, ++it_c) {
                 const uint32_t ac = it_c & 1u;
                 if (ac != group) continue;               // the other group's tile
@@ -544,7 +555,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                 if (!ok) break;
                 tc_fence_after();
                 __syncwarp();   // the TMEM load below is warp-collective
-                const int thr = n_live - 2 * (T - 1 - w);
+                const int thr = n_live - 2 * (T - 1 - w - pcx);
                 // the accumulators are in [-64, 64]: read them as packed 16-bit halves
                 uint32_t v[64];
                 tmem_ld128_p16(tmem + ((uint32_t)(quarter * 32) << 16) + ac * 256u + col0, v);
@@ -580,6 +591,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                     need &= need - 1u;
                     const unsigned long long rr = __shfl_sync(0xffffffffu, r, src);
                     const uint32_t fl = __shfl_sync(0xffffffffu, flags, src);
+                    const int pcr = __shfl_sync(0xffffffffu, pcx, src);
                     const int HP = D.HP;
                     uint32_t xr[4] = {0u, 0u, 0u, 0u};
                     for (int h = 0; h < HP; ++h) xr[h] = __ldg(D.la + rr * HP + h);
@@ -591,7 +603,7 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                                 (unsigned long long)(sl * kTcSlice + part * 32 + lane);
                             bool cand = false;
                             if (c < C.ny) {
-                                int lb = D.a + D.b;
+                                int lb = rd ? pcr + (int)__ldg(D.pcb + c) : D.a + D.b;
                                 for (int h = 0; h < HP; ++h)
                                     lb += __popc(xr[h] ^ __ldg(D.rb + c * HP + h));
                                 cand = lb < T;
@@ -602,7 +614,9 @@ pairs_tc_kernel(const LevelDesc* __restrict__ descs, const TcJobRec* __restrict_
                                 cm &= cm - 1u;
                                 const unsigned long long cc = __shfl_sync(0xffffffffu, c, s2);
                                 int Tn = T;
-                                if (lane == 0) Tn = survivor_scan(D, B, 1, C.xoff, rr - C.xoff, D.a, cc, 1, T);
+                                if (lane == 0)
+                                    Tn = survivor_scan(D, B, 1, C.xoff, rr - C.xoff, rd ? pcr : D.a,
+                                                       cc, 1, T);
                                 T = __shfl_sync(0xffffffffu, Tn, 0);
                             }
                         }
