@@ -489,7 +489,10 @@ bool tensor_enabled() {
 // pair, ~1280 in zero-test mode.  Returns the MMA steps (2) or 0.
 int tc_depth(int n_enc, int t, int popcs, int* n_live) {
     const int nl = std::min(n_enc, 64);
-    if (nl <= 32 || t >= nl / 2) return 0;   // the filter would reject (almost) nothing
+    // the filter would reject (almost) nothing; up to 32 live columns (one probe word) the
+    // +-1 rows carry zeros beyond them, and the 64-column filter is exact over the set's
+    // non-pivot columns
+    if (nl < 8 || t >= nl / 2) return 0;
     const double pass = hamming_pass_rate(nl, t);
     const double cost = 262.0 + 512.0 * 64.0 * pass * 1300.0 / 8.0;
     const double cc = popcs > 0 ? 2048.0 * popcs : 1280.0;
@@ -619,7 +622,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             // the fewest a suffix entry can hold, b - (K - rank); for the cost model a prefix
             // entry typically holds all a of its rows as pivots
             const int rd_allow = T - 1 - (a + std::max(0, b - (K - rank)));
-            if (tensor_enabled() && P.HP >= 2 && b > 0 && (P.full || rd_tensor()) &&
+            if (tensor_enabled() && b > 0 && (P.full || rd_tensor()) &&
                 dev->binom(K, a) < (1ull << 28) && dev->binom(K, b) < (1ull << 28))
                 ks = tc_depth(nred, P.full ? T - 1 - w : rd_allow, P.popcs, &nl);
             if (debug_level() == 2 && pairs > (1ull << 26))
