@@ -559,7 +559,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     // QSFB_DEBUG=5: pairs of this call by sweep and by why a plan stays on the CUDA cores
     // (rank-deficient, zero test, one probe word, no second list, list over 2^28 entries,
     // the cost model, the terms outside the tensor range)
-    unsigned long long why[8] = {0, 0, 0, 0, 0, 0, 0, 0}, tc_sum = 0;
+    unsigned long long why[8] = {0, 0, 0, 0, 0, 0, 0, 0}, tc_sum = 0, edge_lo = 0, edge_hi = 0;
     for (size_t r = 0; r < reqs.size(); ++r) {
         const LevelReq& q = reqs[r];
         SideDev* S = q.side;
@@ -642,6 +642,8 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
             }
             if (debug_level() == 5) {
                 why[6] += lo_pairs + hi_pairs;
+                edge_lo += lo_pairs;
+                edge_hi += hi_pairs;
                 tc_sum += tc_pairs;
             }
             const int p_end = P.p_lo + P.nterms;   // one past the last term
@@ -672,8 +674,10 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     }
     if (debug_level() == 5)
         std::fprintf(stderr, "qsfb plan pairs: tc %llu | cc rank-deficient %llu zero-test %llu "
-                     "one-word %llu one-list %llu big-list %llu cost-model %llu edge-terms %llu\n",
-                     tc_sum, why[0], why[1], why[2], why[3], why[4], why[5], why[6]);
+                     "one-word %llu one-list %llu big-list %llu cost-model %llu edge-terms %llu "
+                     "(few prefix rows %llu, few suffix columns %llu)\n",
+                     tc_sum, why[0], why[1], why[2], why[3], why[4], why[5], why[6], edge_lo,
+                     edge_hi);
     // loop tile: enough jobs to keep every resident warp busy several times over
     // ~16 jobs per resident warp: the launch tail (one job) stays a few % of the level
     const unsigned long long want_jobs =
