@@ -454,7 +454,8 @@ unsigned long long key_init(int bound) {
 }
 
 // QSFB_DEBUG=<level>: diagnostics on stderr (1 failures, 2 plans of heavy levels, 3
-// tensor-core launch statistics); read once.
+// tensor-core launch statistics, 4 planner phase times, 5 pairs by sweep, 6 CUDA-core job
+// statistics); read once.
 int debug_level() {
     static const int lvl = [] {
         const char* e = std::getenv("QSFB_DEBUG");
@@ -901,6 +902,29 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         std::fprintf(stderr, "qsfb tc launch: jobs=%llu tiles=%llu pairs=%llu tile_util=%.3f tiles_per_job=%.2f\n",
                      tc_jobs, tiles, pairs, (double)pairs / ((double)tiles * tcM * tcN),
                      (double)tiles / (double)tc_jobs);
+    }
+
+    if (debug_level() == 6) {   // CUDA-core jobs of this call: how many, how big, how short
+        unsigned long long jobs = 0, pairs = 0, sjobs = 0, spairs = 0;
+        for (const Plan& P : plans) {
+            if (P.tc) continue;
+            const int K = reqs[P.req].side->K;
+            for (int t = 0; t < P.nterms; ++t) {
+                const int p = P.p_lo + t;
+                const unsigned long long nx = dev->binom(p, P.a - 1), ny = dev->binom(K - 1 - p, P.b);
+                const unsigned long long rn = std::max(nx, ny), ln = std::min(nx, ny);
+                const unsigned long long j = ((rn + kRegTile - 1) / kRegTile) *
+                                             ((ln + loop_tile - 1) / loop_tile);
+                jobs += j;
+                pairs += nx * ny;
+                if (ln < (unsigned long long)loop_tile / 4) { sjobs += j; spairs += nx * ny; }
+            }
+        }
+        if (jobs)
+            std::fprintf(stderr, "qsfb cc launch: jobs=%llu pairs=%llu loop_tile=%d pairs_per_job=%.0f "
+                         "short-loop (< tile/4) jobs=%llu pairs=%llu pairs_per_job=%.0f\n",
+                         jobs, pairs, loop_tile, (double)pairs / (double)jobs, sjobs, spairs,
+                         sjobs ? (double)spairs / (double)sjobs : 0.0);
     }
 
     // launch groups: CUDA-core variants (filter, HP, mode), then one tensor-core group
