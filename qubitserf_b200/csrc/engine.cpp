@@ -455,7 +455,7 @@ unsigned long long key_init(int bound) {
 
 // QSFB_DEBUG=<level>: diagnostics on stderr (1 failures, 2 plans of heavy levels, 3
 // tensor-core launch statistics, 4 planner phase times, 5 pairs by sweep, 6 CUDA-core job
-// statistics); read once.
+// statistics, 7 a device timeline line per round); read once.
 int debug_level() {
     static const int lvl = [] {
         const char* e = std::getenv("QSFB_DEBUG");
@@ -543,6 +543,18 @@ int level_size_rc(int K, int w) {
     if (host_binom(K, a) > kMaxListEntries || host_binom(K, b) > kMaxListEntries)
         return kErrMemory;
     return kOk;
+}
+
+// The reference point of the QSFB_DEBUG=7 timelines: one event, recorded on the stream of
+// the first round that asks for it.
+static cudaEvent_t timeline_base(cudaStream_t st) {
+    static const cudaEvent_t base = [st] {
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        return e;
+    }();
+    return base;
 }
 
 int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelOut>& outs,
@@ -1091,6 +1103,17 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         stats->host_plan_s +=
             std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
     cudaStream_t st = s->stream;
+    // QSFB_DEBUG=7: this round's device timeline (staging copy, end of list generation,
+    // tensor sweep, join) against one base event of the process, a line per round
+    const bool timeline = debug_level() == 7;
+    const double plan_ms =
+        1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - tp0).count();
+    cudaEvent_t tl[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (timeline) {
+        timeline_base(st);
+        for (cudaEvent_t& e : tl) cudaEventCreate(&e);
+        cudaEventRecord(tl[0], st);
+    }
     if (cudaMemcpyAsync(d, h, total_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemsetAsync(s->d_ctr.d, 0, s->d_ctr.cap, st) != cudaSuccess) {
         cudaGetLastError();
@@ -1120,6 +1143,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
     cudaEvent_t evm;
     cudaEventCreate(&evm);
     cudaEventRecord(evm, st);
+    if (timeline) cudaEventRecord(tl[1], st);
     // fork: the pair launches (independent levels; they share only the atomic witness keys)
     // go round-robin over the auxiliary streams, the tensor-core sweep first.
     // QSFB_SERIAL_PAIRS (read per call): all on one stream, so that each kernel's events
@@ -1138,6 +1162,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         cudaStream_t gs = s->aux[serial_pairs ? 0 : next_aux];
         next_aux = (next_aux + 1) % Session::kAux;
         if (Gp.tc) cudaEventRecord(s->ev_tc0, gs);
+        if (Gp.tc && timeline) cudaEventRecord(tl[2], gs);
         const cudaError_t e =
             Gp.tc ? launch_pairs_tc(gd, Gp.count, Gp.jobs, dev->d_binom, d + off_recs,
                                     (int*)(d + off_err), dev->num_sms, gs)
@@ -1156,6 +1181,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         }
         if (Gp.tc) {
             cudaEventRecord(s->ev_tc1, gs);
+            if (timeline) cudaEventRecord(tl[3], gs);
             tc_timed = true;
             launches += 1;   // the job-decode kernel
         }
@@ -1168,6 +1194,7 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         cudaStreamWaitEvent(st, s->ev_join[k], 0);
     }
     cudaEventRecord(s->ev1, st);
+    if (timeline) cudaEventRecord(tl[4], st);
     cudaError_t se = cudaMemcpyAsync(h + off_keys, d + off_keys, off_err + 8 - off_keys,
                                      cudaMemcpyDeviceToHost, st);
     if (se == cudaSuccess) se = cudaStreamSynchronize(st);
@@ -1253,6 +1280,15 @@ int run_levels(Session* s, const std::vector<LevelReq>& reqs, std::vector<LevelO
         for (const auto& kv : tc_rows)
             stats->tc_operand_bytes += (kv.second.second - kv.second.first) * kPmRowBytes;
         stats->launches += launches;
+    }
+    if (timeline) {
+        float t[5] = {0.f, 0.f, -1.f, -1.f, 0.f};
+        const cudaEvent_t b = timeline_base(st);
+        for (int i = 0; i < 5; ++i)
+            if ((i != 2 && i != 3) || tc_timed) cudaEventElapsedTime(&t[i], b, tl[i]);
+        std::fprintf(stderr, "qsfb timeline %p plan_ms %.3f h2d %.3f gen_end %.3f tc %.3f %.3f "
+                     "join %.3f\n", (void*)s, plan_ms, t[0], t[1], t[2], t[3], t[4]);
+        for (cudaEvent_t e : tl) cudaEventDestroy(e);
     }
     cudaEventDestroy(evm);
     return kOk;
