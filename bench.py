@@ -395,7 +395,7 @@ def main():
     # --- end to end: the one-shot public call from host matrices, K times, after untimed
     # warm-up calls of the same call (its chunk sizes and sessions differ from the resident
     # run's, and a first call would time their device allocations)
-    for _ in range(max(1, min(args.warmup, 2))):
+    for _ in range(max(1, args.warmup)):
         batch.run()
     e2e_t = []
     alloc0 = _native.alloc_counters()

@@ -117,12 +117,12 @@ void* Device::alloc(size_t bytes) {
     const size_t b = round_bucket(bytes);
     {
         std::lock_guard<std::mutex> lk(mu_);
-        // The bucket itself, else a cached block of the next bucket: a miss maps new memory
-        // (milliseconds for large blocks, kept by the pool for good), while the number of
-        // blocks of one size live at once varies with the timing of concurrent work.  A
-        // block keeps its own size through later releases.
-        auto it = free_.find(b);
-        if (it == free_.end()) it = free_.find(2 * b);
+        // The smallest cached block of this bucket or up to three buckets above it: a miss
+        // maps new memory (milliseconds for large blocks, kept by the pool for good), while
+        // the number of blocks of one size live at once varies with the timing of
+        // concurrent work.  A block keeps its own size through later releases.
+        auto it = free_.lower_bound(b);
+        if (it != free_.end() && it->first > 8 * b) it = free_.end();
         if (it != free_.end()) {
             void* p = it->second;
             const size_t sz = it->first;
